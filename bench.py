@@ -1,0 +1,374 @@
+#!/usr/bin/env python3
+"""Newton updates/s of the implicit 256^2 k=8 DG and condensed-HDG Euler solve on B200.
+
+Workload (the reference's speed protocol, speed_test/2d/benchmark.py:21-44): rotated simple wave
+(alpha = 45 deg, gamma = 3) on a periodic 256 x 256 mesh, Q8 (k = 8, 324 unknowns per cell),
+backward Euler at CFL 5, one stage, GMRES(20) with exact block-Jacobi, ntol = ltol = 1e-12,
+HLL safety 1.1.  A "step" is one Newton update.  Per configuration (method x precision):
+  warm-up : W updates from the projected initial state (untimed),
+  protocol: reset to the initial state, update 1 untimed (the reference's warm-up update),
+  timed   : the next K updates (protocol updates 2..K+1), bracketed by barrier + synchronize and
+            CUDA events on the library's stream; K=3 is exactly the reference's measured set.
+value = (K_dg + K_hdg) / (t_dg + t_hdg) for the mixed-precision (FP32 block-Jacobi factors,
+FP64 everything else) DG and HDG solves; the FP64 forms and the per-method numbers are in
+"breakdown".  e2e repeats the timed updates through the C ABI with host buffers
+(dgh_newton_update_host: state H2D, update, state D2H every step).
+
+--impl reference times the reference algorithm's CPU implementation (the oracle restatement;
+the reference itself needs Eigen, which this image lacks) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Newton updates/s, 256² k=8 DG & HDG, mixed-prec vs FP64 GPU at equal residual tol"
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--nx", type=int, default=256)
+    p.add_argument("--k", type=int, default=8)
+    p.add_argument("--ltol", type=float, default=1e-12)
+    p.add_argument("--configs", default="dg:mixed,hdg:mixed,dg:fp64,hdg:fp64")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-nx", type=int, default=32)
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        pw = [float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows), "power_w_max": max(pw) if pw else None}
+
+
+# ------------------------------------------------------------------------------ distributed plumbing
+def dist_setup(gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=None)
+        pg = dist
+    return rank, local, world, pg
+
+
+def barrier(pg, torch):
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+
+
+def allmax(pg, torch, value: float) -> float:
+    if pg is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------ our arm
+def algorithmic_bytes(kind: str, m: int, cells: int, fw: int, faces: int, t: int, precision: str) -> float:
+    """Bytes one launch of the dominant kernel must move (factors read once, rhs and result)."""
+    s = 4 if precision == "mixed" else 8
+    if kind == "dg":  # k_lu_solve over E blocks: m^2 factors, m perm ints, rhs and result
+        return cells * (m * m * s + m * 4 + 2 * m * 8)
+    if kind == "hdg_schur":  # k_hdg_apply: every S_K read once, lambda gathered, result written
+        return cells * t * t * 8 + faces * fw * 8 * 3
+    raise ValueError(kind)
+
+
+def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: bool, rank: int, local: int):
+    from dg_hdg_euler_cpp_b200 import _lib
+    from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
+
+    K, W = args.steps, args.warmup
+    s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=W + K + 2,
+               method=method, precision=precision, restart=20, max_linear=1500, ntol=args.ltol, ltol=args.ltol,
+               safety=1.1, device=local)
+    it = Integrator(s, method)
+    stream = torch.cuda.ExternalStream(s.stream(), device=s.device)
+    u0 = s.initial()
+    # warm-up
+    it.stage_begin(u0)
+    for _ in range(W):
+        it.update()
+    # protocol: reset, untimed update 1
+    it.stage_begin(u0)
+    first = it.update()
+    barrier(pg, torch)
+    lib = s.lib
+    lib.dgh_timing_enable(s.h, 1)
+    launches0 = s.launch_count()
+    sampler = ClockSampler(local) if sampler_on else None
+    if sampler:
+        sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rows = [it.update() for _ in range(K)]
+    e1.record(stream)
+    e1.synchronize()
+    barrier(pg, torch)
+    if sampler:
+        sampler.stop()
+    ms = allmax(pg, torch, e0.elapsed_time(e1))
+    launches = s.launch_count() - launches0
+    timers = {}
+    for name, cat in (("precond", 0), ("operator", 1), ("arnoldi", 2), ("factor", 3), ("face_factor", 4),
+                      ("condense", 5), ("residual", 6)):
+        tot, cnt = ctypes.c_double(), ctypes.c_int64()
+        lib.dgh_timing_read(s.h, cat, ctypes.byref(tot), ctypes.byref(cnt))
+        timers[name] = {"ms": tot.value, "launches": cnt.value}
+    lib.dgh_timing_enable(s.h, 0)
+    final = np.empty(s.size)
+    lib.dgh_download(s.h, final.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(it.state_ptr()), s.size)
+    out = {
+        "method": method, "precision": precision, "updates": K, "ms": ms, "updates_per_s": 1000.0 * K / ms,
+        "ms_per_update": ms / K, "krylov": [r["krylov_iterations"] for r in rows],
+        "krylov_update1": first["krylov_iterations"],
+        "rms": [r["residual_physical_rms"] for r in rows], "damping": [r["damping"] for r in rows],
+        "launches": launches, "timers": timers, "device_gb": s.device_bytes() / 1e9,
+        "clocks": sampler.summary() if sampler else None,
+    }
+    # dominant per-iteration kernel of this configuration
+    if method == "dg":
+        kb = algorithmic_bytes("dg", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
+        tk = timers["precond"]
+        kernel = "k_lu_solve<%s> (block-Jacobi solve, one launch per Krylov iteration)" % (
+            "float" if precision == "mixed" else "double")
+    else:
+        kb = algorithmic_bytes("hdg_schur", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
+        tk = timers["operator"]
+        kernel = "k_hdg_apply (face-owned Schur apply, one launch per Krylov iteration)"
+    avg_ms = tk["ms"] / max(tk["launches"], 1)
+    achieved = kb / (avg_ms * 1e-3) / 1e9
+    out["roofline"] = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                       "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "bytes_per_launch": kb,
+                       "avg_launch_ms": avg_ms, "launches": tk["launches"]}
+    # e2e through the C ABI with host buffers
+    if not args.no_e2e:
+        it.stage_begin(u0)
+        it.update()
+        host = torch.empty(s.size, dtype=torch.float64, pin_memory=True)
+        lib.dgh_download(s.h, ctypes.c_void_p(host.data_ptr()), ctypes.c_void_p(it.state_ptr()), s.size)
+        st = _lib.dgh_update_stats()
+        barrier(pg, torch)
+        t0 = time.perf_counter()
+        for _ in range(K):
+            rc = lib.dgh_newton_update_host(it.h, ctypes.c_void_p(host.data_ptr()), ctypes.byref(st))
+            if rc != 0:
+                raise RuntimeError(lib.dgh_integrator_error(it.h).decode())
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        barrier(pg, torch)
+        e2e_s = allmax(pg, torch, t1 - t0)
+        out["e2e"] = {"seconds": e2e_s, "updates_per_s": K / e2e_s, "h2d_bytes_per_step": s.size * 8,
+                      "d2h_bytes_per_step": s.size * 8}
+    it.close()
+    s.close()
+    torch.cuda.empty_cache()
+    return out, final
+
+
+def cpu_baseline(args, threads: int, steps: int, warm: int):
+    """The oracle (a restatement of the reference's CPU algorithm) on the host cores: the same
+    protocol at a reduced mesh of the same degree, DG and HDG, scaled by the cell-count ratio."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py
+
+    n = args.cpu_sample_nx
+    scale = (args.nx / n) ** 2
+    res = {}
+    for method in ("dg", "hdg"):
+        o = oracle_py.Oracle(f"--nx {n} --ny {n} --k {args.k} --integrator be --steps 1 --newton-steps "
+                             f"{warm + 1 + steps} --warmup-updates {warm + 1} --cfl 5 --restart 20 --ntol {args.ltol} "
+                             f"--ltol {args.ltol} --safety 1.1", threads=threads)
+        u0 = o.initial()
+        _, st, ups = o.advance(method, u0)
+        timed = ups[warm + 1: warm + 1 + steps]
+        sec = float(np.sum(timed[:, 12]))
+        res[method] = {"sample_seconds_per_update": sec / len(timed), "krylov": timed[:, 3].astype(int).tolist(),
+                       "projected_256_seconds_per_update": sec / len(timed) * scale}
+    total = res["dg"]["projected_256_seconds_per_update"] + res["hdg"]["projected_256_seconds_per_update"]
+    return {"value": 2.0 / total, "unit": "updates/s", "cores": threads, "kind": "port",
+            "sample": f"oracle (C++ restatement of the reference, FP64, {threads} threads) on {n}x{n} k={args.k}, "
+                      f"same BE CFL5 GMRES(20) protocol, {steps} timed updates per method after {warm + 1} warm-up; "
+                      f"per-update time scaled by the cell ratio {scale:g} to 256^2",
+            "per_method": res}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return main_reference(args)
+    import torch
+
+    rank, local, world, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    if peaks_path.exists():
+        peaks = json.loads(peaks_path.read_text())
+        peak_src = "measured"
+    else:
+        peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+        peak_src = "fallback"
+    configs = [c.split(":") for c in args.configs.split(",")]
+    results = {}
+    finals = {}
+    for method, precision in configs:
+        out, final = run_config(args, method, precision, torch, pg, peaks, rank == 0, rank, local)
+        results[f"{method}_{precision}"] = out
+        finals[(method, precision)] = final
+    # error of the mixed-precision state against the all-FP64 state after the same updates
+    for method in ("dg", "hdg"):
+        if (method, "mixed") in finals and (method, "fp64") in finals:
+            a, b = finals[(method, "mixed")], finals[(method, "fp64")]
+            results[f"{method}_mixed"]["rel_error_vs_fp64"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+            results[f"{method}_mixed"]["speedup_vs_fp64"] = (results[f"{method}_mixed"]["updates_per_s"] /
+                                                            results[f"{method}_fp64"]["updates_per_s"])
+            results[f"{method}_mixed"]["krylov_change_vs_fp64"] = (
+                sum(results[f"{method}_mixed"]["krylov"]) - sum(results[f"{method}_fp64"]["krylov"]))
+    head = [k for k in ("dg_mixed", "hdg_mixed") if k in results] or list(results)
+    tot_upd = sum(results[k]["updates"] for k in head)
+    tot_ms = sum(results[k]["ms"] for k in head)
+    value = world * 1000.0 * tot_upd / tot_ms
+    dom = results[head[0]]["roofline"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot_ms / tot_upd, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (FP32 block-Jacobi factors in the mixed forms)", "data": "synthetic",
+        "config": {"workload": f"{args.nx}x{args.nx} k={args.k} rotated simple wave, BE CFL5, GMRES(20), exact "
+                               f"block-Jacobi, ntol=ltol={args.ltol:g}, one Newton update per step; value combines "
+                               f"the {' and '.join(head)} solves", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (factor pool 27-55 GB, Schur pool 10.9 GB)",
+                   "value_definition": "(K_dg+K_hdg)/(t_dg+t_hdg) over the mixed-precision DG and HDG solves"},
+        "roofline": {k: dom[k] for k in ("bound", "achieved", "peak", "unit", "frac")} | {
+            "traffic": None, "kernel": dom["kernel"], "peak_source": peak_src,
+            "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_launch_ms"]},
+        "gpu_launches": int(sum(results[k]["launches"] for k in head)),
+        "breakdown": results,
+    }
+    clocks = [results[k]["clocks"] for k in head if results[k].get("clocks")]
+    if clocks:
+        c0 = clocks[0]
+        line["clocks"] = {"sm_mhz": c0["sm_mhz"], "sm_max_mhz": c0["sm_max_mhz"],
+                          "reasons": sorted({r for c in clocks for r in c["reasons"]})}
+    if not args.no_e2e and all("e2e" in results[k] for k in head):
+        e2e_s = sum(results[k]["e2e"]["seconds"] for k in head)
+        line["e2e"] = {"value": world * tot_upd / e2e_s, "unit": "updates/s",
+                       "h2d_bytes_per_step": results[head[0]]["e2e"]["h2d_bytes_per_step"],
+                       "d2h_bytes_per_step": results[head[0]]["e2e"]["d2h_bytes_per_step"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, os.cpu_count() or 1, 1, 0)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py
+
+    n = args.cpu_sample_nx
+    scale = (args.nx / n) ** 2
+    K, W = args.steps, args.warmup
+    per = {}
+    for method in ("dg", "hdg"):
+        o = oracle_py.Oracle(f"--nx {n} --ny {n} --k {args.k} --integrator be --steps 1 --newton-steps {W + 1 + K} "
+                             f"--warmup-updates {W + 1} --cfl 5 --restart 20 --ntol {args.ltol} --ltol {args.ltol} "
+                             f"--safety 1.1", threads=threads)
+        _, st, ups = o.advance(method, o.initial())
+        timed = ups[W + 1: W + 1 + K]
+        per[method] = {"sample_seconds": float(np.sum(timed[:, 12])), "krylov": timed[:, 3].astype(int).tolist()}
+    total_sample = per["dg"]["sample_seconds"] + per["hdg"]["sample_seconds"]
+    value = 2.0 * K / (total_sample * scale)
+    sample = (f"oracle (C++ restatement of the reference's CPU algorithm, FP64, {threads} threads) on {n}x{n} "
+              f"k={args.k} with the same BE CFL5 GMRES(20) protocol; per-update time scaled by the cell ratio "
+              f"{scale:g} to {args.nx}^2")
+    line = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": K, "warmup": W,
+            "ms_per_step": 1000.0 * total_sample * scale / (2 * K), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.nx}x{args.nx} k={args.k} rotated simple wave, BE CFL5, GMRES(20), exact "
+                                   f"block-Jacobi, ntol=ltol={args.ltol:g}; DG and HDG FP64 (the reference has no "
+                                   f"mixed precision)"},
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample,
+                             "per_method": per},
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1065 @@
+// C ABI of the B200 DG / condensed-HDG Euler solver: context, memory pools, kernel launches,
+// the block-Jacobi preconditioners and the device-resident GMRES(m).
+#include "dgh_gpu.h"
+#include "dgh_kernels_dg.cuh"
+#include "dgh_kernels_hdg.cuh"
+#include "dgh_kernels_init.cuh"
+#include "dgh_kernels_krylov.cuh"
+#include "dgh_kernels_lu.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace dgh;
+
+namespace {
+struct Failure {
+    int code;
+    std::string message;
+};
+[[noreturn]] void fail(int code, const std::string &m) { throw Failure{code, m}; }
+void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) fail(DGH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Gauss-Legendre rule by Newton's method on P_n in extended precision (ascending nodes).
+void gauss_rule(int n, std::vector<double> &x, std::vector<double> &w) {
+    x.assign(n, 0.);
+    w.assign(n, 0.);
+    const double pi = std::acos(-1.);
+    for (int k = 0; k < (n + 1) / 2; ++k) {
+        long double z = std::cos(pi * (k + .75) / (n + .5)), p0 = 1, p1 = z, dp = 1;
+        auto eval = [&]() {
+            p0 = 1;
+            p1 = z;
+            for (int j = 2; j <= n; ++j) {
+                long double p2 = ((2 * j - 1) * z * p1 - (j - 1) * p0) / j;
+                p0 = p1;
+                p1 = p2;
+            }
+            if (n == 1) { p1 = z; p0 = 1; }
+            dp = n * (z * p1 - p0) / (z * z - 1);
+        };
+        for (int it = 0; it < 100; ++it) {
+            eval();
+            long double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs((double)dz) <= 1e-19) break;
+        }
+        eval();
+        x[n - 1 - k] = (double)z;
+        x[k] = -(double)z;
+        w[k] = w[n - 1 - k] = (double)(2 / ((1 - z * z) * dp * dp));
+    }
+    if (n % 2) x[n / 2] = 0;
+}
+std::vector<double> lagrange(const std::vector<double> &x, double z) {
+    const int n = (int)x.size();
+    std::vector<double> v(n, 1.);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            if (i != j) v[i] *= (z - x[j]) / (x[i] - x[j]);
+    return v;
+}
+constexpr int RED_BLOCKS_PER_SM = 4;
+}  // namespace
+
+struct dgh_ctx {
+    dgh_config cfg{};
+    int n = 0, P = 0, m = 0, cells = 0, faces = 0, fw = 0, t = 0, restart = 0;
+    long long N = 0, NT = 0;
+    Grid g{};
+    Basis1D basis{};
+    Case cs{};
+    double step_size = 0, inv_step = 0;
+    int sms = 148, red_grid = 592;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    size_t bytes = 0;
+    std::vector<void *> owned;
+    std::vector<double> xnodes;
+    // device buffers
+    ErrorRule *rule = nullptr;
+    double *old = nullptr, *inv_mass = nullptr, *mass = nullptr, *inv_trace_mass = nullptr;
+    double *speeds = nullptr, *traces = nullptr, *traces2 = nullptr, *partial = nullptr, *red = nullptr;
+    double *vol = nullptr, *fcache = nullptr;
+    int *status = nullptr, *ok = nullptr;
+    double *pinned = nullptr;  // host pinned scratch for scalar read-back
+    bool frozen = false, linearised = false, dg_factored = false, condensed = false, face_factored = false;
+    // DG block Jacobi pool (precision per cfg.precision)
+    void *dg_pool = nullptr;
+    int *dg_perm = nullptr;
+    // HDG condensation
+    double *S = nullptr, *X = nullptr, *Y = nullptr, *cy = nullptr, *hrhs = nullptr;
+    double *aug = nullptr;
+    int *aug_perm = nullptr;
+    int aug_cells = 0;
+    void *face_pool = nullptr;
+    int *face_perm = nullptr;
+    // GMRES
+    double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[2] = {nullptr, nullptr}, *gcoef = nullptr;
+    long long vld = 0;
+    // optional CUDA-event timers per kernel class (dgh_timing_enable / dgh_timing_read)
+    struct TimerRec { int cat; cudaEvent_t a, b; };
+    bool timing = false;
+    std::vector<TimerRec> pending;
+    std::vector<cudaEvent_t> spare;
+    double t_ms[DGH_TIMER_COUNT] = {};
+    int64_t t_n[DGH_TIMER_COUNT] = {};
+    cudaEvent_t event() {
+        if (spare.empty()) {
+            cudaEvent_t e;
+            ck(cudaEventCreate(&e), "cudaEventCreate");
+            return e;
+        }
+        cudaEvent_t e = spare.back();
+        spare.pop_back();
+        return e;
+    }
+    void flush_timers() {
+        if (pending.empty()) return;
+        ck(cudaStreamSynchronize(stream), "sync");
+        for (auto &r : pending) {
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, r.a, r.b), "cudaEventElapsedTime");
+            t_ms[r.cat] += ms;
+            t_n[r.cat] += 1;
+            spare.push_back(r.a);
+            spare.push_back(r.b);
+        }
+        pending.clear();
+    }
+
+    template <class T> T *alloc(size_t count) {
+        void *p = nullptr;
+        const size_t b = std::max<size_t>(count * sizeof(T), 16);
+        ck(cudaMalloc(&p, b), "cudaMalloc");
+        owned.push_back(p);
+        bytes += b;
+        return static_cast<T *>(p);
+    }
+    void launched(int k = 1) {
+        launches += k;
+        ck(cudaGetLastError(), "kernel launch");
+    }
+    void sync() { ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
+    bool mixed() const { return cfg.precision == DGH_PRECISION_MIXED; }
+    bool has_dg() const { return cfg.method == DGH_METHOD_DG || cfg.method == DGH_METHOD_BOTH; }
+    bool has_hdg() const { return cfg.method == DGH_METHOD_HDG || cfg.method == DGH_METHOD_BOTH; }
+    int team_blocks(int cpb) const { return (cells + cpb - 1) / cpb; }
+    // Deterministic weighted reduction helpers (return host values).
+    double reduce_scalar(const double *x, const double *W, bool divide, long long n_) {
+        k_wnorm2<<<red_grid, KR_THREADS, 0, stream>>>(x, W, divide ? 1 : 0, n_, partial);
+        k_reduce<<<1, KR_THREADS, 0, stream>>>(partial, red_grid, red);
+        launched(2);
+        ck(cudaMemcpyAsync(pinned, red, sizeof(double), cudaMemcpyDeviceToHost, stream), "copy");
+        sync();
+        return pinned[0];
+    }
+    void check_status(int mask_clear = 0) {
+        int s = 0;
+        ck(cudaMemcpyAsync(pinned, status, sizeof(int), cudaMemcpyDeviceToHost, stream), "copy status");
+        sync();
+        std::memcpy(&s, pinned, sizeof(int));
+        if (s) {
+            ck(cudaMemsetAsync(status, 0, sizeof(int), stream), "memset");
+            (void)mask_clear;
+            if (s & ST_FROZEN_FACE) fail(DGH_ERR_STATE, "Invalid frozen face state");
+            if (s & ST_CFL_VOLUME) fail(DGH_ERR_STATE, "Invalid CFL volume state");
+            if (s & ST_NONPHYS_MEAN) fail(DGH_ERR_STATE, "Nonphysical cell average");
+            if (s & ST_SHOCK) fail(DGH_ERR_STATE, "Simple wave reaches shock time");
+            if (s & ST_SINGULAR) fail(DGH_ERR_SINGULAR, "Singular block Jacobi factor");
+            if (s & ST_SINGULAR_HDG) fail(DGH_ERR_SINGULAR, "Singular or nonfinite LU factors");
+            fail(DGH_ERR_CUDA, "unknown device status");
+        }
+    }
+};
+
+namespace {
+template <class F> int guard(dgh_ctx *ctx, F &&f) {
+    if (!ctx) return DGH_ERR_INVALID;
+    try {
+        f();
+        return DGH_OK;
+    } catch (const Failure &e) {
+        ctx->err = e.message;
+        return e.code;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return DGH_ERR_CUDA;
+    }
+}
+void need(bool c, const char *m) {
+    if (!c) fail(DGH_ERR_INVALID, m);
+}
+// Records an event pair around a region when timing is enabled.
+struct Timed {
+    dgh_ctx *c;
+    int cat;
+    cudaEvent_t a = nullptr;
+    Timed(dgh_ctx *ctx, int category) : c(ctx), cat(category) {
+        if (c->timing) {
+            a = c->event();
+            ck(cudaEventRecord(a, c->stream), "cudaEventRecord");
+        }
+    }
+    ~Timed() {
+        if (a) {
+            cudaEvent_t b = c->event();
+            cudaEventRecord(b, c->stream);
+            c->pending.push_back({cat, a, b});
+            if (c->pending.size() > 2048) c->flush_timers();
+        }
+    }
+};
+
+#define DGH_DISPATCH_N(nn, ...)               \
+    switch (nn) {                             \
+        case 1: { constexpr int N = 1; __VA_ARGS__; } break; \
+        case 2: { constexpr int N = 2; __VA_ARGS__; } break; \
+        case 3: { constexpr int N = 3; __VA_ARGS__; } break; \
+        case 4: { constexpr int N = 4; __VA_ARGS__; } break; \
+        case 5: { constexpr int N = 5; __VA_ARGS__; } break; \
+        case 6: { constexpr int N = 6; __VA_ARGS__; } break; \
+        case 7: { constexpr int N = 7; __VA_ARGS__; } break; \
+        case 8: { constexpr int N = 8; __VA_ARGS__; } break; \
+        case 9: { constexpr int N = 9; __VA_ARGS__; } break; \
+        default: fail(DGH_ERR_INVALID, "Unsupported face degree"); \
+    }
+
+// ---- launch helpers ---------------------------------------------------------------------------
+void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
+    DGH_DISPATCH_N(c->n, {
+        using T = Team<N>;
+        if (check) k_face_trace<N, true><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, tr, c->basis, c->g, c->ok);
+        else k_face_trace<N, false><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, tr, c->basis, c->g, c->ok);
+    });
+    c->launched();
+}
+
+constexpr int LU_NB = 32, LU_TC = 64;
+template <typename TF> void setup_lu_attrs(size_t smem) {
+    ck(cudaFuncSetAttribute(k_lu<TF, LU_NB, LU_TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "lu attr");
+}
+template <typename TF>
+void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, int bit) {
+    const size_t smem = lu_smem_bytes<TF, LU_NB, LU_TC>(m);
+    setup_lu_attrs<TF>(smem);
+    const int per_sm = std::max(1, (int)((220u * 1024u) / smem));
+    const int grid = std::min(count, c->sms * per_sm);
+    k_lu<TF, LU_NB, LU_TC><<<grid, LU_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, perm, c->status, bit);
+    c->launched();
+}
+template <typename TF>
+void launch_solve(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
+                  double *z) {
+    const size_t smem = sizeof(TF) * m;
+    const int grid = std::min(count, c->sms * 8);
+    k_lu_solve<TF><<<grid, LU_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
+    c->launched();
+}
+
+void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
+    Timed tm(c, DGH_TIMER_PRECOND);
+    if (op == DGH_OP_DG) {
+        need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
+        const size_t stride = (size_t)c->m * c->m;
+        if (c->mixed()) launch_solve<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+        else launch_solve<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+    } else {
+        need(c->face_factored, "Refresh the block-Jacobi preconditioner before applying it");
+        const size_t stride = (size_t)c->fw * c->fw;
+        if (c->mixed()) launch_solve<float>(c, (const float *)c->face_pool, c->face_perm, stride, c->fw, c->faces, x, z);
+        else launch_solve<double>(c, (const double *)c->face_pool, c->face_perm, stride, c->fw, c->faces, x, z);
+    }
+}
+
+void dg_apply(dgh_ctx *c, const double *v, double *out) {
+    need(c->linearised, "Refresh the volume Jacobian before applying it");
+    launch_trace(c, v, c->traces2, false);
+    DGH_DISPATCH_N(c->n, {
+        using T = Team<N>;
+        k_dg_apply<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(v, c->traces2, c->vol, c->fcache, c->speeds,
+                                                                            out, c->basis, c->g, c->inv_step);
+    });
+    c->launched();
+}
+void hdg_apply(dgh_ctx *c, const double *lam, double *out) {
+    need(c->condensed, "Condense the HDG operator before applying it");
+    DGH_DISPATCH_N(c->n, { k_hdg_apply<N><<<c->faces, 256, 0, c->stream>>>(c->S, c->speeds, lam, out, c->basis, c->g); });
+    c->launched();
+}
+void op_apply(dgh_ctx *c, int op, const double *x, double *y) {
+    Timed tm(c, DGH_TIMER_OPERATOR);
+    if (op == DGH_OP_DG) dg_apply(c, x, y);
+    else hdg_apply(c, x, y);
+}
+
+template <int NV> void mdot_t(dgh_ctx *c, const double *V, size_t ld, int K, const double *x, const double *W, long long n) {
+    k_mdot<NV><<<c->red_grid, KR_THREADS, 0, c->stream>>>(V, ld, K, x, W, n, c->partial);
+}
+template <int NV, int MODE>
+void maxpy_t(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, double *x, const double *W, long long n) {
+    k_maxpy_reduce<NV, MODE><<<c->red_grid, KR_THREADS, 0, c->stream>>>(V, ld, K, h, x, W, n, c->partial);
+}
+template <int NV> void lincomb_t(dgh_ctx *c, const double *V, size_t ld, int K, const double *coef, double *out, long long n) {
+    k_lincomb<NV><<<c->red_grid, KR_THREADS, 0, c->stream>>>(V, ld, K, coef, out, n);
+}
+#define DGH_DISPATCH_K(K, CALL) \
+    do { if ((K) <= 4) { CALL(4); } else if ((K) <= 8) { CALL(8); } else if ((K) <= 16) { CALL(16); } else { CALL(32); } } while (0)
+
+void mdot(dgh_ctx *c, const double *V, size_t ld, int K, const double *x, const double *W, long long n, double *out) {
+#define C_(NV) mdot_t<NV>(c, V, ld, K, x, W, n)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    k_reduce<<<K, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, out);
+    c->launched(2);
+}
+void maxpy_dot(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, double *x, const double *W, long long n,
+               double *out) {
+#define C_(NV) maxpy_t<NV, 0>(c, V, ld, K, h, x, W, n)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    k_reduce<<<K, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, out);
+    c->launched(2);
+}
+void maxpy_norm(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, double *x, const double *W, long long n,
+                double *out) {
+#define C_(NV) maxpy_t<NV, 1>(c, V, ld, K, h, x, W, n)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, out);
+    c->launched(2);
+}
+void lincomb(dgh_ctx *c, const double *V, size_t ld, int K, const double *coef, double *out, long long n) {
+#define C_(NV) lincomb_t<NV>(c, V, ld, K, coef, out, n)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    c->launched();
+}
+void axpby(dgh_ctx *c, double a, const double *x, double b, const double *y, double *out, long long n) {
+    k_axpby<<<c->red_grid, KR_THREADS, 0, c->stream>>>(a, x, b, y, out, n);
+    c->launched();
+}
+
+// gmres.cpp:17-86 with the CGS2 passes fused as dot | axpy+dot | axpy+norm.
+void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
+    const long long n = op == DGH_OP_DG ? c->N : c->NT;
+    const double *W = op == DGH_OP_DG ? c->inv_mass : c->inv_trace_mass;
+    const int restart = (int)std::min<long long>(n, c->cfg.restart);
+    double *r = c->gres[op], *w = c->gw, *z = c->gz, *V = c->V;
+    const size_t ld = (size_t)c->vld;
+    double *h1 = c->red, *h2 = c->red + KR_MAXK, *nrm = c->red + 2 * KR_MAXK;
+    std::vector<double> H((size_t)(restart + 1) * restart), cs(restart), sn(restart), g(restart + 1), y(restart);
+    auto Hc = [&](int i, int j) -> double & { return H[(size_t)j * (restart + 1) + i]; };
+    ck(cudaMemsetAsync(x, 0, n * sizeof(double), c->stream), "memset");
+    ck(cudaMemcpyAsync(r, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(rhs, W, false, n)));
+    iters = 0;
+    rel = 0;
+    if (rhs_norm == 0) return;
+    while (iters < limit) {
+        // beta = ||r||; V0 = r / beta
+        k_wnorm2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(r, W, 0, n, c->partial);
+        k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, nrm);
+        k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(r, nrm, 1, V, n);
+        c->launched(3);
+        ck(cudaMemcpyAsync(c->pinned, nrm, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        const double beta = std::sqrt(std::max(0.0, c->pinned[0]));
+        if (beta <= tol * rhs_norm) {
+            rel = beta / rhs_norm;
+            return;
+        }
+        std::fill(H.begin(), H.end(), 0.);
+        std::fill(g.begin(), g.end(), 0.);
+        g[0] = beta;
+        int count = 0;
+        for (int j = 0; j < restart && iters < limit; ++j) {
+            precond_apply(c, op, V + (size_t)j * ld, z);
+            op_apply(c, op, z, w);
+            {
+                Timed tm(c, DGH_TIMER_ARNOLDI);
+                mdot(c, V, ld, j + 1, w, W, n, h1);
+                maxpy_dot(c, V, ld, j + 1, h1, w, W, n, h2);
+                maxpy_norm(c, V, ld, j + 1, h2, w, W, n, nrm);
+                k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(w, nrm, 1, V + (size_t)(j + 1) * ld, n);
+                c->launched();
+            }
+            ck(cudaMemcpyAsync(c->pinned, c->red, (2 * KR_MAXK + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+               "copy");
+            c->sync();
+            const double *hh1 = c->pinned, *hh2 = c->pinned + KR_MAXK;
+            for (int i = 0; i <= j; ++i) Hc(i, j) = (0. + hh1[i]) + hh2[i];
+            const double next = std::sqrt(std::max(0.0, c->pinned[2 * KR_MAXK]));
+            Hc(j + 1, j) = next;
+            for (int i = 0; i < j; ++i) {
+                const double a = Hc(i, j), b = Hc(i + 1, j);
+                Hc(i, j) = cs[i] * a + sn[i] * b;
+                Hc(i + 1, j) = -sn[i] * a + cs[i] * b;
+            }
+            const double d = std::hypot(Hc(j, j), Hc(j + 1, j));
+            if (!(std::isfinite(d) && d > 0)) fail(DGH_ERR_BREAKDOWN, "GMRES Arnoldi breakdown");
+            cs[j] = Hc(j, j) / d;
+            sn[j] = Hc(j + 1, j) / d;
+            Hc(j, j) = d;
+            Hc(j + 1, j) = 0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] *= cs[j];
+            ++iters;
+            count = j + 1;
+            if (std::abs(g[j + 1]) <= tol * rhs_norm || next <= std::numeric_limits<double>::min()) break;
+        }
+        for (int i = count - 1; i >= 0; --i) {
+            double value = g[i];
+            for (int j = i + 1; j < count; ++j) value -= Hc(i, j) * y[j];
+            y[i] = value / Hc(i, i);
+        }
+        std::memcpy(c->pinned, y.data(), count * sizeof(double));
+        ck(cudaMemcpyAsync(c->gcoef, c->pinned, count * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+        lincomb(c, V, ld, count, c->gcoef, w, n);
+        precond_apply(c, op, w, z);
+        axpby(c, 1., x, 1., z, x, n);
+        op_apply(c, op, x, w);
+        axpby(c, 1., rhs, -1., w, r, n);
+        const double rn = std::sqrt(std::max(0.0, c->reduce_scalar(r, W, false, n)));
+        rel = rn / rhs_norm;
+        if (!std::isfinite(rel)) fail(DGH_ERR_NONFINITE, "Nonfinite GMRES residual");
+        if (rel <= tol) return;
+    }
+    fail(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+}
+
+void build_rule(dgh_ctx *c) {
+    ErrorRule h{};
+    std::vector<double> ex, ew;
+    const int Q = std::max(20, 2 * c->n + 3);
+    gauss_rule(Q, ex, ew);
+    h.Q = Q;
+    for (int q = 0; q < Q; ++q) {
+        h.ex[q] = ex[q];
+        h.ew[q] = ew[q];
+        auto v = lagrange(c->xnodes, ex[q]);
+        for (int i = 0; i < c->n; ++i) h.ev[q * c->n + i] = v[i];
+    }
+    for (int i = 0; i < c->n; ++i)
+        for (int q = 0; q < Q; ++q) h.proj[i * Q + q] = h.ev[q * c->n + i] * ew[q] / c->basis.w[i];
+    c->rule = c->alloc<ErrorRule>(1);
+    ck(cudaMemcpy(c->rule, &h, sizeof(h), cudaMemcpyHostToDevice), "upload rule");
+}
+
+__global__ void k_fill_mass(double *mass, double *inv_mass, Basis1D b, Grid g, int n, long long N) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int P = n * n, node = (int)(i % P), ix = node % n, iy = node / n;
+    const double m = .25 * g.hx * g.hy * b.w[ix] * b.w[iy];
+    mass[i] = m;
+    inv_mass[i] = 1 / m;
+}
+__global__ void k_fill_trace_mass(double *inv_tm, Basis1D b, Grid g, int n, long long NT) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NT) return;
+    const int fw = 4 * n, face = (int)(i / fw), q = (int)(i % fw) % n;
+    inv_tm[i] = 1 / face_weight(g, b, face, q);
+}
+}  // namespace
+
+// ============================================================================ C ABI
+extern "C" {
+
+void dgh_config_default(dgh_config *c) {
+    std::memset(c, 0, sizeof(*c));
+    c->nx = 8; c->ny = 8; c->degree = 3; c->quadrature = 0;
+    c->restart = 30; c->max_linear = 1500; c->max_newton = 30; c->steps = 0;
+    c->newton_steps = 0; c->warmup_updates = 0;
+    c->cfl = 2.; c->final_time = .2; c->safety = 1.1;
+    c->nonlinear_tolerance = 1e-12; c->linear_tolerance = 1e-12;
+    c->method = DGH_METHOD_BOTH; c->integrator = DGH_INTEGRATOR_DIRK3; c->testcase = DGH_TEST_DIAGONAL;
+    c->precision = DGH_PRECISION_FP64; c->check_update = 0; c->device = 0;
+}
+
+static thread_local std::string g_create_error;
+
+int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
+    if (!cfg || !out) return DGH_ERR_INVALID;
+    *out = nullptr;
+    dgh_ctx *c = new dgh_ctx;
+    c->cfg = *cfg;
+    const int rc = guard(c, [&] {
+        const dgh_config &k = *cfg;
+        // config.cpp:6-22
+        need(k.nx >= 3 && k.ny >= 3 && k.degree >= 0 && k.degree <= 8 && k.quadrature >= 0, "Invalid mesh or degree");
+        need(k.quadrature == 0 || k.quadrature >= k.degree + 1, "Quadrature must be >= degree+1");
+        need(k.quadrature == 0 || k.quadrature == k.degree + 1, "Over-integration (--quad > k+1) is not supported");
+        need(k.restart > 0 && k.max_linear > 0 && k.max_newton > 0 && k.steps >= 0, "Invalid iteration limit");
+        need(k.newton_steps >= 0 && k.warmup_updates >= 0, "Invalid timing update count");
+        need(std::isfinite(k.cfl) && k.cfl > 0 && std::isfinite(k.final_time) && k.final_time >= 0,
+             "CFL must be positive and final time nonnegative");
+        need(std::isfinite(k.safety) && k.safety >= 1 && std::isfinite(k.nonlinear_tolerance) &&
+                 k.nonlinear_tolerance > 0 && std::isfinite(k.linear_tolerance) && k.linear_tolerance > 0 &&
+                 k.linear_tolerance < 1,
+             "Invalid solver tolerance or wave-speed safety");
+        need(k.method >= 0 && k.method <= 2, "Method must be dg, hdg, or both");
+        need(k.testcase >= 0 && k.testcase <= 2, "Invalid testcase");
+        need(k.precision == 0 || k.precision == 1, "Invalid precision");
+        need(k.restart <= KR_MAXK - 1, "restart must be at most 31 on the device GMRES");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(DGH_ERR_CUDA, "no CUDA device available");
+        ck(cudaSetDevice(k.device), "cudaSetDevice");
+        cudaDeviceProp prop{};
+        ck(cudaGetDeviceProperties(&prop, k.device), "cudaGetDeviceProperties");
+        if (prop.major < 10) fail(DGH_ERR_CUDA, "this library is built for sm_100a (B200) only");
+        c->sms = prop.multiProcessorCount;
+        c->red_grid = c->sms * RED_BLOCKS_PER_SM;
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaMallocHost((void **)&c->pinned, 4096), "cudaMallocHost");
+
+        c->n = k.degree + 1;
+        c->P = c->n * c->n;
+        c->m = NVAR * c->P;
+        c->cells = k.nx * k.ny;
+        c->faces = 2 * c->cells;
+        c->fw = NVAR * c->n;
+        c->t = NFACES * c->fw;
+        c->N = (long long)c->cells * c->m;
+        c->NT = (long long)c->faces * c->fw;
+        // example.hpp:9-14
+        const double pi = std::acos(-1.);
+        c->cs.kind = k.testcase == DGH_TEST_DIAGONAL ? 0 : (k.testcase == DGH_TEST_WAVE ? 1 : 2);
+        c->cs.cosine = std::cos(45. * pi / 180.);
+        c->cs.sine = std::sin(45. * pi / 180.);
+        c->cs.lx = c->cs.kind == 0 ? 2. / c->cs.cosine : 2.;
+        c->cs.ly = c->cs.kind == 0 ? 2. / c->cs.sine : 2.;
+        c->cs.gamma = 3.;
+        c->g.nx = k.nx;
+        c->g.ny = k.ny;
+        c->g.cells = c->cells;
+        c->g.hx = c->cs.lx / k.nx;
+        c->g.hy = c->cs.ly / k.ny;
+        c->g.gamma = 3.;
+        // nodal_basis.hpp:34-65
+        std::vector<double> x, w;
+        gauss_rule(c->n, x, w);
+        c->xnodes = x;
+        const int n = c->n;
+        std::vector<double> bary(n, 1.);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                if (i != j) bary[i] /= x[i] - x[j];
+        std::vector<double> D(n * n, 0.);
+        for (int i = 0; i < n; ++i) {
+            double s = 0;
+            for (int j = 0; j < n; ++j)
+                if (i != j) {
+                    D[i * n + j] = bary[j] / (bary[i] * (x[i] - x[j]));
+                    s += D[i * n + j];
+                }
+            D[i * n + i] = -s;
+        }
+        auto eL = lagrange(x, -1.), eR = lagrange(x, 1.);
+        for (int i = 0; i < n; ++i) {
+            c->basis.w[i] = w[i];
+            c->basis.eL[i] = eL[i];
+            c->basis.eR[i] = eR[i];
+        }
+        for (int q = 0; q < n; ++q)
+            for (int i = 0; i < n; ++i) c->basis.dw[q * n + i] = w[q] * D[q * n + i];
+
+        // ---- pools (sized once; nothing else allocates on the hot path)
+        c->old = c->alloc<double>(c->N);
+        c->mass = c->alloc<double>(c->N);
+        c->inv_mass = c->alloc<double>(c->N);
+        c->inv_trace_mass = c->alloc<double>(c->NT);
+        c->speeds = c->alloc<double>(2 * (size_t)c->faces * n);
+        c->traces = c->alloc<double>((size_t)c->cells * NFACES * n * NVAR);
+        c->traces2 = c->alloc<double>((size_t)c->cells * NFACES * n * NVAR);
+        c->partial = c->alloc<double>((size_t)std::max<long long>(KR_MAXK * c->red_grid, 4LL * c->cells + 64));
+        c->red = c->alloc<double>(4 * KR_MAXK);
+        c->vol = c->alloc<double>((size_t)c->cells * c->P * 3);
+        c->fcache = c->alloc<double>((size_t)c->faces * n * 8);
+        c->status = c->alloc<int>(1);
+        c->ok = c->alloc<int>(1);
+        ck(cudaMemset(c->status, 0, sizeof(int)), "memset");
+        build_rule(c);
+        const int tb = 256;
+        k_fill_mass<<<(unsigned)((c->N + tb - 1) / tb), tb, 0, c->stream>>>(c->mass, c->inv_mass, c->basis, c->g, n, c->N);
+        k_fill_trace_mass<<<(unsigned)((c->NT + tb - 1) / tb), tb, 0, c->stream>>>(c->inv_trace_mass, c->basis, c->g, n, c->NT);
+        c->launched(2);
+        const size_t tsz = c->mixed() ? sizeof(float) : sizeof(double);
+        if (c->has_dg()) {
+            c->dg_pool = c->alloc<char>((size_t)c->cells * c->m * c->m * tsz);
+            c->dg_perm = c->alloc<int>((size_t)c->cells * c->m);
+        }
+        if (c->has_hdg()) {
+            c->S = c->alloc<double>((size_t)c->cells * c->t * c->t);
+            c->X = c->alloc<double>((size_t)c->cells * c->m * c->t);
+            c->Y = c->alloc<double>((size_t)c->cells * c->m);
+            c->cy = c->alloc<double>((size_t)c->cells * c->t);
+            c->hrhs = c->alloc<double>(c->NT);
+            const size_t per_cell = (size_t)c->m * (c->m + c->t + 1) * sizeof(double);
+            const size_t budget = (size_t)8 << 30;  // condensation workspace: at most 8 GiB
+            c->aug_cells = (int)std::max<size_t>(1, std::min<size_t>(c->cells, budget / per_cell));
+            c->aug = c->alloc<double>((size_t)c->aug_cells * c->m * (c->m + c->t + 1));
+            c->aug_perm = c->alloc<int>((size_t)c->aug_cells * c->m);
+            c->face_pool = c->alloc<char>((size_t)c->faces * c->fw * c->fw * tsz);
+            c->face_perm = c->alloc<int>((size_t)c->faces * c->fw);
+        }
+        const long long vn = std::max(c->has_dg() ? c->N : 0LL, c->has_hdg() ? c->NT : 0LL);
+        c->vld = ((vn + 31) / 32) * 32;
+        c->restart = k.restart;
+        c->V = c->alloc<double>((size_t)c->vld * (k.restart + 1));
+        c->gw = c->alloc<double>(vn);
+        c->gz = c->alloc<double>(vn);
+        if (c->has_dg()) c->gres[DGH_OP_DG] = c->alloc<double>(c->N);
+        if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
+        c->gcoef = c->alloc<double>(KR_MAXK);
+        c->sync();
+    });
+    if (rc != DGH_OK) {
+        g_create_error = c->err;
+        dgh_ctx_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return DGH_OK;
+}
+
+int dgh_ctx_destroy(dgh_ctx *c) {
+    if (!c) return DGH_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &r : c->pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : c->spare) cudaEventDestroy(e);
+    for (void *p : c->owned) cudaFree(p);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DGH_OK;
+}
+
+const char *dgh_last_error(const dgh_ctx *c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int dgh_sizes(const dgh_ctx *c, int64_t s[8]) {
+    if (!c || !s) return DGH_ERR_INVALID;
+    s[0] = c->N; s[1] = c->NT; s[2] = c->m; s[3] = c->cells; s[4] = c->faces; s[5] = c->n; s[6] = c->t; s[7] = c->fw;
+    return DGH_OK;
+}
+void *dgh_stream(const dgh_ctx *c) { return c ? (void *)c->stream : nullptr; }
+int dgh_get_config(const dgh_ctx *c, dgh_config *out) {
+    if (!c || !out) return DGH_ERR_INVALID;
+    *out = c->cfg;
+    return DGH_OK;
+}
+int dgh_geometry(const dgh_ctx *c, double out[4]) {
+    if (!c || !out) return DGH_ERR_INVALID;
+    out[0] = c->g.hx; out[1] = c->g.hy; out[2] = c->cs.lx; out[3] = c->cs.ly;
+    return DGH_OK;
+}
+int dgh_nodes(const dgh_ctx *c, double *x, double *w) {
+    if (!c) return DGH_ERR_INVALID;
+    for (int i = 0; i < c->n; ++i) {
+        if (x) x[i] = c->xnodes[i];
+        if (w) w[i] = c->basis.w[i];
+    }
+    return DGH_OK;
+}
+int dgh_sync(dgh_ctx *c) { return guard(c, [&] { c->sync(); }); }
+int dgh_device_bytes(const dgh_ctx *c, int64_t *b) {
+    if (!c || !b) return DGH_ERR_INVALID;
+    *b = (int64_t)c->bytes;
+    return DGH_OK;
+}
+int64_t dgh_launch_count(const dgh_ctx *c) { return c ? c->launches : 0; }
+int dgh_timing_enable(dgh_ctx *c, int on) {
+    return guard(c, [&] {
+        c->flush_timers();
+        for (int k = 0; k < DGH_TIMER_COUNT; ++k) {
+            c->t_ms[k] = 0;
+            c->t_n[k] = 0;
+        }
+        c->timing = on != 0;
+    });
+}
+int dgh_timing_read(dgh_ctx *c, int category, double *ms, int64_t *count) {
+    return guard(c, [&] {
+        need(category >= 0 && category < DGH_TIMER_COUNT, "Invalid timer category");
+        c->flush_timers();
+        if (ms) *ms = c->t_ms[category];
+        if (count) *count = c->t_n[category];
+    });
+}
+
+int dgh_vec_alloc(dgh_ctx *c, int64_t n, double **dev) {
+    return guard(c, [&] {
+        need(dev && n > 0, "Invalid vector size");
+        ck(cudaMalloc((void **)dev, n * sizeof(double)), "cudaMalloc");
+        ck(cudaMemsetAsync(*dev, 0, n * sizeof(double), c->stream), "memset");
+    });
+}
+int dgh_vec_free(dgh_ctx *c, double *dev) {
+    return guard(c, [&] { ck(cudaFree(dev), "cudaFree"); });
+}
+int dgh_upload(dgh_ctx *c, double *dev, const double *host, int64_t n) {
+    return guard(c, [&] { ck(cudaMemcpyAsync(dev, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream), "h2d"); });
+}
+int dgh_download(dgh_ctx *c, double *host, const double *dev, int64_t n) {
+    return guard(c, [&] {
+        ck(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+        c->sync();
+    });
+}
+int dgh_axpby(dgh_ctx *c, double a, const double *x, double b, const double *y, double *out, int64_t n) {
+    return guard(c, [&] { axpby(c, a, x, b, y, out, n); });
+}
+
+// ---- Problem ------------------------------------------------------------------------------------
+int dgh_initial(dgh_ctx *c, double *u) {
+    return guard(c, [&] {
+        need(u, "null state");
+        DGH_DISPATCH_N(c->n, { k_initial<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, c->status); });
+        c->launched();
+        c->check_status();
+        // initial_and_error.cpp:53 — the projected state must be admissible
+        const int one = 1;
+        std::memcpy(c->pinned, &one, sizeof(int));
+        ck(cudaMemcpyAsync(c->ok, c->pinned, sizeof(int), cudaMemcpyHostToDevice, c->stream), "copy");
+        launch_trace(c, u, c->traces, true);
+        ck(cudaMemcpyAsync(c->pinned, c->ok, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        int ok = 0;
+        std::memcpy(&ok, c->pinned, sizeof(int));
+        if (!ok) fail(DGH_ERR_STATE, "Invalid projected initial state");
+    });
+}
+
+int dgh_freeze(dgh_ctx *c, const double *u, double *rate) {
+    return guard(c, [&] {
+        need(u && rate, "null argument");
+        ck(cudaMemcpyAsync(c->old, u, c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+        launch_trace(c, u, c->traces, false);
+        DGH_DISPATCH_N(c->n, {
+            const int tot = 2 * c->cells * N;
+            k_speeds<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, c->g, c->cfg.safety, c->status);
+            using T = Team<N>;
+            k_rate<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->speeds, c->g, c->partial, c->status);
+        });
+        c->launched(2);
+        c->check_status();
+        DGH_DISPATCH_N(c->n, {
+            const int nb = c->team_blocks(Team<N>::CPB);
+            std::vector<double> part(nb);
+            ck(cudaMemcpyAsync(part.data(), c->partial, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+            c->sync();
+            double r = 0;
+            for (double p : part) r = std::max(r, p);
+            *rate = r;
+        });
+        c->frozen = true;
+        c->linearised = c->dg_factored = c->condensed = c->face_factored = false;
+    });
+}
+
+int dgh_set_stage(dgh_ctx *c, const double *old, double step) {
+    return guard(c, [&] {
+        need(old, "null argument");
+        if (old != c->old)
+            ck(cudaMemcpyAsync(c->old, old, c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+        c->step_size = step;
+        c->inv_step = 1. / step;
+        c->linearised = c->dg_factored = c->condensed = c->face_factored = false;
+    });
+}
+
+int dgh_residual(dgh_ctx *c, const double *u, double *r) {
+    return guard(c, [&] {
+        need(u && r, "null argument");
+        need(c->frozen, "Freeze the wave speeds before evaluating the residual");
+        Timed tm(c, DGH_TIMER_RESIDUAL);
+        launch_trace(c, u, c->traces, false);
+        DGH_DISPATCH_N(c->n, {
+            using T = Team<N>;
+            k_residual<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->old, c->traces, c->speeds, r,
+                                                                               c->basis, c->g, 1. / c->step_size);
+        });
+        c->launched();
+    });
+}
+
+int dgh_admissible(dgh_ctx *c, const double *u, int *okp) {
+    return guard(c, [&] {
+        need(u && okp, "null argument");
+        const int one = 1;
+        std::memcpy(c->pinned, &one, sizeof(int));
+        ck(cudaMemcpyAsync(c->ok, c->pinned, sizeof(int), cudaMemcpyHostToDevice, c->stream), "copy");
+        launch_trace(c, u, c->traces, true);
+        ck(cudaMemcpyAsync(c->pinned, c->ok, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        std::memcpy(okp, c->pinned, sizeof(int));
+    });
+}
+
+int dgh_trace(dgh_ctx *c, const double *u, double *lam) {
+    return guard(c, [&] {
+        need(c->frozen, "Freeze the wave speeds first");
+        launch_trace(c, u, c->traces, false);
+        DGH_DISPATCH_N(c->n, {
+            const int tot = 2 * c->cells * N;
+            k_trace_lambda<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, lam, c->g);
+        });
+        c->launched();
+    });
+}
+
+int dgh_dual_norm(dgh_ctx *c, const double *r, double *out) {
+    return guard(c, [&] { *out = std::sqrt(c->reduce_scalar(r, c->mass, true, c->N)); });
+}
+int dgh_state_norm(dgh_ctx *c, const double *u, double *out) {
+    return guard(c, [&] { *out = std::sqrt(c->reduce_scalar(u, c->mass, false, c->N)); });
+}
+
+int dgh_integral(dgh_ctx *c, const double *u, double out[4]) {
+    return guard(c, [&] {
+        DGH_DISPATCH_N(c->n, {
+            const int tot = c->cells * NVAR;
+            k_integral<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(u, c->basis, c->g, c->partial);
+        });
+        c->launched();
+        std::vector<double> part((size_t)c->cells * 4);
+        ck(cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        for (int v = 0; v < 4; ++v) out[v] = 0;
+        for (int cell = 0; cell < c->cells; ++cell)
+            for (int v = 0; v < 4; ++v) out[v] += part[(size_t)cell * 4 + v];
+    });
+}
+
+int dgh_l2_error(dgh_ctx *c, const double *u, double time, double out[4]) {
+    return guard(c, [&] {
+        DGH_DISPATCH_N(c->n, {
+            k_l2_error<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, time, c->partial, c->status);
+        });
+        c->launched();
+        c->check_status();
+        std::vector<double> part((size_t)c->cells * 4);
+        ck(cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        for (int v = 0; v < 4; ++v) out[v] = 0;
+        for (int cell = 0; cell < c->cells; ++cell)
+            for (int v = 0; v < 4; ++v) out[v] += part[(size_t)cell * 4 + v];
+        for (int v = 0; v < 4; ++v) out[v] = std::sqrt(out[v]);
+    });
+}
+
+int dgh_speeds(dgh_ctx *c, double *host_ab) {
+    return guard(c, [&] {
+        ck(cudaMemcpyAsync(host_ab, c->speeds, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream), "copy");
+        c->sync();
+    });
+}
+
+// ---- DGOperator --------------------------------------------------------------------------------
+namespace {
+void linearise(dgh_ctx *c, const double *u) {
+    need(c->frozen, "Freeze the wave speeds before refreshing the Jacobian");
+    need(c->step_size > 0, "Set the time step before refreshing the Jacobian");
+    launch_trace(c, u, c->traces, false);
+    DGH_DISPATCH_N(c->n, {
+        const long long tv = (long long)c->cells * N * N;
+        k_volume_cache<N><<<(unsigned)((tv + 255) / 256), 256, 0, c->stream>>>(u, c->vol, c->g);
+        const int tf = 2 * c->cells * N;
+        k_face_cache<N><<<(tf + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, c->fcache, c->basis, c->g);
+    });
+    c->launched(2);
+    c->linearised = true;
+    c->dg_factored = c->condensed = c->face_factored = false;
+}
+}  // namespace
+
+int dgh_dg_refresh(dgh_ctx *c, const double *u) {
+    return guard(c, [&] { linearise(c, u); });
+}
+int dgh_dg_apply(dgh_ctx *c, const double *v, double *jv) {
+    return guard(c, [&] { dg_apply(c, v, jv); });
+}
+int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
+    return guard(c, [&] {
+        need(c->linearised, "Refresh the volume Jacobian before assembling a block");
+        need(row == col && row >= 0 && row < c->cells, "Only diagonal cell blocks are exposed on the device");
+        double *tmp = c->alloc<double>((size_t)c->m * c->m);
+        DGH_DISPATCH_N(c->n, {
+            k_dg_assemble<N, double><<<1, 256, 0, c->stream>>>(tmp, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step,
+                                                                row, 1);
+        });
+        c->launched();
+        ck(cudaMemcpyAsync(host_block, tmp, (size_t)c->m * c->m * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        ck(cudaFree(tmp), "cudaFree");
+        c->owned.pop_back();
+        c->bytes -= std::max<size_t>((size_t)c->m * c->m * sizeof(double), 16);
+    });
+}
+
+// ---- BlockJacobi -------------------------------------------------------------------------------
+int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
+    return guard(c, [&] {
+        Timed tm(c, op == DGH_OP_DG ? DGH_TIMER_FACTOR : DGH_TIMER_FACE_FACTOR);
+        if (op == DGH_OP_DG) {
+            need(c->dg_pool, "context has no DG operator");
+            need(c->linearised, "Refresh the volume Jacobian before assembling a block");
+            const size_t stride = (size_t)c->m * c->m;
+            const int grid = std::min(c->cells, c->sms * 8);
+            if (c->mixed()) {
+                DGH_DISPATCH_N(c->n, {
+                    k_dg_assemble<N, float><<<grid, 256, 0, c->stream>>>((float *)c->dg_pool, c->vol, c->fcache, c->speeds,
+                                                                         c->basis, c->g, c->inv_step, 0, c->cells);
+                });
+                c->launched();
+                launch_lu<float>(c, (float *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR);
+            } else {
+                DGH_DISPATCH_N(c->n, {
+                    k_dg_assemble<N, double><<<grid, 256, 0, c->stream>>>((double *)c->dg_pool, c->vol, c->fcache, c->speeds,
+                                                                          c->basis, c->g, c->inv_step, 0, c->cells);
+                });
+                c->launched();
+                launch_lu<double>(c, (double *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR);
+            }
+            c->check_status();
+            c->dg_factored = true;
+        } else {
+            need(c->face_pool, "context has no HDG operator");
+            need(c->condensed, "Condense the HDG operator before refreshing its preconditioner");
+            const long long tot = (long long)c->faces * c->fw * c->fw;
+            const size_t stride = (size_t)c->fw * c->fw;
+            if (c->mixed()) {
+                DGH_DISPATCH_N(c->n, {
+                    k_face_blocks<N, float><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (float *)c->face_pool,
+                                                                                                 c->basis, c->g);
+                });
+                c->launched();
+                launch_lu<float>(c, (float *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR);
+            } else {
+                DGH_DISPATCH_N(c->n, {
+                    k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (double *)c->face_pool,
+                                                                                                  c->basis, c->g);
+                });
+                c->launched();
+                launch_lu<double>(c, (double *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR);
+            }
+            c->check_status();
+            c->face_factored = true;
+        }
+    });
+}
+int dgh_precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
+    return guard(c, [&] { precond_apply(c, op, x, z); });
+}
+
+// ---- HybridOperator ------------------------------------------------------------------------------
+int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
+    return guard(c, [&] {
+        need(c->S, "context has no HDG operator");
+        Timed tm(c, DGH_TIMER_CONDENSE);
+        linearise(c, u);
+        const int ld = c->m + c->t + 1;
+        for (int first = 0; first < c->cells; first += c->aug_cells) {
+            const int count = std::min(c->aug_cells, c->cells - first);
+            const int grid = std::min(count, c->sms * 8);
+            DGH_DISPATCH_N(c->n, {
+                k_hdg_assemble<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->vol, c->fcache, c->speeds, r, c->basis, c->g,
+                                                                       c->inv_step, first, count);
+            });
+            c->launched();
+            launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG);
+            k_backsolve<double><<<std::min(count, c->sms * 2), LU_THREADS, 0, c->stream>>>(c->aug, (size_t)c->m * ld, c->m, ld, count);
+            c->launched();
+            DGH_DISPATCH_N(c->n, {
+                k_hdg_schur<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y, c->cy, c->basis,
+                                                                    c->g, first, count);
+            });
+            c->launched();
+        }
+        DGH_DISPATCH_N(c->n, {
+            const long long tot = c->NT;
+            k_hdg_rhs<N><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->cy, c->hrhs, c->g);
+        });
+        c->launched();
+        c->check_status();
+        c->condensed = true;
+    });
+}
+int dgh_hdg_rhs(dgh_ctx *c, double *rhs) {
+    return guard(c, [&] {
+        need(c->condensed, "Condense the HDG operator first");
+        ck(cudaMemcpyAsync(rhs, c->hrhs, c->NT * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    });
+}
+int dgh_hdg_apply(dgh_ctx *c, const double *lam, double *out) {
+    return guard(c, [&] { hdg_apply(c, lam, out); });
+}
+int dgh_hdg_block(dgh_ctx *c, int row, int col, double *host_block) {
+    return guard(c, [&] {
+        need(c->condensed, "Condense the HDG operator first");
+        need(row == col && row >= 0 && row < c->faces, "Only diagonal face blocks are exposed on the device");
+        const long long tot = (long long)c->faces * c->fw * c->fw;
+        double *tmp = c->alloc<double>(tot);
+        DGH_DISPATCH_N(c->n, {
+            k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, tmp, c->basis, c->g);
+        });
+        c->launched();
+        ck(cudaMemcpyAsync(host_block, tmp + (size_t)row * c->fw * c->fw, (size_t)c->fw * c->fw * sizeof(double),
+                           cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        ck(cudaFree(tmp), "cudaFree");
+        c->owned.pop_back();
+        c->bytes -= std::max<size_t>(tot * sizeof(double), 16);
+    });
+}
+int dgh_hdg_recover(dgh_ctx *c, const double *dl, double *du) {
+    return guard(c, [&] {
+        need(c->condensed, "Condense the HDG operator first");
+        DGH_DISPATCH_N(c->n, { k_hdg_recover<N><<<c->cells, 256, 0, c->stream>>>(c->X, c->Y, dl, du, c->g); });
+        c->launched();
+    });
+}
+int dgh_hdg_recovered_residual(dgh_ctx *c, const double *e, double *out) {
+    return guard(c, [&] {
+        need(c->condensed, "Condense the HDG operator first");
+        DGH_DISPATCH_N(c->n, {
+            const long long tot = (long long)c->cells * N * N;
+            k_hdg_recovered_residual<N><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(e, c->speeds, out, c->basis, c->g);
+        });
+        c->launched();
+    });
+}
+
+// ---- GMRES -------------------------------------------------------------------------------------------
+int dgh_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int *iterations, double *relative) {
+    return guard(c, [&] {
+        need(op == DGH_OP_DG ? c->has_dg() : c->has_hdg(), "context lacks the requested operator");
+        int it = 0;
+        double rel = 0;
+        try {
+            gmres(c, op, rhs, x, limit, tol, it, rel);
+        } catch (...) {
+            if (iterations) *iterations = it;
+            throw;
+        }
+        if (iterations) *iterations = it;
+        if (relative) *relative = rel;
+    });
+}
+const double *dgh_gmres_residual(dgh_ctx *c, int op) {
+    if (!c || (op != 0 && op != 1)) return nullptr;
+    return c->gres[op];
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// Device-resident Arnoldi pieces of the restarted, right-preconditioned GMRES(m) with
+// classical Gram-Schmidt applied twice and a weighted inner product (gmres.cpp:17-86).
+// Reductions are deterministic: a fixed grid writes per-block partial sums, and k_reduce adds
+// them in a fixed tree order.  The two CGS2 passes are fused so the basis is swept three times
+// per iteration instead of four: dot | axpy+dot | axpy+norm.
+#pragma once
+#include "dgh_common.cuh"
+
+namespace dgh {
+
+constexpr int KR_THREADS = 256;
+constexpr int KR_MAXK = 32;
+
+template <int NV>
+__device__ inline void block_reduce_store(double (&acc)[NV], int K, double *partial, int G) {
+    __shared__ double red[KR_MAXK][KR_THREADS / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        if (k >= K) break;
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0;
+#pragma unroll
+        for (int w = 0; w < KR_THREADS / 32; ++w) s += red[threadIdx.x][w];
+        partial[(size_t)threadIdx.x * G + blockIdx.x] = s;
+    }
+}
+
+// partial[k*G + blk] = sum_i V_k[i] W[i] x[i], k < K
+template <int NV>
+__global__ void __launch_bounds__(KR_THREADS)
+k_mdot(const double *__restrict__ V, size_t ldv, int K, const double *__restrict__ x,
+       const double *__restrict__ W, long long n, double *__restrict__ partial) {
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0;
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+        const double wx = W[i] * x[i];
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+            if (k < K) acc[k] += V[k * ldv + i] * wx;
+    }
+    block_reduce_store<NV>(acc, K, partial, gridDim.x);
+}
+
+// x -= sum_k V_k h_k, then partial dots of the updated x with every V_k (MODE 0) or the
+// weighted squared norm of the updated x (MODE 1).
+template <int NV, int MODE>
+__global__ void __launch_bounds__(KR_THREADS)
+k_maxpy_reduce(const double *__restrict__ V, size_t ldv, int K, const double *__restrict__ h,
+               double *__restrict__ x, const double *__restrict__ W, long long n, double *__restrict__ partial) {
+    __shared__ double hs[KR_MAXK];
+    if (threadIdx.x < K) hs[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    double acc[MODE == 0 ? NV : 1];
+#pragma unroll
+    for (int k = 0; k < (MODE == 0 ? NV : 1); ++k) acc[k] = 0;
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+        double v[NV];
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+            if (k < K) {
+                v[k] = V[k * ldv + i];
+                s += v[k] * hs[k];
+            }
+        const double xn = x[i] - s;
+        x[i] = xn;
+        const double wx = W[i] * xn;
+        if (MODE == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+                if (k < K) acc[k] += v[k] * wx;
+        } else {
+            acc[0] += xn * wx;
+        }
+    }
+    block_reduce_store<MODE == 0 ? NV : 1>(acc, MODE == 0 ? K : 1, partial, gridDim.x);
+}
+
+// out[k] = sum_b partial[k*G + b]  (one CTA per k, fixed order)
+__global__ void __launch_bounds__(KR_THREADS) k_reduce(const double *__restrict__ partial, int G, double *__restrict__ out) {
+    __shared__ double red[KR_THREADS / 32];
+    const int k = blockIdx.x;
+    double s = 0;
+    for (int b = threadIdx.x; b < G; b += KR_THREADS) s += partial[(size_t)k * G + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < KR_THREADS / 32; ++w) t += red[w];
+        out[k] = t;
+    }
+}
+
+// out[i] = sum_k V_k[i] c_k
+template <int NV>
+__global__ void __launch_bounds__(KR_THREADS)
+k_lincomb(const double *__restrict__ V, size_t ldv, int K, const double *__restrict__ c, double *__restrict__ out,
+          long long n) {
+    __shared__ double cs[KR_MAXK];
+    if (threadIdx.x < K) cs[threadIdx.x] = c[threadIdx.x];
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+            if (k < K) s += V[k * ldv + i] * cs[k];
+        out[i] = s;
+    }
+}
+
+// out = x / s  when s > 0 (s read on the device: the norm of the preceding reduction)
+__global__ void k_scale_div(const double *__restrict__ x, const double *__restrict__ s2, int sqrt_first,
+                            double *__restrict__ out, long long n) {
+    const double s = sqrt_first ? sqrt(fmax(0., *s2)) : *s2;
+    if (!(s > 0)) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = x[i] / s;
+}
+
+// y = a*x + b*y  (general axpby used for x += z, r = rhs - Ax, trial = state + theta*dir)
+__global__ void k_axpby(double a, const double *__restrict__ x, double b, const double *__restrict__ y,
+                        double *__restrict__ out, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = a * x[i] + b * y[i];
+}
+
+// weighted squared norm partials: sum x^2 * W  (W = inverse mass, mass, or inverse trace mass)
+__global__ void __launch_bounds__(KR_THREADS)
+k_wnorm2(const double *__restrict__ x, const double *__restrict__ W, int divide, long long n,
+         double *__restrict__ partial) {
+    double acc[1] = {0};
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS)
+        acc[0] += divide ? x[i] * x[i] / W[i] : x[i] * x[i] * W[i];
+    block_reduce_store<1>(acc, 1, partial, gridDim.x);
+}
+
+}  // namespace dgh

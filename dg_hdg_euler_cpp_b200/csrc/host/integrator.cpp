@@ -1,0 +1,384 @@
+// Host time integrator over the dgh_gpu.h C ABI: SSP-DIRK(4,3) or backward Euler, per-stage
+// freezing, Newton with the residual-acceptance target, the HDG Schur-tolerance retry and the
+// Armijo line search with the admissibility check (time_integrator.cpp:48-213).  Only scalars
+// live on the host; every vector stays in device memory.
+#include "dgh_gpu.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace {
+struct Failure {
+    int code;
+    std::string message;
+};
+}  // namespace
+
+struct dgh_integrator {
+    dgh_ctx *ctx = nullptr;
+    int method = DGH_METHOD_DG;
+    dgh_config cfg{};
+    int64_t N = 0, NT = 0;
+    double lx = 0, ly = 0;
+    std::string err;
+    std::vector<double *> owned;
+    double *state = nullptr, *trial = nullptr, *residual = nullptr, *trial_residual = nullptr, *direction = nullptr;
+    double *rhs = nullptr, *lambda = nullptr, *tdir = nullptr, *eq_err = nullptr, *indep = nullptr;
+    double *step_state = nullptr, *stage_base = nullptr, *slopes[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *solution = nullptr;
+    // current stage
+    double tau = 0, old_norm = 0, initial_rms = -1, step = 0, rate = 0, elapsed_time = 0;
+    int stage = 0, steps_done = 0, stages = 1;
+    bool residual_ready = false;
+    dgh_run_stats run{};
+
+    void ck(int rc) {
+        if (rc != DGH_OK) throw Failure{rc, dgh_last_error(ctx)};
+    }
+    double *vec(int64_t n) {
+        double *p = nullptr;
+        ck(dgh_vec_alloc(ctx, n, &p));
+        owned.push_back(p);
+        return p;
+    }
+    double dual(const double *x) {
+        double v = 0;
+        ck(dgh_dual_norm(ctx, x, &v));
+        return v;
+    }
+    double snorm(const double *x) {
+        double v = 0;
+        ck(dgh_state_norm(ctx, x, &v));
+        return v;
+    }
+    // Residual (when not already available) and its norm at the top of a Newton iteration.
+    double prepare(double &rms) {
+        if (!residual_ready) ck(dgh_residual(ctx, state, residual));
+        const double norm = dual(residual);
+        rms = norm / std::sqrt(lx * ly);
+        if (initial_rms < 0) initial_rms = rms;
+        return norm;
+    }
+    // The body of one Newton iteration after the convergence test (time_integrator.cpp:104-220).
+    void update(double norm, double rms, int it, dgh_update_stats &out) {
+        const auto start = std::chrono::steady_clock::now();
+        (void)start;
+        const double allowance =
+            128 * std::numeric_limits<double>::epsilon() * ((snorm(state) + old_norm) / tau + norm);
+        const double target = std::max(10 * cfg.linear_tolerance * norm, allowance);
+        int iterations = 0;
+        double relative = 0;
+        if (method == DGH_METHOD_DG) {
+            ck(dgh_dg_refresh(ctx, state));
+            ck(dgh_axpby(ctx, -1., residual, 0., residual, rhs, N));
+            ck(dgh_block_jacobi_refresh(ctx, DGH_OP_DG));
+            ck(dgh_gmres(ctx, DGH_OP_DG, rhs, direction, cfg.max_linear, cfg.linear_tolerance, &iterations, &relative));
+            const double *res = dgh_gmres_residual(ctx, DGH_OP_DG);
+            ck(dgh_axpby(ctx, -1., res, 0., res, eq_err, N));
+        } else {
+            ck(dgh_hdg_refresh_projected(ctx, state, residual));
+            ck(dgh_hdg_rhs(ctx, rhs));
+            ck(dgh_block_jacobi_refresh(ctx, DGH_OP_HDG));
+            double tolerance = cfg.linear_tolerance;
+            bool valid = false;
+            for (int attempt = 0; attempt < 4; ++attempt) {
+                int cur = 0;
+                double rel = 0;
+                ck(dgh_gmres(ctx, DGH_OP_HDG, rhs, tdir, cfg.max_linear, tolerance, &cur, &rel));
+                iterations += cur;
+                relative = rel;
+                ck(dgh_hdg_recover(ctx, tdir, direction));
+                const double *res = dgh_gmres_residual(ctx, DGH_OP_HDG);
+                ck(dgh_axpby(ctx, -1., res, 0., res, lambda, NT));
+                ck(dgh_hdg_recovered_residual(ctx, lambda, eq_err));
+                valid = dual(eq_err) <= target;
+                if (valid) break;
+                tolerance *= .01;
+            }
+            if (!valid) throw Failure{DGH_ERR_SOLVER, "Recovered DG residual criterion failed after Schur refinement"};
+        }
+        const double error_norm = dual(eq_err);
+        if (!(error_norm <= target)) throw Failure{DGH_ERR_SOLVER, "DG Newton linear residual too large"};
+        if (method == DGH_METHOD_HDG && cfg.check_update) {
+            // time_integrator.cpp:153-162: an independent DG J*v of the recovered update.  The
+            // condensation linearised the same state, so the DG caches are already current.
+            ck(dgh_dg_apply(ctx, direction, indep));
+            ck(dgh_axpby(ctx, 1., indep, 1., residual, indep, N));
+            if (!(dual(indep) <= std::max(4 * target, 1e-12)))
+                throw Failure{DGH_ERR_SOLVER, "Independent recovered DG equation check failed"};
+            ck(dgh_axpby(ctx, 1., indep, -1., eq_err, indep, N));
+            if (!(dual(indep) <= std::max(4 * allowance, 1e-12)))
+                throw Failure{DGH_ERR_SOLVER, "Recovered residual identity failed"};
+        }
+        double damping = 1.;
+        bool accepted = false;
+        for (int search = 0; search < 30; ++search) {
+            ck(dgh_axpby(ctx, 1., state, damping, direction, trial, N));
+            int ok = 0;
+            ck(dgh_admissible(ctx, trial, &ok));
+            if (ok) {
+                ck(dgh_residual(ctx, trial, trial_residual));
+                if (dual(trial_residual) <= (1 - 1e-4 * damping) * norm + allowance) {
+                    accepted = true;
+                    break;
+                }
+            }
+            damping *= .5;
+        }
+        if (!accepted) throw Failure{DGH_ERR_SOLVER, "Newton line search failed"};
+        std::swap(state, trial);
+        std::swap(residual, trial_residual);
+        residual_ready = true;
+        out.step = steps_done;
+        out.stage = stage;
+        out.iteration = it;
+        out.krylov_iterations = iterations;
+        out.linear_relative_residual = relative;
+        out.dg_linear_relative_residual = norm > 0 ? error_norm / norm : 0.;
+        out.residual_physical_rms = rms;
+        out.damping = damping;
+    }
+};
+
+namespace {
+constexpr double kAlpha = .24169426078821, kBeta = kAlpha / 4., kEta = .12915286960590;
+constexpr double kA[4][4] = {{kAlpha, 0, 0, 0}, {-kAlpha, kAlpha, 0, 0}, {0, 1 - kAlpha, kAlpha, 0},
+                             {kBeta, kEta, .5 - kBeta - kEta - kAlpha, kAlpha}};
+constexpr double kB[4] = {0, 1. / 6, 1. / 6, 2. / 3}, kC[4] = {kAlpha, 0, 1, .5};
+using Clock = std::chrono::steady_clock;
+double since(Clock::time_point s) { return std::chrono::duration<double>(Clock::now() - s).count(); }
+
+template <class F> int guarded(dgh_integrator *it, F &&f) {
+    if (!it) return DGH_ERR_INVALID;
+    try {
+        f();
+        return DGH_OK;
+    } catch (const Failure &e) {
+        it->err = e.message;
+        return e.code;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char *dgh_integrator_error(const dgh_integrator *it) { return it ? it->err.c_str() : ""; }
+
+int dgh_integrator_create(dgh_ctx *ctx, int method, dgh_integrator **out) {
+    if (!ctx || !out || (method != DGH_METHOD_DG && method != DGH_METHOD_HDG)) return DGH_ERR_INVALID;
+    auto *it = new dgh_integrator;
+    it->ctx = ctx;
+    it->method = method;
+    const int rc = guarded(it, [&] {
+        int64_t s[8];
+        it->ck(dgh_sizes(ctx, s));
+        it->N = s[0];
+        it->NT = s[1];
+        double geo[4];
+        it->ck(dgh_geometry(ctx, geo));
+        it->lx = geo[2];
+        it->ly = geo[3];
+        it->ck(dgh_get_config(ctx, &it->cfg));
+        const int64_t N = it->N, NT = it->NT;
+        it->state = it->vec(N); it->trial = it->vec(N); it->residual = it->vec(N);
+        it->trial_residual = it->vec(N); it->direction = it->vec(N);
+        it->rhs = it->vec(method == DGH_METHOD_DG ? N : NT);
+        it->lambda = it->vec(NT); it->tdir = it->vec(NT);
+        it->eq_err = it->vec(N); it->indep = it->vec(N);
+        it->step_state = it->vec(N); it->stage_base = it->vec(N); it->solution = it->vec(N);
+        for (auto &p : it->slopes) p = it->vec(N);
+    });
+    if (rc != DGH_OK) {
+        dgh_integrator_destroy(it);
+        return rc;
+    }
+    *out = it;
+    return DGH_OK;
+}
+
+int dgh_integrator_destroy(dgh_integrator *it) {
+    if (!it) return DGH_OK;
+    for (double *p : it->owned) dgh_vec_free(it->ctx, p);
+    delete it;
+    return DGH_OK;
+}
+
+double *dgh_integrator_state(dgh_integrator *it) { return it ? it->state : nullptr; }
+
+// time_integrator.cpp:48-213 (the full run).  The integrator reads its configuration from the
+// context it was created on.
+int dgh_advance(dgh_integrator *it, double *host_solution, dgh_run_stats *stats, dgh_update_stats *updates,
+                int max_updates) {
+    return guarded(it, [&] {
+        const dgh_config &c = it->cfg;
+        dgh_ctx *ctx = it->ctx;
+        const int64_t N = it->N;
+        it->ck(dgh_upload(ctx, it->solution, host_solution, N));
+        int ok = 0;
+        it->ck(dgh_admissible(ctx, it->solution, &ok));
+        if (!ok) throw Failure{DGH_ERR_STATE, "Invalid initial solution"};
+        const double shock = c.testcase == DGH_TEST_WAVE ? std::numeric_limits<double>::infinity()
+                                                         : 4 / ((3. + 1) * std::acos(-1.));
+        if (!(c.steps > 0 || c.final_time < shock)) throw Failure{DGH_ERR_STATE, "Final time reaches simple-wave shock"};
+        const int stages = c.integrator == DGH_INTEGRATOR_BE ? 1 : 4;
+        it->stages = stages;
+        dgh_run_stats st{};
+        int recorded = 0;
+        double rate0 = 0;
+        it->ck(dgh_freeze(ctx, it->solution, &rate0));
+        double initial_integral[4];
+        it->ck(dgh_integral(ctx, it->solution, initial_integral));
+        const auto begin = Clock::now();
+        it->steps_done = 0;
+        while (c.steps > 0 ? st.steps < c.steps : st.final_time < c.final_time) {
+            double rate = 0;
+            it->ck(dgh_freeze(ctx, it->solution, &rate));
+            double step = c.cfl / rate;
+            if (c.steps == 0) {
+                const double remaining = c.final_time - st.final_time;
+                step = std::min(step, remaining);
+                if (remaining - step <= 16 * std::numeric_limits<double>::epsilon() * std::max(remaining, c.final_time))
+                    step = remaining;
+            }
+            if (!(std::isfinite(step) && step > 0 && st.final_time + step > st.final_time))
+                throw Failure{DGH_ERR_STATE, "Invalid CFL step"};
+            if (!(st.final_time + step < shock)) throw Failure{DGH_ERR_STATE, "Step reaches simple-wave shock"};
+            it->ck(dgh_axpby(ctx, 1., it->solution, 0., it->solution, it->step_state, N));
+            it->ck(dgh_axpby(ctx, 1., it->solution, 0., it->solution, it->state, N));
+            for (int stage = 0; stage < stages; ++stage) {
+                const double diagonal = stages == 1 ? 1. : kA[stage][stage];
+                it->ck(dgh_axpby(ctx, 1., it->step_state, 0., it->step_state, it->stage_base, N));
+                for (int j = 0; j < stage; ++j)
+                    it->ck(dgh_axpby(ctx, 1., it->stage_base, step * kA[stage][j], it->slopes[j], it->stage_base, N));
+                double unused = 0;
+                if (stage > 0) it->ck(dgh_freeze(ctx, it->state, &unused));
+                it->ck(dgh_set_stage(ctx, it->stage_base, diagonal * step));
+                it->tau = diagonal * step;
+                it->old_norm = it->snorm(it->stage_base);
+                it->stage = stage;
+                it->initial_rms = -1.;
+                it->residual_ready = false;
+                const int limit = c.newton_steps > 0 ? c.newton_steps : c.max_newton;
+                bool converged = false;
+                for (int k = 0; k <= limit; ++k) {
+                    const auto t0 = Clock::now();
+                    double rms = 0;
+                    const double norm = it->prepare(rms);
+                    if (c.newton_steps == 0 && rms <= c.nonlinear_tolerance * std::max(1., it->initial_rms)) {
+                        converged = true;
+                        break;
+                    }
+                    if (k == limit) break;
+                    dgh_update_stats u{};
+                    it->steps_done = st.steps;
+                    it->update(norm, rms, k, u);
+                    const double duration = since(t0);
+                    u.iteration_s = duration;
+                    u.time = st.final_time + step;
+                    u.stage_time = st.final_time + (stages == 1 ? 1. : kC[stage]) * step;
+                    u.dt = step;
+                    u.cfl = step * rate;
+                    st.max_linear_residual = std::max(st.max_linear_residual, u.linear_relative_residual);
+                    st.max_dg_linear_residual = std::max(st.max_dg_linear_residual, u.dg_linear_relative_residual);
+                    st.krylov_iterations += u.krylov_iterations;
+                    if (st.newton_iterations >= c.warmup_updates) {
+                        st.measured_newton_seconds += duration;
+                        ++st.measured_updates;
+                    }
+                    ++st.newton_iterations;
+                    if (updates && recorded < max_updates) updates[recorded] = u;
+                    ++recorded;
+                }
+                if (!(converged || c.newton_steps > 0)) throw Failure{DGH_ERR_SOLVER, "Newton iteration limit reached"};
+                it->ck(dgh_axpby(ctx, 1. / it->tau, it->state, -1. / it->tau, it->stage_base, it->slopes[stage], N));
+            }
+            if (stages == 1) {
+                it->ck(dgh_axpby(ctx, 1., it->state, 0., it->state, it->solution, N));
+            } else {
+                it->ck(dgh_axpby(ctx, 1., it->step_state, 0., it->step_state, it->solution, N));
+                for (int s = 0; s < stages; ++s)
+                    it->ck(dgh_axpby(ctx, 1., it->solution, step * kB[s], it->slopes[s], it->solution, N));
+                int ok2 = 0;
+                it->ck(dgh_admissible(ctx, it->solution, &ok2));
+                if (!ok2) throw Failure{DGH_ERR_STATE, "DIRK3 step produced an inadmissible state"};
+            }
+            st.final_time = c.steps == 0 && step >= c.final_time - st.final_time ? c.final_time : st.final_time + step;
+            st.minimum_step = st.steps == 0 ? step : std::min(st.minimum_step, step);
+            st.maximum_step = std::max(st.maximum_step, step);
+            ++st.steps;
+            double now[4];
+            it->ck(dgh_integral(ctx, it->solution, now));
+            double drift = 0;
+            for (int v = 0; v < 4; ++v) drift = std::max(drift, std::abs(now[v] - initial_integral[v]));
+            st.conservation_drift = std::max(st.conservation_drift, drift);
+        }
+        st.seconds = since(begin);
+        st.updates_recorded = recorded;
+        it->ck(dgh_download(ctx, host_solution, it->solution, N));
+        if (stats) *stats = st;
+    });
+}
+
+int dgh_stage_begin(dgh_integrator *it, const double *u, double *dt) {
+    return guarded(it, [&] {
+        dgh_ctx *ctx = it->ctx;
+        const int64_t N = it->N;
+        double rate = 0;
+        it->ck(dgh_freeze(ctx, u, &rate));
+        const double step = it->cfg.cfl / rate;
+        it->ck(dgh_axpby(ctx, 1., u, 0., u, it->state, N));
+        it->ck(dgh_axpby(ctx, 1., u, 0., u, it->stage_base, N));
+        it->ck(dgh_set_stage(ctx, it->stage_base, step));
+        it->tau = step;
+        it->step = step;
+        it->rate = rate;
+        it->old_norm = it->snorm(it->stage_base);
+        it->stage = 0;
+        it->initial_rms = -1.;
+        it->residual_ready = false;
+        if (dt) *dt = step;
+    });
+}
+
+int dgh_newton_update(dgh_integrator *it, dgh_update_stats *stats) {
+    return guarded(it, [&] {
+        const auto t0 = Clock::now();
+        double rms = 0;
+        const double norm = it->prepare(rms);
+        dgh_update_stats u{};
+        it->update(norm, rms, 0, u);
+        it->ck(dgh_sync(it->ctx));
+        u.iteration_s = since(t0);
+        u.dt = it->step;
+        u.time = it->step;
+        u.stage_time = it->step;
+        u.cfl = it->step * it->rate;
+        if (stats) *stats = u;
+    });
+}
+
+int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_stats *stats) {
+    return guarded(it, [&] {
+        const auto t0 = Clock::now();
+        it->ck(dgh_upload(it->ctx, it->state, host_state, it->N));
+        it->residual_ready = false;
+        double rms = 0;
+        const double norm = it->prepare(rms);
+        dgh_update_stats u{};
+        it->update(norm, rms, 0, u);
+        it->ck(dgh_download(it->ctx, host_state, it->state, it->N));
+        u.iteration_s = since(t0);
+        u.dt = it->step;
+        u.time = it->step;
+        u.stage_time = it->step;
+        u.cfl = it->step * it->rate;
+        if (stats) *stats = u;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,296 @@
+"""Python mirror of the reference's solver surface over the C ABI (include/dgh_gpu.h).
+
+`Solver` exposes the calls of the reference's Problem (discretization.hpp:7-45), DGOperator
+(dg_operator.hpp:5-17), BlockJacobi (block_jacobi.hpp:7-47), HybridOperator (hybrid.hpp:6-32)
+and GMRES (gmres.hpp:21-35) with the same names and argument meaning, and `advance` mirrors
+TimeIntegrator::advance (time_integrator.hpp:21-40).  Vectors are torch CUDA tensors (FP64) in
+the reference layout; torch only provides device memory here, every kernel is the library's.
+Errors raise DGHError carrying the reference's require() message.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+METHODS = {"dg": 0, "hdg": 1, "both": 2}
+INTEGRATORS = {"ssp-dirk3": 0, "be": 1}
+TESTCASES = {"diagonal": 0, "wave": 1, "axis": 2}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+OPS = {"dg": 0, "hdg": 1}
+
+
+class DGHError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def make_config(**kw) -> _lib.dgh_config:
+    lib = _lib.load()
+    cfg = _lib.dgh_config()
+    lib.dgh_config_default(ctypes.byref(cfg))
+    aliases = {"k": "degree", "ntol": "nonlinear_tolerance", "ltol": "linear_tolerance", "T": "final_time"}
+    for key, val in kw.items():
+        key = aliases.get(key, key)
+        if key == "method":
+            val = METHODS[val] if isinstance(val, str) else val
+        elif key == "integrator":
+            val = INTEGRATORS[val] if isinstance(val, str) else val
+        elif key == "testcase":
+            val = TESTCASES[val] if isinstance(val, str) else val
+        elif key == "precision":
+            val = PRECISIONS[val] if isinstance(val, str) else val
+        if not hasattr(cfg, key):
+            raise KeyError(key)
+        setattr(cfg, key, val)
+    return cfg
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Solver:
+    """One GPU context: the Problem plus the DG and/or HDG operators of one configuration."""
+
+    def __init__(self, **kw):
+        import torch
+
+        self.torch = torch
+        self.lib = _lib.load()
+        self.cfg = make_config(**kw)
+        h = ctypes.c_void_p()
+        rc = self.lib.dgh_ctx_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_last_error(None).decode())
+        self.h = h
+        s = (ctypes.c_int64 * 8)()
+        self._rc(self.lib.dgh_sizes(self.h, s))
+        self.size, self.trace_size, self.block, self.cells, self.faces, self.n, self.local_trace, self.face_width = (
+            int(x) for x in s)
+        g = (ctypes.c_double * 4)()
+        self._rc(self.lib.dgh_geometry(self.h, g))
+        self.hx, self.hy, self.lx, self.ly = list(g)
+        self.device = torch.device("cuda", self.cfg.device)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dgh_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- plumbing
+    def _rc(self, rc: int):
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_last_error(self.h).decode())
+
+    def _call(self, name, *args):
+        self.torch.cuda.synchronize(self.device)
+        self._rc(getattr(self.lib, name)(self.h, *args))
+        self._rc(self.lib.dgh_sync(self.h))
+
+    def vec(self, n=None):
+        return self.torch.zeros(self.size if n is None else n, dtype=self.torch.float64, device=self.device)
+
+    def tensor(self, a):
+        return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=self.device)
+
+    def stream(self):
+        return self.lib.dgh_stream(self.h)
+
+    def launch_count(self) -> int:
+        return int(self.lib.dgh_launch_count(self.h))
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64()
+        self._rc(self.lib.dgh_device_bytes(self.h, ctypes.byref(b)))
+        return int(b.value)
+
+    # ---- Problem
+    def initial(self):
+        u = self.vec()
+        self._call("dgh_initial", _ptr(u))
+        return u
+
+    def freeze(self, u) -> float:
+        r = ctypes.c_double()
+        self._call("dgh_freeze", _ptr(u), ctypes.byref(r))
+        return r.value
+
+    def set_stage(self, old, step: float):
+        self._call("dgh_set_stage", _ptr(old), ctypes.c_double(step))
+
+    def residual(self, u):
+        r = self.vec()
+        self._call("dgh_residual", _ptr(u), _ptr(r))
+        return r
+
+    def admissible(self, u) -> bool:
+        ok = ctypes.c_int()
+        self._call("dgh_admissible", _ptr(u), ctypes.byref(ok))
+        return bool(ok.value)
+
+    def trace(self, u):
+        lam = self.vec(self.trace_size)
+        self._call("dgh_trace", _ptr(u), _ptr(lam))
+        return lam
+
+    def dual_norm(self, r) -> float:
+        v = ctypes.c_double()
+        self._call("dgh_dual_norm", _ptr(r), ctypes.byref(v))
+        return v.value
+
+    def state_norm(self, u) -> float:
+        v = ctypes.c_double()
+        self._call("dgh_state_norm", _ptr(u), ctypes.byref(v))
+        return v.value
+
+    def residual_rms(self, r) -> float:
+        return self.dual_norm(r) / float(np.sqrt(self.lx * self.ly))
+
+    def integral(self, u) -> np.ndarray:
+        out = (ctypes.c_double * 4)()
+        self._call("dgh_integral", _ptr(u), out)
+        return np.array(out[:])
+
+    def l2_error(self, u, time: float) -> np.ndarray:
+        out = (ctypes.c_double * 4)()
+        self._call("dgh_l2_error", _ptr(u), ctypes.c_double(time), out)
+        return np.array(out[:])
+
+    def speeds(self) -> np.ndarray:
+        ab = np.zeros(2 * self.faces * self.n)
+        self._call("dgh_speeds", ab.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return ab.reshape(-1, 2)
+
+    # ---- DGOperator
+    def dg_refresh(self, u):
+        self._call("dgh_dg_refresh", _ptr(u))
+
+    def dg_apply(self, v):
+        out = self.vec()
+        self._call("dgh_dg_apply", _ptr(v), _ptr(out))
+        return out
+
+    def dg_block(self, row: int, col: int) -> np.ndarray:
+        out = np.zeros(self.block * self.block)
+        self._call("dgh_dg_block", row, col, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out.reshape(self.block, self.block)
+
+    # ---- BlockJacobi
+    def precond_refresh(self, op: str):
+        self._call("dgh_block_jacobi_refresh", OPS[op])
+
+    def precond_apply(self, op: str, x):
+        z = self.vec(self.size if op == "dg" else self.trace_size)
+        self._call("dgh_precond_apply", OPS[op], _ptr(x), _ptr(z))
+        return z
+
+    # ---- HybridOperator
+    def hdg_refresh_projected(self, u, r):
+        self._call("dgh_hdg_refresh_projected", _ptr(u), _ptr(r))
+
+    def hdg_rhs(self):
+        out = self.vec(self.trace_size)
+        self._call("dgh_hdg_rhs", _ptr(out))
+        return out
+
+    def hdg_apply(self, lam):
+        out = self.vec(self.trace_size)
+        self._call("dgh_hdg_apply", _ptr(lam), _ptr(out))
+        return out
+
+    def hdg_block(self, row: int, col: int) -> np.ndarray:
+        fw = self.face_width
+        out = np.zeros(fw * fw)
+        self._call("dgh_hdg_block", row, col, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out.reshape(fw, fw)
+
+    def hdg_recover(self, dlam):
+        out = self.vec()
+        self._call("dgh_hdg_recover", _ptr(dlam), _ptr(out))
+        return out
+
+    def hdg_recovered_residual(self, e):
+        out = self.vec()
+        self._call("dgh_hdg_recovered_residual", _ptr(e), _ptr(out))
+        return out
+
+    # ---- GMRES
+    def gmres(self, op: str, rhs, limit: int, tol: float):
+        """Returns (x, iterations, relative residual, true residual)."""
+        x = self.vec(self.size if op == "dg" else self.trace_size)
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        self._call("dgh_gmres", OPS[op], _ptr(rhs), _ptr(x), limit, ctypes.c_double(tol), ctypes.byref(it),
+                   ctypes.byref(rel))
+        res_ptr = self.lib.dgh_gmres_residual(self.h, OPS[op])
+        res = self.vec(x.numel())
+        self._call("dgh_axpby", ctypes.c_double(1.0), ctypes.c_void_p(res_ptr), ctypes.c_double(0.0),
+                   ctypes.c_void_p(res_ptr), _ptr(res), x.numel())
+        return x, it.value, rel.value, res
+
+    # ---- TimeIntegrator
+    def advance(self, method: str, solution: np.ndarray, max_updates: int = 100000):
+        """TimeIntegrator::advance on a host state; returns (state, run stats dict, update rows)."""
+        it = ctypes.c_void_p()
+        self._rc(self.lib.dgh_integrator_create(self.h, METHODS[method], ctypes.byref(it)))
+        try:
+            sol = np.ascontiguousarray(solution, dtype=np.float64).copy()
+            st = _lib.dgh_run_stats()
+            rows = (_lib.dgh_update_stats * max_updates)()
+            rc = self.lib.dgh_advance(it, sol.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st), rows, max_updates)
+            if rc != 0:
+                raise DGHError(rc, self.lib.dgh_integrator_error(it).decode())
+            stats = {f: getattr(st, f) for f, _ in _lib.dgh_run_stats._fields_}
+            ups = [{f: getattr(rows[i], f) for f, _ in _lib.dgh_update_stats._fields_}
+                   for i in range(min(st.updates_recorded, max_updates))]
+            return sol, stats, ups
+        finally:
+            self.lib.dgh_integrator_destroy(it)
+
+
+class Integrator:
+    """Single Newton updates of one backward-Euler stage (the speed protocol's unit of work)."""
+
+    def __init__(self, solver: Solver, method: str):
+        self.s = solver
+        self.lib = solver.lib
+        self.h = ctypes.c_void_p()
+        solver._rc(self.lib.dgh_integrator_create(solver.h, METHODS[method], ctypes.byref(self.h)))
+
+    def _rc(self, rc):
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_integrator_error(self.h).decode())
+
+    def stage_begin(self, u) -> float:
+        dt = ctypes.c_double()
+        self.s.torch.cuda.synchronize(self.s.device)
+        self._rc(self.lib.dgh_stage_begin(self.h, _ptr(u), ctypes.byref(dt)))
+        return dt.value
+
+    def update(self) -> dict:
+        st = _lib.dgh_update_stats()
+        self._rc(self.lib.dgh_newton_update(self.h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _lib.dgh_update_stats._fields_}
+
+    def state_ptr(self) -> int:
+        return int(self.lib.dgh_integrator_state(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.dgh_integrator_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,192 @@
+/* dgh_gpu.h — C ABI of the B200 (sm_100a) implicit 2D DG / condensed-HDG Euler solver.
+ *
+ * Drop-in boundary for the reference YueWu2002/DG_HDG_Euler_Cpp.  The reference has no FFI;
+ * its internal seams are C++ classes, and each entry point below replaces one of them:
+ *   Problem        dg_hdg_2d/include/euler/discretization.hpp:7-45
+ *   DGOperator     dg_hdg_2d/include/euler/dg_operator.hpp:5-17
+ *   BlockJacobi    common/include/euler/linalg/block_jacobi.hpp:7-47
+ *   HybridOperator dg_hdg_2d/include/euler/hybrid.hpp:6-32
+ *   GMRES          common/include/euler/linalg/gmres.hpp:21-35
+ *   TimeIntegrator dg_hdg_2d/include/euler/time_integrator.hpp:21-40
+ *   Config         dg_hdg_2d/include/euler/config.hpp:7-18
+ *
+ * Conventions
+ *  - Every vector argument named u, r, v, x, z, lambda ... is a DEVICE pointer to FP64 data in
+ *    the reference layout (types.hpp:22-31 for volume vectors: per cell, NVAR sheets of n*n
+ *    nodes with x fastest; discretization.cpp:65-68 for trace vectors: per face NVAR lines of
+ *    n values).  Arguments named host_* are host pointers.
+ *  - All work is ordered on the context's CUDA stream (dgh_stream).  Functions that return a
+ *    host scalar synchronise that stream.
+ *  - Every function returns a dgh_status; on failure dgh_last_error() gives the reference's
+ *    require() message (e.g. "Singular block Jacobi factor", "GMRES iteration limit reached").
+ *  - A context owns all device memory it needs; nothing allocates after dgh_ctx_create except
+ *    the optional helpers dgh_vec_alloc/dgh_vec_free.  A context is not thread-safe, as the
+ *    reference's operators are not (DESIGN.md:42-43 of the reference).
+ *  - There is no CPU fallback: without a usable sm_100 device, dgh_ctx_create fails.
+ */
+#ifndef DGH_GPU_H
+#define DGH_GPU_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dgh_ctx dgh_ctx;
+
+typedef enum dgh_status {
+    DGH_OK = 0,
+    DGH_ERR_INVALID = 1,      /* bad argument or configuration (config.cpp:6-22)          */
+    DGH_ERR_CUDA = 2,         /* CUDA runtime error, no device, or out of device memory    */
+    DGH_ERR_SINGULAR = 3,     /* singular or non-finite block factor (block_jacobi.hpp:16) */
+    DGH_ERR_NONFINITE = 4,    /* non-finite GMRES residual (gmres.cpp:117)                 */
+    DGH_ERR_GMRES_LIMIT = 5,  /* GMRES iteration limit reached (gmres.cpp:121)             */
+    DGH_ERR_BREAKDOWN = 6,    /* GMRES Arnoldi breakdown (gmres.cpp:92)                    */
+    DGH_ERR_STATE = 7,        /* invalid physical state (physics.cpp:108, discretization)  */
+    DGH_ERR_SOLVER = 8        /* Newton / line search / HDG acceptance failure             */
+} dgh_status;
+
+enum { DGH_METHOD_DG = 0, DGH_METHOD_HDG = 1, DGH_METHOD_BOTH = 2 };
+enum { DGH_INTEGRATOR_DIRK3 = 0, DGH_INTEGRATOR_BE = 1 };
+enum { DGH_TEST_DIAGONAL = 0, DGH_TEST_WAVE = 1, DGH_TEST_AXIS = 2 };
+/* Precision of the block-Jacobi factors and their solves.  Residuals, J*v, the Schur apply,
+ * the HDG condensation, Arnoldi and the least-squares problem are always FP64. */
+enum { DGH_PRECISION_FP64 = 0, DGH_PRECISION_MIXED = 1 };
+enum { DGH_OP_DG = 0, DGH_OP_HDG = 1 };
+
+/* config.hpp:7-18 plus the precision and the operators to allocate. */
+typedef struct dgh_config {
+    int nx, ny, degree, quadrature; /* quadrature 0 or degree+1 (collocated Gauss)       */
+    int restart, max_linear, max_newton, steps, newton_steps, warmup_updates;
+    double cfl, final_time, safety, nonlinear_tolerance, linear_tolerance;
+    int method;       /* DGH_METHOD_*: which operators the context allocates               */
+    int integrator;   /* DGH_INTEGRATOR_*                                                  */
+    int testcase;     /* DGH_TEST_*                                                        */
+    int precision;    /* DGH_PRECISION_*                                                   */
+    int check_update; /* HDG: independent DG J*v check of every update (time_integrator.cpp:153-162) */
+    int device;       /* CUDA device ordinal                                               */
+} dgh_config;
+
+/* config.hpp:7-18 defaults: nx=ny=8, k=3, restart 30, max_linear 1500, max_newton 30,
+ * cfl 2, T 0.2, safety 1.1, ntol = ltol = 1e-12, ssp-dirk3, diagonal test case, both methods. */
+void dgh_config_default(dgh_config *cfg);
+
+/* ---- context ----------------------------------------------------------------------------- */
+int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out);
+int dgh_ctx_destroy(dgh_ctx *ctx);
+const char *dgh_last_error(const dgh_ctx *ctx);
+/* sizes[0..7]: volume size, trace size, cell block width m, cells, faces, nodes per direction
+ * n, local trace size t, face width fw */
+int dgh_sizes(const dgh_ctx *ctx, int64_t sizes[8]);
+/* The configuration the context was created with. */
+int dgh_get_config(const dgh_ctx *ctx, dgh_config *out);
+void *dgh_stream(const dgh_ctx *ctx);       /* the cudaStream_t all work is ordered on */
+/* out[0..3] = hx, hy, lx, ly (discretization.cpp:4-8, example.hpp:9-14) */
+int dgh_geometry(const dgh_ctx *ctx, double out[4]);
+/* Gauss nodes and weights on [-1,1] (n values each; either pointer may be NULL) */
+int dgh_nodes(const dgh_ctx *ctx, double *x, double *w);
+int dgh_sync(dgh_ctx *ctx);
+/* Device bytes held by the context (the pools sized at creation). */
+int dgh_device_bytes(const dgh_ctx *ctx, int64_t *bytes);
+/* Number of kernels this context has launched since creation (for launch accounting). */
+int64_t dgh_launch_count(const dgh_ctx *ctx);
+/* Optional CUDA-event timers around each class of kernel work (no counterpart in the reference,
+ * which times whole Newton updates only: time_integrator.cpp:93,180).  Enabling resets them. */
+enum {
+    DGH_TIMER_PRECOND = 0,     /* block-Jacobi solves (the per-iteration factor stream)      */
+    DGH_TIMER_OPERATOR = 1,    /* J*v or the Schur apply                                    */
+    DGH_TIMER_ARNOLDI = 2,     /* CGS2 dots/updates and the basis normalisation             */
+    DGH_TIMER_FACTOR = 3,      /* DG block assembly + batched LU                            */
+    DGH_TIMER_FACE_FACTOR = 4, /* HDG face-block assembly + batched LU                      */
+    DGH_TIMER_CONDENSE = 5,    /* HDG condensation: assembly, LU, back substitution, S, Cy  */
+    DGH_TIMER_RESIDUAL = 6,    /* R(u)                                                      */
+    DGH_TIMER_COUNT = 7
+};
+int dgh_timing_enable(dgh_ctx *ctx, int on);
+int dgh_timing_read(dgh_ctx *ctx, int category, double *total_ms, int64_t *count);
+
+/* ---- vector helpers (device memory, stream-ordered) ---------------------------------------- */
+int dgh_vec_alloc(dgh_ctx *ctx, int64_t n, double **dev);
+int dgh_vec_free(dgh_ctx *ctx, double *dev);
+int dgh_upload(dgh_ctx *ctx, double *dev, const double *host, int64_t n);
+int dgh_download(dgh_ctx *ctx, double *host, const double *dev, int64_t n);
+/* out = a*x + b*y (any of x, y, out may alias) */
+int dgh_axpby(dgh_ctx *ctx, double a, const double *x, double b, const double *y, double *out, int64_t n);
+
+/* ---- Problem (discretization.hpp:7-45) ------------------------------------------------------ */
+int dgh_initial(dgh_ctx *ctx, double *u);                          /* initial_and_error.cpp:4-54 */
+int dgh_freeze(dgh_ctx *ctx, const double *u, double *rate);       /* discretization.cpp:163-195; old = u */
+int dgh_set_stage(dgh_ctx *ctx, const double *old, double step_size); /* Problem::old, step_size */
+int dgh_residual(dgh_ctx *ctx, const double *u, double *r);        /* discretization.cpp:123-140 */
+int dgh_admissible(dgh_ctx *ctx, const double *u, int *ok);        /* discretization.cpp:219-233 */
+int dgh_trace(dgh_ctx *ctx, const double *u, double *lambda);      /* discretization.cpp:196-210 */
+int dgh_dual_norm(dgh_ctx *ctx, const double *r, double *out);     /* sqrt(r^T M^-1 r), time_integrator.cpp:42 */
+int dgh_state_norm(dgh_ctx *ctx, const double *u, double *out);    /* sqrt(u^T M u), time_integrator.cpp:45 */
+int dgh_integral(dgh_ctx *ctx, const double *u, double out[4]);    /* discretization.cpp:237-243 */
+int dgh_l2_error(dgh_ctx *ctx, const double *u, double time, double out[4]); /* initial_and_error.cpp:55-73 */
+int dgh_speeds(dgh_ctx *ctx, double *host_ab);                     /* frozen (a,b) per face node */
+
+/* ---- DGOperator (dg_operator.hpp:5-17) ------------------------------------------------------ */
+int dgh_dg_refresh(dgh_ctx *ctx, const double *u);                 /* dg_operator.cpp:6-9 */
+int dgh_dg_apply(dgh_ctx *ctx, const double *v, double *jv);       /* dg_operator.cpp:10-21 */
+/* Diagonal block (row == col), copied to the host row-major m x m (dg_operator.cpp:22-48). */
+int dgh_dg_block(dgh_ctx *ctx, int row, int col, double *host_block);
+
+/* ---- BlockJacobi (block_jacobi.hpp:7-47) ---------------------------------------------------- */
+/* op DGH_OP_DG: assemble and factor the E cell blocks from the current DG linearisation;
+ * op DGH_OP_HDG: the 2E face blocks of the current condensed operator. */
+int dgh_block_jacobi_refresh(dgh_ctx *ctx, int op);
+int dgh_precond_apply(dgh_ctx *ctx, int op, const double *x, double *z);
+
+/* ---- HybridOperator (hybrid.hpp:6-32) ------------------------------------------------------- */
+int dgh_hdg_refresh_projected(dgh_ctx *ctx, const double *u, const double *r); /* hybrid.cpp:28-30,56-72 */
+int dgh_hdg_rhs(dgh_ctx *ctx, double *rhs);                        /* condensed right-hand side */
+int dgh_hdg_apply(dgh_ctx *ctx, const double *lambda, double *out); /* hybrid.cpp:73-82 */
+int dgh_hdg_block(dgh_ctx *ctx, int row, int col, double *host_block); /* hybrid.cpp:83-96, row == col */
+int dgh_hdg_recover(dgh_ctx *ctx, const double *dlambda, double *du); /* hybrid.cpp:97-105 */
+int dgh_hdg_recovered_residual(dgh_ctx *ctx, const double *e, double *out); /* hybrid.cpp:106-121 */
+
+/* ---- GMRES (gmres.cpp:17-86) ---------------------------------------------------------------- */
+/* Right-preconditioned restarted GMRES(restart) with CGS2 in the M^-1 (DG) or inverse trace
+ * mass (HDG) inner product, on op with its block-Jacobi preconditioner.  x is overwritten. */
+int dgh_gmres(dgh_ctx *ctx, int op, const double *rhs, double *x, int limit, double tol,
+              int *iterations, double *relative);
+/* Device pointer to the true residual rhs - A x of the last dgh_gmres call on op. */
+const double *dgh_gmres_residual(dgh_ctx *ctx, int op);
+
+/* ---- TimeIntegrator (time_integrator.hpp:21-40, time_integrator.cpp:48-213) ------------------ */
+typedef struct dgh_update_stats { /* time_integrator.hpp:9-13 */
+    int step, stage, iteration, krylov_iterations;
+    double time, stage_time, dt, cfl, residual_physical_rms, damping;
+    double linear_relative_residual, dg_linear_relative_residual, iteration_s;
+} dgh_update_stats;
+typedef struct dgh_run_stats { /* time_integrator.hpp:14-20 */
+    double final_time, conservation_drift, seconds, max_linear_residual;
+    double max_dg_linear_residual, minimum_step, maximum_step, measured_newton_seconds;
+    int steps, newton_iterations, krylov_iterations, measured_updates, updates_recorded;
+} dgh_run_stats;
+
+typedef struct dgh_integrator dgh_integrator;
+int dgh_integrator_create(dgh_ctx *ctx, int method, dgh_integrator **out);
+int dgh_integrator_destroy(dgh_integrator *it);
+/* Message of the integrator's last failure (the reference's require() text). */
+const char *dgh_integrator_error(const dgh_integrator *it);
+/* Full run (TimeIntegrator::advance); host_solution is read and overwritten on the host.
+ * Up to max_updates per-update rows are written to updates (may be NULL). */
+int dgh_advance(dgh_integrator *it, double *host_solution, dgh_run_stats *stats,
+                dgh_update_stats *updates, int max_updates);
+/* Speed protocol pieces (speed_test/2d/benchmark.py:21-44): start one backward-Euler stage
+ * from a device state (freeze, dt = cfl/rate, old = state), then run single Newton updates
+ * (time_integrator.cpp:133-234 for one `it`). */
+int dgh_stage_begin(dgh_integrator *it, const double *u, double *dt);
+int dgh_newton_update(dgh_integrator *it, dgh_update_stats *stats);
+/* The same Newton update through host buffers: host_state is copied to the device first and
+ * the updated state is copied back (the end-to-end form of the call). */
+int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_stats *stats);
+/* Device pointer to the integrator's current Newton state (size dgh_sizes()[0]). */
+double *dgh_integrator_state(dgh_integrator *it);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGH_GPU_H */

@@ -1,0 +1,83 @@
+"""CPU-side checks of the C ABI library: it builds for sm_100a, loads, and exports every entry
+point include/dgh_gpu.h declares; without a GPU, context creation fails with an error code
+instead of falling back to the CPU."""
+import ctypes
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = ROOT / "include" / "dgh_gpu.h"
+
+
+def declared_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    names = re.findall(r"\b(dgh_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    if not _lib.LIB_PATH.exists():
+        _lib.build()
+    return _lib.load()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) >= 45
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    assert set(declared_functions()) == set(_lib.SIGNATURES)
+
+
+def test_config_defaults_match_reference(lib):
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    cfg = _lib.dgh_config()
+    lib.dgh_config_default(ctypes.byref(cfg))
+    # dg_hdg_2d/include/euler/config.hpp:7-18
+    assert (cfg.nx, cfg.ny, cfg.degree, cfg.quadrature) == (8, 8, 3, 0)
+    assert (cfg.restart, cfg.max_linear, cfg.max_newton, cfg.steps) == (30, 1500, 30, 0)
+    assert (cfg.cfl, cfg.final_time, cfg.safety) == (2.0, 0.2, 1.1)
+    assert cfg.nonlinear_tolerance == cfg.linear_tolerance == 1e-12
+
+
+def test_invalid_configuration_is_rejected_before_any_device_work(lib):
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    cfg = _lib.dgh_config()
+    lib.dgh_config_default(ctypes.byref(cfg))
+    cfg.degree = 9  # config.cpp:7 allows k <= 8
+    h = ctypes.c_void_p()
+    rc = lib.dgh_ctx_create(ctypes.byref(cfg), ctypes.byref(h))
+    assert rc == 1 and not h.value
+    assert b"Invalid mesh or degree" in lib.dgh_last_error(None)
+
+
+def test_no_cpu_fallback_without_gpu(lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    cfg = _lib.dgh_config()
+    lib.dgh_config_default(ctypes.byref(cfg))
+    h = ctypes.c_void_p()
+    rc = lib.dgh_ctx_create(ctypes.byref(cfg), ctypes.byref(h))
+    assert rc == 2 and not h.value  # DGH_ERR_CUDA
+
+
+def test_kernels_are_built_for_sm100a():
+    log = (ROOT / "dg_hdg_euler_cpp_b200" / "lib" / "ptxas.log").read_text()
+    assert "sm_100a" in log
+    assert "k_lu" in log and "k_dg_apply" in log and "k_hdg_apply" in log
