@@ -243,25 +243,37 @@ void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
     c->launched();
 }
 
-constexpr int LU_NB = 32, LU_TC = 64;
+// Panel width 32; U12 tile width 32 for FP64 (two CTAs per SM fit in shared memory at m = 324)
+// and 64 for FP32.
+constexpr int LU_NB = 32;
+template <typename TF> constexpr int lu_tc() { return sizeof(TF) == 8 ? 32 : 64; }
 template <typename TF> void setup_lu_attrs(size_t smem) {
-    ck(cudaFuncSetAttribute(k_lu<TF, LU_NB, LU_TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "lu attr");
+    ck(cudaFuncSetAttribute(k_lu<TF, LU_NB, lu_tc<TF>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+       "lu attr");
 }
 template <typename TF>
-void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, int bit) {
-    const size_t smem = lu_smem_bytes<TF, LU_NB, LU_TC>(m);
+void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out) {
+    constexpr int TC = lu_tc<TF>();
+    const size_t smem = lu_smem_bytes<TF, LU_NB, TC>(m);
     setup_lu_attrs<TF>(smem);
-    const int per_sm = std::max(1, (int)((220u * 1024u) / smem));
-    const int grid = std::min(count, c->sms * per_sm);
-    k_lu<TF, LU_NB, LU_TC><<<grid, LU_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, perm, c->status, bit);
+    int per_sm = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu<TF, LU_NB, TC>, LU_THREADS, smem), "occupancy");
+    const int grid = std::min(count, c->sms * std::max(1, per_sm));
+    k_lu<TF, LU_NB, TC><<<grid, LU_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, perm, c->status, bit,
+                                                               slab_out ? 1 : 0);
     c->launched();
 }
+// One warp per block; enough warps for every SM to keep its warp slots (and their loads) busy.
 template <typename TF>
 void launch_solve(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
                   double *z) {
-    const size_t smem = sizeof(TF) * m;
-    const int grid = std::min(count, c->sms * 8);
-    k_lu_solve<TF><<<grid, LU_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
+    constexpr int wpc = SOLVE_THREADS / 32;
+    const size_t smem = sizeof(TF) * (size_t)m * wpc;
+    const int want = (count + wpc - 1) / wpc;
+    int resident = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve<TF>, SOLVE_THREADS, smem), "occupancy");
+    const int grid = std::min(want, c->sms * std::max(1, resident));
+    k_lu_solve<TF><<<grid, SOLVE_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
     c->launched();
 }
 
@@ -311,8 +323,16 @@ void maxpy_t(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, dou
 template <int NV> void lincomb_t(dgh_ctx *c, const double *V, size_t ld, int K, const double *coef, double *out, long long n) {
     k_lincomb<NV><<<c->red_grid, KR_THREADS, 0, c->stream>>>(V, ld, K, coef, out, n);
 }
-#define DGH_DISPATCH_K(K, CALL) \
-    do { if ((K) <= 4) { CALL(4); } else if ((K) <= 8) { CALL(8); } else if ((K) <= 16) { CALL(16); } else { CALL(32); } } while (0)
+// Arnoldi kernels are instantiated for the exact number of basis vectors (1..32), so their
+// loops unroll without predicates.
+#define DGH_K8(CALL, b) case b + 1: CALL(b + 1); break; case b + 2: CALL(b + 2); break; case b + 3: CALL(b + 3); break; \
+    case b + 4: CALL(b + 4); break; case b + 5: CALL(b + 5); break; case b + 6: CALL(b + 6); break;              \
+    case b + 7: CALL(b + 7); break; case b + 8: CALL(b + 8); break;
+#define DGH_DISPATCH_K(K, CALL)                                                                 \
+    switch (K) {                                                                                \
+        DGH_K8(CALL, 0) DGH_K8(CALL, 8) DGH_K8(CALL, 16) DGH_K8(CALL, 24)                       \
+        default: fail(DGH_ERR_INVALID, "Krylov basis too large");                               \
+    }
 
 void mdot(dgh_ctx *c, const double *V, size_t ld, int K, const double *x, const double *W, long long n, double *out) {
 #define C_(NV) mdot_t<NV>(c, V, ld, K, x, W, n)
@@ -923,14 +943,14 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
                                                                          c->basis, c->g, c->inv_step, 0, c->cells);
                 });
                 c->launched();
-                launch_lu<float>(c, (float *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR);
+                launch_lu<float>(c, (float *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR, true);
             } else {
                 DGH_DISPATCH_N(c->n, {
                     k_dg_assemble<N, double><<<grid, 256, 0, c->stream>>>((double *)c->dg_pool, c->vol, c->fcache, c->speeds,
                                                                           c->basis, c->g, c->inv_step, 0, c->cells);
                 });
                 c->launched();
-                launch_lu<double>(c, (double *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR);
+                launch_lu<double>(c, (double *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR, true);
             }
             c->check_status();
             c->dg_factored = true;
@@ -945,14 +965,14 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
                                                                                                  c->basis, c->g);
                 });
                 c->launched();
-                launch_lu<float>(c, (float *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR);
+                launch_lu<float>(c, (float *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR, true);
             } else {
                 DGH_DISPATCH_N(c->n, {
                     k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (double *)c->face_pool,
                                                                                                   c->basis, c->g);
                 });
                 c->launched();
-                launch_lu<double>(c, (double *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR);
+                launch_lu<double>(c, (double *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR, true);
             }
             c->check_status();
             c->face_factored = true;
@@ -978,7 +998,7 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
                                                                        c->inv_step, first, count);
             });
             c->launched();
-            launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG);
+            launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
             k_backsolve<double><<<std::min(count, c->sms * 2), LU_THREADS, 0, c->stream>>>(c->aug, (size_t)c->m * ld, c->m, ld, count);
             c->launched();
             DGH_DISPATCH_N(c->n, {

@@ -43,8 +43,7 @@ k_mdot(const double *__restrict__ V, size_t ldv, int K, const double *__restrict
     for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
         const double wx = W[i] * x[i];
 #pragma unroll
-        for (int k = 0; k < NV; ++k)
-            if (k < K) acc[k] += V[k * ldv + i] * wx;
+        for (int k = 0; k < NV; ++k) acc[k] += V[k * ldv + i] * wx;
     }
     block_reduce_store<NV>(acc, K, partial, gridDim.x);
 }
@@ -65,18 +64,16 @@ k_maxpy_reduce(const double *__restrict__ V, size_t ldv, int K, const double *__
         double v[NV];
         double s = 0;
 #pragma unroll
-        for (int k = 0; k < NV; ++k)
-            if (k < K) {
-                v[k] = V[k * ldv + i];
-                s += v[k] * hs[k];
-            }
+        for (int k = 0; k < NV; ++k) {
+            v[k] = V[k * ldv + i];
+            s += v[k] * hs[k];
+        }
         const double xn = x[i] - s;
         x[i] = xn;
         const double wx = W[i] * xn;
         if (MODE == 0) {
 #pragma unroll
-            for (int k = 0; k < NV; ++k)
-                if (k < K) acc[k] += v[k] * wx;
+            for (int k = 0; k < NV; ++k) acc[k] += v[k] * wx;
         } else {
             acc[0] += xn * wx;
         }
@@ -112,8 +109,7 @@ k_lincomb(const double *__restrict__ V, size_t ldv, int K, const double *__restr
     for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
         double s = 0;
 #pragma unroll
-        for (int k = 0; k < NV; ++k)
-            if (k < K) s += V[k * ldv + i] * cs[k];
+        for (int k = 0; k < NV; ++k) s += V[k * ldv + i] * cs[k];
         out[i] = s;
     }
 }
@@ -128,8 +124,7 @@ __global__ void k_scale_div(const double *__restrict__ x, const double *__restri
 }
 
 // y = a*x + b*y  (general axpby used for x += z, r = rhs - Ax, trial = state + theta*dir)
-__global__ void k_axpby(double a, const double *__restrict__ x, double b, const double *__restrict__ y,
-                        double *__restrict__ out, long long n) {
+__global__ void k_axpby(double a, const double *x, double b, const double *y, double *out, long long n) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = a * x[i] + b * y[i];
 }

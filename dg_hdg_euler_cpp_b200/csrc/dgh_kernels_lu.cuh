@@ -14,27 +14,124 @@ namespace dgh {
 
 template <typename T> __device__ inline T tabs(T x) { return x < T(0) ? -x : x; }
 
+// Slab layout of a factored block (written by k_lu with slab_out, read by k_lu_solve): rows
+// 32s..32s+nt-1 form slab s; inside a slab, columns come in groups of W = 16 bytes / sizeof(T)
+// and each row's W values of a group are adjacent: element (32s + i, j) sits at
+// 32 s m + (j / W) nt W + i W + j % W.  Lane i of a warp then loads its row's next W columns as
+// one 16-byte vector, and the warp's load of a column group is nt*16 contiguous bytes.
+// m = 4n^2 (cells) and 4n (faces) are multiples of W, so every group is complete.
+template <typename T> struct SlabVec;
+template <> struct SlabVec<double> {
+    using V = double2;
+    static constexpr int W = 2;
+    __device__ static double dot(const V &a, const double *y) { return a.x * y[0] + a.y * y[1]; }
+};
+template <> struct SlabVec<float> {
+    using V = float4;
+    static constexpr int W = 4;
+    __device__ static float dot(const V &a, const float *y) { return a.x * y[0] + a.y * y[1] + a.z * y[2] + a.w * y[3]; }
+};
+template <typename T> __device__ inline size_t slab_at(int nt, int i, int j) {
+    constexpr int W = SlabVec<T>::W;
+    return (size_t)(j / W) * nt * W + i * W + j % W;
+}
+
 constexpr int LU_THREADS = 256;
 
 template <typename T, int NB, int TC>
 constexpr size_t lu_smem_bytes(int m) {
-    return sizeof(T) * ((size_t)m * (NB + 1) + (size_t)NB * TC) + sizeof(int) * ((size_t)m + NB);
+    return sizeof(T) * ((size_t)m * (NB + 1) + (size_t)NB * TC + (size_t)NB * (NB + 1)) +
+           sizeof(int) * ((size_t)4 * m + NB);
 }
 
+// Unblocked LU of the NB-column panel held in shared memory by the whole CTA: per column, a
+// warp-shuffle pivot search (the first largest |a| wins) whose per-warp candidates every thread
+// combines in the same order, the row interchange, and the rank-1 update with threads owning
+// rows (three barriers per column).  The interchanges go to swp[] (panel-relative).  Also forms
+// Li = L11^{-1}, the inverse of the unit-lower diagonal block, so U12 = L11^{-1} A12 is a product.
+template <typename T, int NB>
+__device__ void panel_factor(T *P, int rows, int nb, int *swp, T *Li, T *cand_v, int *cand_i) {
+    constexpr int PP = NB + 1, NW = LU_THREADS / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int jj = 0; jj < nb; ++jj) {
+        T best = T(-1);
+        int bi = 0x7fffffff;
+        for (int r = jj + tid; r < rows; r += LU_THREADS) {
+            const T a = tabs(P[r * PP + jj]);
+            if (a > best) { best = a; bi = r; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (lane == 0) {
+            cand_v[warp] = best;
+            cand_i[warp] = bi;
+        }
+        __syncthreads();
+        best = cand_v[0];
+        bi = cand_i[0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w)
+            if (cand_v[w] > best || (cand_v[w] == best && cand_i[w] < bi)) { best = cand_v[w]; bi = cand_i[w]; }
+        const int p = (bi == 0x7fffffff || !(best == best)) ? jj : bi;  // NaN column: keep the diagonal
+        if (tid == 0) swp[jj] = p;
+        if (p != jj && tid < nb) {
+            const T t = P[jj * PP + tid];
+            P[jj * PP + tid] = P[p * PP + tid];
+            P[p * PP + tid] = t;
+        }
+        __syncthreads();
+        const T pivot = P[jj * PP + jj];
+        for (int r = jj + 1 + tid; r < rows; r += LU_THREADS) {
+            T l = P[r * PP + jj];
+            if (pivot != T(0)) l = l / pivot;
+            P[r * PP + jj] = l;
+            for (int c = jj + 1; c < nb; ++c) P[r * PP + c] -= l * P[jj * PP + c];
+        }
+        __syncthreads();
+    }
+    if (tid < nb) {  // Li = L11^{-1}, column tid
+        const int c = tid;
+        for (int i = 0; i < nb; ++i) Li[i * PP + c] = i == c ? T(1) : T(0);
+        for (int i = c + 1; i < nb; ++i) {
+            T s = 0;
+            for (int l = c; l < i; ++l) s += P[i * PP + l] * Li[l * PP + c];
+            Li[i * PP + c] = -s;
+        }
+    }
+    __syncthreads();
+}
+
+// Right-looking blocked LU.  Row interchanges are never executed one at a time: the columns
+// right of the panel are read through the panel's row permutation when its U12 tile and the
+// trailing rows are formed (a row moved by the panel's pivoting comes from the panel's top
+// rows, which are written only after the trailing update, so the gather is race-free), and the
+// L columns of earlier panels are permuted once at the end (lfix, skipped for the augmented
+// HDG matrices, whose L factor is not needed after the forward elimination).
 template <typename T, int NB, int TC>
 __global__ void __launch_bounds__(LU_THREADS)
 k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restrict__ perm_out, int *status,
-     int singular_bit) {
+     int singular_bit, int slab_out) {
     constexpr int PP = NB + 1;
+    static_assert(LU_THREADS % TC == 0 && NB % (LU_THREADS / TC) == 0, "tile shape");
     extern __shared__ __align__(16) unsigned char smraw[];
     T *P = reinterpret_cast<T *>(smraw);  // panel rows k0..m-1, NB columns, pitch PP
-    T *U = P + (size_t)m * PP;            // U12 tile: NB x TC
-    int *piv = reinterpret_cast<int *>(U + NB * TC);
-    int *swp = piv + m;
-    __shared__ T red_v[LU_THREADS / 32];
-    __shared__ int red_i[LU_THREADS / 32];
+    T *U = P + (size_t)m * PP;            // A12 / U12 tile: NB x TC
+    T *Li = U + NB * TC;                  // L11^{-1}: NB x NB, pitch PP
+    int *piv = reinterpret_cast<int *>(Li + NB * PP);  // position -> original row
+    int *src = piv + m;                   // panel-relative source position of each position
+    int *ipiv = src + m;                  // LAPACK-style interchange list
+    int *inv = ipiv + m;                  // scratch for the L fix-up
+    int *swp = inv + m;
     __shared__ int bad;
+    __shared__ T cand_v[LU_THREADS / 32];
+    __shared__ int cand_i[LU_THREADS / 32];
+    static_assert(NB == 32, "panel rows are moved by one warp lane per column");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = LU_THREADS / 32;
 
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         T *A = pool + (size_t)blk * stride;
@@ -43,228 +140,234 @@ k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restr
         __syncthreads();
         for (int k0 = 0; k0 < m; k0 += NB) {
             const int nb = min(NB, m - k0), rows = m - k0;
-            for (int idx = tid; idx < rows * nb; idx += LU_THREADS) {
-                const int r = idx / nb, c = idx % nb;
-                P[r * PP + c] = A[(size_t)(k0 + r) * ld + k0 + c];
-            }
+            if (lane < nb)
+                for (int r = warp; r < rows; r += NW) P[r * PP + lane] = A[(size_t)(k0 + r) * ld + k0 + lane];
+            for (int i = tid; i < rows; i += LU_THREADS) src[i] = i;
             __syncthreads();
-            // ---- unblocked factorisation of the panel
-            for (int jj = 0; jj < nb; ++jj) {
-                T best = T(-1);
-                int bi = 0x7fffffff;
-                for (int r = jj + tid; r < rows; r += LU_THREADS) {
-                    const T a = tabs(P[r * PP + jj]);
-                    if (a > best || (a == best && r < bi)) { best = a; bi = r; }
+            panel_factor<T, NB>(P, rows, nb, swp, Li, cand_v, cand_i);
+            if (tid == 0)
+                for (int jj = 0; jj < nb; ++jj) {
+                    const int p = swp[jj];
+                    ipiv[k0 + jj] = k0 + p;
+                    int t = src[jj]; src[jj] = src[p]; src[p] = t;
+                    t = piv[k0 + jj]; piv[k0 + jj] = piv[k0 + p]; piv[k0 + p] = t;
                 }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    const T ob = __shfl_down_sync(0xffffffffu, best, o);
-                    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-                    if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-                }
-                if (lane == 0) { red_v[warp] = best; red_i[warp] = bi; }
-                __syncthreads();
-                if (tid == 0) {
-                    T b0 = red_v[0];
-                    int i0 = red_i[0];
-                    for (int w = 1; w < LU_THREADS / 32; ++w)
-                        if (red_v[w] > b0 || (red_v[w] == b0 && red_i[w] < i0)) { b0 = red_v[w]; i0 = red_i[w]; }
-                    if (i0 == 0x7fffffff || !(b0 == b0)) i0 = jj;  // NaN column: keep the diagonal
-                    swp[jj] = i0;
-                }
-                __syncthreads();
-                const int p = swp[jj];
-                if (p != jj)
-                    for (int c = tid; c < nb; c += LU_THREADS) {
-                        const T t = P[jj * PP + c];
-                        P[jj * PP + c] = P[p * PP + c];
-                        P[p * PP + c] = t;
-                    }
-                __syncthreads();
-                const T pivot = P[jj * PP + jj];
-                for (int r = jj + 1 + tid; r < rows; r += LU_THREADS) {
-                    T l = P[r * PP + jj];
-                    if (pivot != T(0)) l = l / pivot;
-                    P[r * PP + jj] = l;
-                    for (int c = jj + 1; c < nb; ++c) P[r * PP + c] -= l * P[jj * PP + c];
-                }
-                __syncthreads();
-            }
-            // ---- write the panel back
-            for (int idx = tid; idx < rows * nb; idx += LU_THREADS) {
-                const int r = idx / nb, c = idx % nb;
-                A[(size_t)(k0 + r) * ld + k0 + c] = P[r * PP + c];
-            }
-            // ---- apply the panel's row interchanges to all other columns, in order
-            for (int jj = 0; jj < nb; ++jj) {
-                const int r1 = k0 + jj, r2 = k0 + swp[jj];
-                if (r1 != r2) {
-                    for (int c = tid; c < ld - nb; c += LU_THREADS) {
-                        const int col = c < k0 ? c : c + nb;
-                        const T t = A[(size_t)r1 * ld + col];
-                        A[(size_t)r1 * ld + col] = A[(size_t)r2 * ld + col];
-                        A[(size_t)r2 * ld + col] = t;
-                    }
-                    if (tid == 0) {
-                        const int t = piv[r1];
-                        piv[r1] = piv[r2];
-                        piv[r2] = t;
-                    }
-                }
-                __syncthreads();
-            }
-            // ---- U12 = L11^{-1} A12 and the trailing update, one column tile at a time
+            if (lane < nb)
+                for (int r = warp; r < rows; r += NW) A[(size_t)(k0 + r) * ld + k0 + lane] = P[r * PP + lane];
+            __syncthreads();
             for (int c0 = k0 + nb; c0 < ld; c0 += TC) {
                 const int tc = min(TC, ld - c0);
-                for (int idx = tid; idx < nb * TC; idx += LU_THREADS) {
+                for (int idx = tid; idx < NB * TC; idx += LU_THREADS) {
                     const int i = idx / TC, c = idx % TC;
-                    U[i * TC + c] = c < tc ? A[(size_t)(k0 + i) * ld + c0 + c] : T(0);
+                    U[i * TC + c] = (c < tc && i < nb) ? A[(size_t)(k0 + src[i]) * ld + c0 + c] : T(0);
                 }
                 __syncthreads();
-                if (tid < tc)
-                    for (int i = 1; i < nb; ++i) {
-                        T val = U[i * TC + tid];
-                        for (int l = 0; l < i; ++l) val -= P[i * PP + l] * U[l * TC + tid];
-                        U[i * TC + tid] = val;
+                {  // U12 = L11^{-1} A12
+                    constexpr int RG = LU_THREADS / TC, RPT = NB / RG;
+                    const int c = tid % TC, rg = tid / TC;
+                    T out[RPT];
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q) {
+                        const int i = rg + RG * q;
+                        T acc = 0;
+                        for (int l = 0; l <= i && l < nb; ++l) acc += Li[i * PP + l] * U[l * TC + c];
+                        out[q] = acc;
                     }
-                __syncthreads();
-                for (int idx = tid; idx < nb * tc; idx += LU_THREADS) {
-                    const int i = idx / tc, c = idx % tc;
-                    A[(size_t)(k0 + i) * ld + c0 + c] = U[i * TC + c];
+                    __syncthreads();
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q) U[(rg + RG * q) * TC + c] = out[q];
                 }
-                // trailing rows k0+nb .. m-1
+                __syncthreads();
+                // trailing rows: A[k0+nb+r] = A[k0+src[nb+r]] - L21 U12 (loads one pass ahead)
                 const int R = rows - nb;
                 const int tx = tid % (TC / 4), ty = tid / (TC / 4);
                 constexpr int TY = LU_THREADS / (TC / 4);
-                for (int rb = 0; rb < R; rb += 4 * TY) {
-                    T acc[4][4];
-                    int rr[4];
+                T nxt[4][4];
+                auto load_pass = [&](int rb) {
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        rr[k] = rb + ty + TY * k;
+                        const int r = min(rb + ty + TY * k, R - 1);
+                        const T *rowp = A + (size_t)(k0 + src[nb + r]) * ld + c0 + 4 * tx;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int c = 4 * tx + j;
-                            acc[k][j] = (rr[k] < R && c < tc) ? A[(size_t)(k0 + nb + rr[k]) * ld + c0 + c] : T(0);
-                        }
+                        for (int j = 0; j < 4; ++j) nxt[k][j] = (4 * tx + j < tc) ? rowp[j] : T(0);
                     }
+                };
+                if (R > 0) load_pass(0);
+                for (int rb = 0; rb < R; rb += 4 * TY) {
+                    T acc[4][4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[k][j] = nxt[k][j];
+                    if (rb + 4 * TY < R) load_pass(rb + 4 * TY);
+                    const T *lrow[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) lrow[k] = P + (size_t)(nb + min(rb + ty + TY * k, R - 1)) * PP;
+                    const T *ucol = U + 4 * tx;
+#pragma unroll 4
                     for (int l = 0; l < nb; ++l) {
                         T uu[4];
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) uu[j] = U[l * TC + 4 * tx + j];
+                        for (int j = 0; j < 4; ++j) uu[j] = ucol[l * TC + j];
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
-                            const T lv = rr[k] < R ? P[(nb + rr[k]) * PP + l] : T(0);
+                            const T lv = lrow[k][l];
 #pragma unroll
                             for (int j = 0; j < 4; ++j) acc[k][j] -= lv * uu[j];
                         }
                     }
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = rb + ty + TY * k;
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
                             const int c = 4 * tx + j;
-                            if (rr[k] < R && c < tc) A[(size_t)(k0 + nb + rr[k]) * ld + c0 + c] = acc[k][j];
+                            if (r < R && c < tc) A[(size_t)(k0 + nb + r) * ld + c0 + c] = acc[k][j];
                         }
+                    }
+                }
+                __syncthreads();
+                for (int i = tid / TC; i < nb; i += LU_THREADS / TC) {
+                    const int c = tid % TC;
+                    if (c < tc) A[(size_t)(k0 + i) * ld + c0 + c] = U[i * TC + c];
+                }
+                __syncthreads();
+            }
+        }
+        // ---- L fix-up: panel q's L rows were written in the arrangement after panel q; gather
+        // them into the final arrangement (piv) through the inverse arrangement of that time.
+        if (slab_out) {
+            for (int i = tid; i < m; i += LU_THREADS) {
+                src[i] = i;  // arrangement: position -> original row
+                inv[i] = i;  // original row -> position
+            }
+            __syncthreads();
+            for (int k0 = 0; k0 < m; k0 += NB) {
+                const int nb = min(NB, m - k0), base = k0 + nb;
+                if (tid == 0)
+                    for (int jj = 0; jj < nb; ++jj) {
+                        const int a = k0 + jj, b = ipiv[k0 + jj];
+                        const int ra = src[a], rb = src[b];
+                        src[a] = rb; src[b] = ra;
+                        inv[rb] = a; inv[ra] = b;
+                    }
+                __syncthreads();
+                if (base < m && lane < nb) {
+                    for (int i = warp; i < m - base; i += NW) P[i * PP + lane] = A[(size_t)inv[piv[base + i]] * ld + k0 + lane];
+                }
+                __syncthreads();
+                if (base < m && lane < nb) {
+                    for (int i = warp; i < m - base; i += NW) A[(size_t)(base + i) * ld + k0 + lane] = P[i * PP + lane];
                 }
                 __syncthreads();
             }
         }
         // ---- singularity check on the diagonal (block_jacobi.hpp:16-18, dense_lu.hpp:13-16)
         for (int i = tid; i < m; i += LU_THREADS) {
-            const T d = A[(size_t)i * ld + i];
-            const double dd = (double)d;
+            const double dd = (double)A[(size_t)i * ld + i];
             if (!isfinite(dd) || !(fabs(dd) > 2.2250738585072014e-308)) bad = 1;
             perm_out[(size_t)blk * m + i] = piv[i];
         }
         __syncthreads();
         if (tid == 0 && bad) atomicOr(status, singular_bit);
+        // ---- in-place conversion to the slab layout read by k_lu_solve (ld == m only)
+        if (slab_out) {
+            constexpr int W = SlabVec<T>::W;
+            for (int r0 = 0; r0 < m; r0 += 32) {
+                const int nt = min(32, m - r0);
+                T *reg = A + (size_t)r0 * m;
+                for (int idx = tid; idx < nt * m; idx += LU_THREADS) P[idx] = reg[idx];
+                __syncthreads();
+                // destination index e = g*nt*W + i*W + w holds row i, column g*W + w
+                for (int g = warp; g < m / W; g += NW)
+                    for (int e = lane; e < nt * W; e += 32) reg[(size_t)g * nt * W + e] = P[(e / W) * m + g * W + e % W];
+                __syncthreads();
+            }
+        }
         __syncthreads();
     }
 }
 
 // Block solve z = A^{-1} b with the factors of k_lu (block_jacobi.hpp:24-39): permute, unit
-// lower solve, upper solve.  Rows are streamed once; 32-row tiles use a warp-per-row GEMV
-// against the solved part and a one-warp triangular solve for the diagonal tile.  T is the
-// factor and arithmetic precision; b and z are FP64.
+// lower solve, upper solve.  One warp owns one block and streams its factors exactly once with
+// no CTA-wide barriers; lane i owns row 32 s + i of slab s and reads 16-byte column groups of
+// the slab layout above.  Off-diagonal parts are per-lane dot products; the diagonal triangles
+// of the 32-row slabs are solved with warp shuffles.  T is the factor and arithmetic precision
+// (FP32 factors accumulate in FP32); b and z are FP64.
+constexpr int SOLVE_THREADS = 256;
 template <typename T>
-__global__ void __launch_bounds__(LU_THREADS)
+__global__ void __launch_bounds__(SOLVE_THREADS)
 k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stride, int m, int count,
            const double *__restrict__ rhs, double *__restrict__ z) {
+    using SV = SlabVec<T>;
+    using V = typename SV::V;
+    constexpr int W = SV::W;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T *y = reinterpret_cast<T *>(smraw);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = LU_THREADS / 32;
-    for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    T *y = reinterpret_cast<T *>(smraw) + (size_t)wib * m;
+    const int warps = gridDim.x * (SOLVE_THREADS / 32);
+    const int slabs = (m + 31) / 32;
+    for (int blk = blockIdx.x * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
         const T *A = pool + (size_t)blk * stride;
         const int *pm = perm + (size_t)blk * m;
         const double *b = rhs + (size_t)blk * m;
-        for (int i = tid; i < m; i += LU_THREADS) y[i] = (T)b[pm[i]];
-        __syncthreads();
-        // forward: L y = P b (unit diagonal)
-        for (int r0 = 0; r0 < m; r0 += 32) {
-            const int nt = min(32, m - r0);
-            if (r0 > 0) {
-                for (int rr = warp; rr < nt; rr += NW) {
-                    const T *row = A + (size_t)(r0 + rr) * m;
-                    T s = 0;
-                    for (int j = lane; j < r0; j += 32) s += row[j] * y[j];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-                    if (lane == 0) y[r0 + rr] -= s;
+        for (int i = lane; i < m; i += 32) y[i] = (T)b[pm[i]];
+        __syncwarp();
+        // forward: L y = P b
+        for (int s = 0; s < slabs; ++s) {
+            const int r0 = 32 * s, nt = min(32, m - r0);
+            const T *S = A + (size_t)r0 * m;
+            const V *Sv = reinterpret_cast<const V *>(S);
+            const bool act = lane < nt;
+            T acc0 = 0, acc1 = 0;
+            if (act) {
+                const int groups = r0 / W;
+                int g = 0;
+                for (; g + 2 <= groups; g += 2) {
+                    const V a = Sv[(size_t)g * nt + lane], c = Sv[(size_t)(g + 1) * nt + lane];
+                    acc0 += SV::dot(a, y + g * W);
+                    acc1 += SV::dot(c, y + (g + 1) * W);
                 }
-                __syncthreads();
+                for (; g < groups; ++g) acc0 += SV::dot(Sv[(size_t)g * nt + lane], y + g * W);
             }
-            if (warp == 0) {
-                T yi = lane < nt ? y[r0 + lane] : T(0);
-                T L[32];
-                const T *row = A + (size_t)(r0 + min(lane, nt - 1)) * m + r0;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) L[j] = (j < lane && lane < nt) ? row[j] : T(0);
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const T yj = __shfl_sync(0xffffffffu, yi, j);
-                    if (j < nt) yi -= L[j] * yj;
-                }
-                if (lane < nt) y[r0 + lane] = yi;
+            T t = act ? y[r0 + lane] - (acc0 + acc1) : T(0);
+            for (int jj = 0; jj < nt; ++jj) {
+                const T l = (act && lane > jj) ? S[slab_at<T>(nt, lane, r0 + jj)] : T(0);
+                const T yj = __shfl_sync(0xffffffffu, t, jj);
+                t -= l * yj;
             }
-            __syncthreads();
+            if (act) y[r0 + lane] = t;
+            __syncwarp();
         }
         // backward: U z = y
-        const int last = ((m - 1) / 32) * 32;
-        for (int r0 = last; r0 >= 0; r0 -= 32) {
-            const int nt = min(32, m - r0), hi = r0 + nt;
-            if (hi < m) {
-                for (int rr = warp; rr < nt; rr += NW) {
-                    const T *row = A + (size_t)(r0 + rr) * m;
-                    T s = 0;
-                    for (int j = hi + lane; j < m; j += 32) s += row[j] * y[j];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-                    if (lane == 0) y[r0 + rr] -= s;
+        for (int s = slabs - 1; s >= 0; --s) {
+            const int r0 = 32 * s, nt = min(32, m - r0), hi = r0 + nt;
+            const T *S = A + (size_t)r0 * m;
+            const V *Sv = reinterpret_cast<const V *>(S);
+            const bool act = lane < nt;
+            T acc0 = 0, acc1 = 0;
+            if (act) {
+                const int g1 = m / W;
+                int g = hi / W;
+                for (; g + 2 <= g1; g += 2) {
+                    const V a = Sv[(size_t)g * nt + lane], c = Sv[(size_t)(g + 1) * nt + lane];
+                    acc0 += SV::dot(a, y + g * W);
+                    acc1 += SV::dot(c, y + (g + 1) * W);
                 }
-                __syncthreads();
+                for (; g < g1; ++g) acc0 += SV::dot(Sv[(size_t)g * nt + lane], y + g * W);
             }
-            if (warp == 0) {
-                T yi = lane < nt ? y[r0 + lane] : T(0);
-                T Ur[32];
-                const T *row = A + (size_t)(r0 + min(lane, nt - 1)) * m + r0;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) Ur[j] = (j >= lane && j < nt && lane < nt) ? row[j] : T(0);
-#pragma unroll
-                for (int j = 31; j >= 0; --j) {
-                    if (j < nt) {
-                        if (lane == j) yi = yi / Ur[j];
-                        const T yj = __shfl_sync(0xffffffffu, yi, j);
-                        if (lane < j) yi -= Ur[j] * yj;
-                    }
-                }
-                if (lane < nt) y[r0 + lane] = yi;
+            T t = act ? y[r0 + lane] - (acc0 + acc1) : T(0);
+            for (int jj = nt - 1; jj >= 0; --jj) {
+                const T u = act ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
+                if (lane == jj) t = t / u;
+                const T yj = __shfl_sync(0xffffffffu, t, jj);
+                if (lane < jj) t -= u * yj;
             }
-            __syncthreads();
+            if (act) y[r0 + lane] = t;
+            __syncwarp();
         }
-        for (int i = tid; i < m; i += LU_THREADS) z[(size_t)blk * m + i] = (double)y[i];
-        __syncthreads();
+        for (int i = lane; i < m; i += 32) z[(size_t)blk * m + i] = (double)y[i];
+        __syncwarp();
     }
 }
 
