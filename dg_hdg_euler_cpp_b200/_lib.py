@@ -104,6 +104,8 @@ SIGNATURES = {
     "dgh_newton_update": (ctypes.c_int, [_VP, ctypes.POINTER(dgh_update_stats)]),
     "dgh_newton_update_host": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(dgh_update_stats)]),
     "dgh_integrator_state": (_VP, [_VP]),
+    "dgh_residual_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            _VP, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),
 }
 
 _lib = None

@@ -186,6 +186,30 @@ int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_st
 /* Device pointer to the integrator's current Newton state (size dgh_sizes()[0]). */
 double *dgh_integrator_state(dgh_integrator *it);
 
+/* ---- Allocation-free residual ---------------------------------------------------------------
+ * No counterpart in the reference.  R(u) exactly as dgh_residual computes it, for callers that
+ * cannot allocate device memory: an allocation-free time loop, work issued while a stream is
+ * being captured into a CUDA graph (cudaMalloc is not permitted there), or a host that plans
+ * every byte of device memory itself.  It needs no context and allocates nothing (no cudaMalloc,
+ * no cudaFree, no allocating library call): its only scratch, the face restrictions of u
+ * (16 (k+1) doubles per cell), lives in a fixed device array of DGH_NOALLOC_TRACE_CAPACITY
+ * doubles (16 MiB) that every GPU loading this library holds until the process exits.
+ *  - Limit: nx * ny * 16 * (degree + 1) <= DGH_NOALLOC_TRACE_CAPACITY (e.g. 120 x 120 cells at
+ *    k = 8, 200 x 200 at k = 2); larger meshes return DGH_ERR_INVALID with the sizes in errbuf.
+ *  - Inputs u, old (stage base) and speeds (frozen (a, b) per face node, as dgh_speeds returns
+ *    them) and the output r are device pointers the caller owns; geometry follows testcase
+ *    (DGH_TEST_*) and gamma = 3.  Work is queued on stream (a cudaStream_t; NULL = default).
+ *  - The first call on a device looks up the scratch array's device address with that device
+ *    current; make that first call before any stream capture.
+ *  - Every call shares the one scratch array and the kernels overwrite all of it that they read,
+ *    so nothing needs clearing between calls; but calls whose work overlaps on the GPU (other
+ *    streams, other host threads) race on it and must be ordered by the caller.
+ *  - errbuf (may be NULL) receives a message of at most errbuf_len bytes on failure. */
+#define DGH_NOALLOC_TRACE_CAPACITY 2097152
+int dgh_residual_noalloc(int nx, int ny, int degree, int testcase, double step_size, const double *u,
+                         const double *old, const double *speeds, double *r, void *stream, char *errbuf,
+                         int errbuf_len);
+
 #ifdef __cplusplus
 }
 #endif
