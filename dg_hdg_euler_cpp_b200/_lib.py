@@ -40,6 +40,14 @@ class dgh_update_stats(ctypes.Structure):
     ]
 
 
+class dgh_adjoint_stats(ctypes.Structure):
+    _fields_ = [
+        ("objective", ctypes.c_double), ("final_time", ctypes.c_double), ("steps", ctypes.c_int),
+        ("checkpoints", ctypes.c_int), ("forward_newton", ctypes.c_int), ("adjoint_krylov", ctypes.c_int),
+        ("recomputed_steps", ctypes.c_int),
+    ]
+
+
 class dgh_run_stats(ctypes.Structure):
     _fields_ = [
         ("final_time", ctypes.c_double), ("conservation_drift", ctypes.c_double), ("seconds", ctypes.c_double),
@@ -83,9 +91,14 @@ SIGNATURES = {
     "dgh_integral": (ctypes.c_int, [_VP, _VP, _D]),
     "dgh_l2_error": (ctypes.c_int, [_VP, _VP, ctypes.c_double, _D]),
     "dgh_speeds": (ctypes.c_int, [_VP, _D]),
+    "dgh_copy_speeds": (ctypes.c_int, [_VP, _VP]),
+    "dgh_set_speeds": (ctypes.c_int, [_VP, _VP]),
+    "dgh_mass_axpby": (ctypes.c_int, [_VP, ctypes.c_double, _VP, ctypes.c_double, _VP, _VP]),
+    "dgh_rho2": (ctypes.c_int, [_VP, _VP, _D, _VP]),
     "dgh_dg_refresh": (ctypes.c_int, [_VP, _VP]),
     "dgh_dg_apply": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_dg_block": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "dgh_dg_apply_T": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_block_jacobi_refresh": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dgh_precond_apply": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP]),
     "dgh_hdg_refresh_projected": (ctypes.c_int, [_VP, _VP, _VP]),
@@ -104,6 +117,8 @@ SIGNATURES = {
     "dgh_newton_update": (ctypes.c_int, [_VP, ctypes.POINTER(dgh_update_stats)]),
     "dgh_newton_update_host": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(dgh_update_stats)]),
     "dgh_integrator_state": (_VP, [_VP]),
+    "dgh_dirk3_adjoint": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.POINTER(dgh_adjoint_stats)]),
+    "dgh_dirk3_replay": (ctypes.c_int, [_VP, _VP, _D]),
     "dgh_residual_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             _VP, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),
 }

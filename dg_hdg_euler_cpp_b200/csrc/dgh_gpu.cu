@@ -103,7 +103,7 @@ struct dgh_ctx {
     void *face_pool = nullptr;
     int *face_perm = nullptr;
     // GMRES
-    double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[2] = {nullptr, nullptr}, *gcoef = nullptr;
+    double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[3] = {nullptr, nullptr, nullptr}, *gcoef = nullptr;
     long long vld = 0;
     // optional CUDA-event timers per kernel class (dgh_timing_enable / dgh_timing_read)
     struct TimerRec { int cat; cudaEvent_t a, b; };
@@ -277,8 +277,28 @@ void launch_solve(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, in
     c->launched();
 }
 
+template <typename TF>
+void launch_solve_t(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
+                    double *z) {
+    constexpr int wpc = SOLVE_THREADS / 32;
+    const size_t smem = sizeof(TF) * (size_t)m * wpc;
+    const int want = (count + wpc - 1) / wpc;
+    int resident = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve_t<TF>, SOLVE_THREADS, smem), "occupancy");
+    const int grid = std::min(want, c->sms * std::max(1, resident));
+    k_lu_solve_t<TF><<<grid, SOLVE_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
+    c->launched();
+}
+
 void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     Timed tm(c, DGH_TIMER_PRECOND);
+    if (op == DGH_OP_DG_T) {
+        need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
+        const size_t stride = (size_t)c->m * c->m;
+        if (c->mixed()) launch_solve_t<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+        else launch_solve_t<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+        return;
+    }
     if (op == DGH_OP_DG) {
         need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->m * c->m;
@@ -302,6 +322,17 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
     });
     c->launched();
 }
+void dg_apply_t(dgh_ctx *c, const double *w, double *out) {
+    need(c->linearised, "Refresh the volume Jacobian before applying it");
+    launch_trace(c, w, c->traces2, false);
+    DGH_DISPATCH_N(c->n, {
+        using T = Team<N>;
+        k_dg_apply_t<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(w, c->traces2, c->vol, c->fcache,
+                                                                              c->speeds, out, c->basis, c->g,
+                                                                              c->inv_step);
+    });
+    c->launched();
+}
 void hdg_apply(dgh_ctx *c, const double *lam, double *out) {
     need(c->condensed, "Condense the HDG operator before applying it");
     DGH_DISPATCH_N(c->n, { k_hdg_apply<N><<<c->faces, 256, 0, c->stream>>>(c->S, c->speeds, lam, out, c->basis, c->g); });
@@ -310,6 +341,7 @@ void hdg_apply(dgh_ctx *c, const double *lam, double *out) {
 void op_apply(dgh_ctx *c, int op, const double *x, double *y) {
     Timed tm(c, DGH_TIMER_OPERATOR);
     if (op == DGH_OP_DG) dg_apply(c, x, y);
+    else if (op == DGH_OP_DG_T) dg_apply_t(c, x, y);
     else hdg_apply(c, x, y);
 }
 
@@ -370,8 +402,8 @@ void axpby(dgh_ctx *c, double a, const double *x, double b, const double *y, dou
 
 // gmres.cpp:17-86 with the CGS2 passes fused as dot | axpy+dot | axpy+norm.
 void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
-    const long long n = op == DGH_OP_DG ? c->N : c->NT;
-    const double *W = op == DGH_OP_DG ? c->inv_mass : c->inv_trace_mass;
+    const long long n = op == DGH_OP_HDG ? c->NT : c->N;
+    const double *W = op == DGH_OP_HDG ? c->inv_trace_mass : c->inv_mass;
     const int restart = (int)std::min<long long>(n, c->cfg.restart);
     double *r = c->gres[op], *w = c->gw, *z = c->gz, *V = c->V;
     const size_t ld = (size_t)c->vld;
@@ -636,7 +668,10 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->V = c->alloc<double>((size_t)c->vld * (k.restart + 1));
         c->gw = c->alloc<double>(vn);
         c->gz = c->alloc<double>(vn);
-        if (c->has_dg()) c->gres[DGH_OP_DG] = c->alloc<double>(c->N);
+        if (c->has_dg()) {
+            c->gres[DGH_OP_DG] = c->alloc<double>(c->N);
+            c->gres[DGH_OP_DG_T] = c->alloc<double>(c->N);
+        }
         if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
         c->gcoef = c->alloc<double>(KR_MAXK);
         c->sync();
@@ -878,6 +913,37 @@ int dgh_l2_error(dgh_ctx *c, const double *u, double time, double out[4]) {
     });
 }
 
+int dgh_copy_speeds(dgh_ctx *c, double *dev_ab) {
+    return guard(c, [&] {
+        need(c->frozen, "Freeze the wave speeds first");
+        ck(cudaMemcpyAsync(dev_ab, c->speeds, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                           c->stream), "copy");
+    });
+}
+int dgh_set_speeds(dgh_ctx *c, const double *dev_ab) {
+    return guard(c, [&] {
+        ck(cudaMemcpyAsync(c->speeds, dev_ab, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                           c->stream), "copy");
+        c->frozen = true;
+        c->linearised = c->dg_factored = c->condensed = c->face_factored = false;
+    });
+}
+int dgh_mass_axpby(dgh_ctx *c, double a, const double *x, double b, const double *y, double *out) {
+    return guard(c, [&] {
+        k_mass_axpby<<<c->red_grid, KR_THREADS, 0, c->stream>>>(a, x, c->mass, b, y, out, c->N);
+        c->launched();
+    });
+}
+int dgh_rho2(dgh_ctx *c, const double *u, double *value, double *grad) {
+    return guard(c, [&] {
+        k_rho2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(u, c->mass, c->P, c->N, grad, c->partial);
+        k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, c->red);
+        c->launched(2);
+        ck(cudaMemcpyAsync(c->pinned, c->red, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        *value = c->pinned[0];
+    });
+}
 int dgh_speeds(dgh_ctx *c, double *host_ab) {
     return guard(c, [&] {
         ck(cudaMemcpyAsync(host_ab, c->speeds, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToHost,
@@ -909,6 +975,9 @@ int dgh_dg_refresh(dgh_ctx *c, const double *u) {
 }
 int dgh_dg_apply(dgh_ctx *c, const double *v, double *jv) {
     return guard(c, [&] { dg_apply(c, v, jv); });
+}
+int dgh_dg_apply_T(dgh_ctx *c, const double *w, double *jtw) {
+    return guard(c, [&] { dg_apply_t(c, w, jtw); });
 }
 int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
     return guard(c, [&] {
@@ -1064,7 +1133,8 @@ int dgh_hdg_recovered_residual(dgh_ctx *c, const double *e, double *out) {
 // ---- GMRES -------------------------------------------------------------------------------------------
 int dgh_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int *iterations, double *relative) {
     return guard(c, [&] {
-        need(op == DGH_OP_DG ? c->has_dg() : c->has_hdg(), "context lacks the requested operator");
+        need(op >= 0 && op <= 2, "Invalid operator");
+        need(op == DGH_OP_HDG ? c->has_hdg() : c->has_dg(), "context lacks the requested operator");
         int it = 0;
         double rel = 0;
         try {
@@ -1078,7 +1148,7 @@ int dgh_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, doubl
     });
 }
 const double *dgh_gmres_residual(dgh_ctx *c, int op) {
-    if (!c || (op != 0 && op != 1)) return nullptr;
+    if (!c || op < 0 || op > 2) return nullptr;
     return c->gres[op];
 }
 

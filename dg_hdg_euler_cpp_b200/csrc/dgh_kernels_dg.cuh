@@ -300,6 +300,88 @@ k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const d
     }
 }
 
+// ---- adjoint J^T w (the transpose of k_dg_apply, same frozen speeds and caches) -------------
+// Volume: for node (a, b), gx = sum_i dw[a n + i] w(i, b) and gy = sum_j dw[b n + j] w(a, j);
+// (J^T w)(a, b) = M w / tau - (hy/2) w_b Ax^T gx - (hx/2) w_a Ay^T gy.  Faces: with the jump
+// z = E_right-side w_L - E_left-side w_R of the two cells sharing a face, the left cell receives
+// lift((blend_l A_L + pen I)^T z) and the right cell lift((blend_r A_R - pen I)^T z).
+// Needs the face traces of w (k_face_trace on w).
+template <int N>
+__global__ void __launch_bounds__(Team<N>::THREADS)
+k_dg_apply_t(const double *__restrict__ w, const double *__restrict__ wtr, const double *__restrict__ vol,
+             const double *__restrict__ fcache, const double *__restrict__ speeds, double *__restrict__ out,
+             Basis1D b, Grid g, double inv_step) {
+    using T = Team<N>;
+    __shared__ double ws[T::CPB][NVAR * T::P];
+    __shared__ double ff[T::CPB][NFACES * N * NVAR];
+    const int sub = threadIdx.x / T::TPC, lt = threadIdx.x % T::TPC;
+    const int cell = blockIdx.x * T::CPB + sub;
+    const bool active = cell < g.cells;
+    const size_t base = (size_t)cell * NVAR * T::P;
+    if (active)
+        for (int k = lt; k < NVAR * T::P; k += T::TPC) ws[sub][k] = w[base + k];
+    if (active)
+        for (int k = lt; k < NFACES * N; k += T::TPC) {
+            const int side = k / N, q = k % N, axis = side / 2;
+            const int nb = neighbor(g, cell, side), face = face_of(g, cell, side);
+            const double *own = wtr + ((size_t)cell * NFACES + side) * N * NVAR + q * NVAR;
+            const double *oth = wtr + ((size_t)nb * NFACES + (side ^ 1)) * N * NVAR + q * NVAR;
+            double z[4];
+#pragma unroll
+            for (int v = 0; v < NVAR; ++v) z[v] = side % 2 ? own[v] - oth[v] : oth[v] - own[v];
+            const bool left = side % 2;
+            const double *c = fcache + ((size_t)face * N + q) * 8;
+            const double sa = speeds[2 * (face * N + q)], sb = speeds[2 * (face * N + q) + 1];
+            const double pen = face_weight(g, b, face, q) * sa * sb / (sa + sb);
+            double a[16];
+            if (left) cached_jacobian(g.gamma, c[0], c[1], c[2], axis, a);
+            else cached_jacobian(g.gamma, c[3], c[4], c[5], axis, a);
+            const double blend = left ? c[6] : c[7], sp = left ? pen : -pen;
+#pragma unroll
+            for (int ww = 0; ww < NVAR; ++ww) {
+                double s = 0;
+#pragma unroll
+                for (int v = 0; v < NVAR; ++v) s += a[v * 4 + ww] * z[v];
+                ff[sub][k * NVAR + ww] = blend * s + sp * z[ww];
+            }
+        }
+    __syncthreads();
+    if (!active || lt >= T::P) return;
+    const int ix = lt % N, iy = lt / N;
+    const double mass = .25 * g.hx * g.hy * b.w[ix] * b.w[iy];
+    const double sx = .5 * g.hy, sy = .5 * g.hx;
+    double gx[4], gy[4];
+#pragma unroll
+    for (int v = 0; v < NVAR; ++v) {
+        double x = 0, y = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            x += b.dw[ix * N + i] * ws[sub][v * T::P + i + N * iy];
+            y += b.dw[iy * N + i] * ws[sub][v * T::P + ix + N * i];
+        }
+        gx[v] = x;
+        gy[v] = y;
+    }
+    const double *c = vol + ((size_t)cell * T::P + lt) * 3;
+    double ax[16], ay[16];
+    cached_jacobian(g.gamma, c[0], c[1], c[2], 0, ax);
+    cached_jacobian(g.gamma, c[0], c[1], c[2], 1, ay);
+#pragma unroll
+    for (int ww = 0; ww < NVAR; ++ww) {
+        double tx = 0, ty = 0;
+#pragma unroll
+        for (int v = 0; v < NVAR; ++v) {
+            tx += ax[v * 4 + ww] * gx[v];
+            ty += ay[v * 4 + ww] * gy[v];
+        }
+        double val = mass * ws[sub][ww * T::P + lt] * inv_step;
+        if (N > 1) val -= sx * b.w[iy] * tx + sy * b.w[ix] * ty;
+        val += b.eL[ix] * ff[sub][(0 * N + iy) * NVAR + ww] + b.eR[ix] * ff[sub][(1 * N + iy) * NVAR + ww] +
+               b.eL[iy] * ff[sub][(2 * N + ix) * NVAR + ww] + b.eR[iy] * ff[sub][(3 * N + ix) * NVAR + ww];
+        out[base + ww * T::P + lt] = val;
+    }
+}
+
 // ---- per-cell Jacobian tables used by the block assemblies ---------------------------------
 // jx/jy[node*16 + v*4 + w]: physical flux Jacobians at the nodes; fj[(side*N+q)*16 + v*4 + w]:
 // the face derivative per side (HLL self-coupling for DG with its lift sign, or the HDG

@@ -139,4 +139,25 @@ k_wnorm2(const double *__restrict__ x, const double *__restrict__ W, int divide,
     block_reduce_store<1>(acc, 1, partial, gridDim.x);
 }
 
+// out = a * M x + b * y  (M the diagonal mass matrix)
+__global__ void k_mass_axpby(double a, const double *x, const double *mass, double b, const double *y, double *out,
+                             long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = a * (mass[i] * x[i]) + b * y[i];
+}
+
+// Objective sum M rho^2 over the density sheets (partials) and its gradient 2 M rho (0 elsewhere).
+__global__ void __launch_bounds__(KR_THREADS)
+k_rho2(const double *__restrict__ u, const double *__restrict__ mass, int plane, long long n, double *__restrict__ grad,
+       double *__restrict__ partial) {
+    double acc[1] = {0};
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+        const bool rho = ((i / plane) % 4) == 0;
+        const double v = rho ? u[i] : 0.;
+        acc[0] += mass[i] * v * v;
+        if (grad) grad[i] = 2. * mass[i] * v;
+    }
+    block_reduce_store<1>(acc, 1, partial, gridDim.x);
+}
+
 }  // namespace dgh

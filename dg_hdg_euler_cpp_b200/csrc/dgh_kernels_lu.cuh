@@ -371,6 +371,92 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
     }
 }
 
+// Transposed block solve z = A^{-T} b with the same slab-layout factors (A = P^T L U, so
+// A^{-T} b = P^T L^{-T} U^{-T} b): a forward solve with U^T (lower, with U's diagonal), a
+// backward solve with L^T (unit upper), then the scatter z[perm[i]] = x[i].  Slab s holds rows
+// 32s.. of U and L; once a slab's unknowns are final, its rows are applied to the remaining
+// unknowns with each lane owning one 16-byte column group (no CTA barriers, one warp per block).
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS)
+k_lu_solve_t(const T *__restrict__ pool, const int *__restrict__ perm, size_t stride, int m, int count,
+             const double *__restrict__ rhs, double *__restrict__ z) {
+    using SV = SlabVec<T>;
+    using V = typename SV::V;
+    constexpr int W = SV::W;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    T *y = reinterpret_cast<T *>(smraw) + (size_t)wib * m;
+    const int warps = gridDim.x * (SOLVE_THREADS / 32);
+    const int slabs = (m + 31) / 32;
+    for (int blk = blockIdx.x * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
+        const T *A = pool + (size_t)blk * stride;
+        const int *pm = perm + (size_t)blk * m;
+        const double *b = rhs + (size_t)blk * m;
+        for (int i = lane; i < m; i += 32) y[i] = (T)b[i];
+        __syncwarp();
+        // U^T y = b, forward by slabs
+        for (int s = 0; s < slabs; ++s) {
+            const int r0 = 32 * s, nt = min(32, m - r0), hi = r0 + nt;
+            const T *S = A + (size_t)r0 * m;
+            T t = lane < nt ? y[r0 + lane] : T(0);
+            for (int jj = 0; jj < nt; ++jj) {
+                const T d = lane == jj ? S[slab_at<T>(nt, jj, r0 + jj)] : T(1);
+                if (lane == jj) t = t / d;
+                const T yj = __shfl_sync(0xffffffffu, t, jj);
+                // U^T[r0+lane][r0+jj] = U[r0+jj][r0+lane], nonzero for lane > jj
+                if (lane > jj && lane < nt) t -= S[slab_at<T>(nt, jj, r0 + lane)] * yj;
+            }
+            if (lane < nt) y[r0 + lane] = t;
+            __syncwarp();
+            for (int g = hi / W + lane; g < m / W; g += 32) {
+                T acc[W];
+#pragma unroll
+                for (int e = 0; e < W; ++e) acc[e] = 0;
+                for (int i = 0; i < nt; ++i) {
+                    const V v = reinterpret_cast<const V *>(S)[(size_t)g * nt + i];
+                    const T yi = y[r0 + i];
+                    const T *vv = reinterpret_cast<const T *>(&v);
+#pragma unroll
+                    for (int e = 0; e < W; ++e) acc[e] += vv[e] * yi;
+                }
+#pragma unroll
+                for (int e = 0; e < W; ++e) y[g * W + e] -= acc[e];
+            }
+            __syncwarp();
+        }
+        // L^T x = y (unit upper), backward by slabs
+        for (int s = slabs - 1; s >= 0; --s) {
+            const int r0 = 32 * s, nt = min(32, m - r0);
+            const T *S = A + (size_t)r0 * m;
+            T t = lane < nt ? y[r0 + lane] : T(0);
+            for (int jj = nt - 1; jj >= 0; --jj) {
+                const T yj = __shfl_sync(0xffffffffu, t, jj);
+                // L^T[r0+lane][r0+jj] = L[r0+jj][r0+lane], nonzero for lane < jj
+                if (lane < jj) t -= S[slab_at<T>(nt, jj, r0 + lane)] * yj;
+            }
+            if (lane < nt) y[r0 + lane] = t;
+            __syncwarp();
+            for (int g = lane; g < r0 / W; g += 32) {
+                T acc[W];
+#pragma unroll
+                for (int e = 0; e < W; ++e) acc[e] = 0;
+                for (int i = 0; i < nt; ++i) {
+                    const V v = reinterpret_cast<const V *>(S)[(size_t)g * nt + i];
+                    const T yi = y[r0 + i];
+                    const T *vv = reinterpret_cast<const T *>(&v);
+#pragma unroll
+                    for (int e = 0; e < W; ++e) acc[e] += vv[e] * yi;
+                }
+#pragma unroll
+                for (int e = 0; e < W; ++e) y[g * W + e] -= acc[e];
+            }
+            __syncwarp();
+        }
+        for (int i = lane; i < m; i += 32) z[(size_t)blk * m + pm[i]] = (double)y[i];
+        __syncwarp();
+    }
+}
+
 // Multi-RHS back substitution U X = Y in place on columns [m, ld) of each factored matrix.
 // Row tiles of 32 from the bottom; RHS tiles of 64 columns.  Per tile: Y_I -= U_{I,>I} X_{>I}
 // staged through shared memory in chunks of 32, then a column-parallel 32x32 triangular solve.

@@ -36,6 +36,18 @@ struct dgh_integrator {
     int stage = 0, steps_done = 0, stages = 1;
     bool residual_ready = false;
     dgh_run_stats run{};
+    // discrete adjoint: recorded trajectory (dt per step, frozen speeds per stage, checkpoints)
+    struct Adjoint {
+        int steps = 0, every = 0, stages = 0;
+        int64_t sz = 0;  // doubles of one speeds record
+        std::vector<double> dt;
+        double *speeds = nullptr;           // [steps][stages][sz]
+        std::vector<double *> checkpoints;  // U^n for n % every == 0
+        std::vector<double *> stage_states; // [every][stages]
+        double *ubar = nullptr, *ubs = nullptr, *psi = nullptr, *kbar[4] = {nullptr, nullptr, nullptr, nullptr};
+        double *u = nullptr, *step = nullptr;
+        int forward_newton = 0, adjoint_krylov = 0, recomputed = 0;
+    } adj;
 
     void ck(int rc) {
         if (rc != DGH_OK) throw Failure{rc, dgh_last_error(ctx)};
@@ -381,4 +393,180 @@ int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_st
     });
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Discrete adjoint of SSP-DIRK(4,3) (or backward Euler) for the DG solve, with the step sizes and
+// the frozen wave speeds of the recorded forward trajectory held fixed (they are non-smooth
+// functions of the state: dt = CFL / max(...), Einfeldt bounds with max()).  For stage s,
+// R(U_s) = M (U_s - U_b,s)/tau_s - L(U_s) = 0 and K_s = (U_s - U_b,s)/tau_s, so with
+// psi = J_s^{-T} Kbar_s the stage base receives Ubar_b,s = (M psi / tau_s - Kbar_s) / tau_s, where
+// Kbar_s = dt b_s Ubar^{n+1} + sum_{r>s} dt a_rs Ubar_b,r and Ubar^n = Ubar^{n+1} + sum_s Ubar_b,s.
+// J_s^T solves use GMRES on the adjoint operator with the transposed block-Jacobi factors.
+namespace {
+// One stage's Newton solve to the nonlinear tolerance (time_integrator.cpp:133-142 without the
+// statistics); returns the number of updates.
+int newton_stage(dgh_integrator *it) {
+    const dgh_config &c = it->cfg;
+    it->initial_rms = -1.;
+    it->residual_ready = false;
+    int updates = 0;
+    for (int k = 0; k <= c.max_newton; ++k) {
+        double rms = 0;
+        const double norm = it->prepare(rms);
+        if (rms <= c.nonlinear_tolerance * std::max(1., it->initial_rms)) return updates;
+        if (k == c.max_newton) break;
+        dgh_update_stats u{};
+        it->update(norm, rms, k, u);
+        ++updates;
+    }
+    throw Failure{DGH_ERR_SOLVER, "Newton iteration limit reached"};
+}
+
+// Forward DIRK3/BE from `u` over steps [first, last): records dt and speeds when `record`,
+// replays them otherwise; stores stage solutions into adj.stage_states when `keep`.
+void forward(dgh_integrator *it, double *u, int first, int last, bool record, bool keep, bool checkpoint) {
+    auto &a = it->adj;
+    dgh_ctx *ctx = it->ctx;
+    const int64_t N = it->N;
+    const int S = a.stages;
+    for (int n = first; n < last; ++n) {
+        if (checkpoint && n % a.every == 0) it->ck(dgh_axpby(ctx, 1., u, 0., u, a.checkpoints[n / a.every], N));
+        double dt;
+        if (record) {
+            double rate = 0;
+            it->ck(dgh_freeze(ctx, u, &rate));
+            dt = it->cfg.cfl / rate;
+            a.dt[n] = dt;
+            it->ck(dgh_copy_speeds(ctx, a.speeds + ((size_t)n * S) * a.sz));
+        } else {
+            dt = a.dt[n];
+            it->ck(dgh_set_speeds(ctx, a.speeds + ((size_t)n * S) * a.sz));
+        }
+        it->ck(dgh_axpby(ctx, 1., u, 0., u, it->step_state, N));
+        it->ck(dgh_axpby(ctx, 1., u, 0., u, it->state, N));
+        for (int s = 0; s < S; ++s) {
+            const double diag = S == 1 ? 1. : kA[s][s];
+            it->ck(dgh_axpby(ctx, 1., it->step_state, 0., it->step_state, it->stage_base, N));
+            for (int j = 0; j < s; ++j)
+                it->ck(dgh_axpby(ctx, 1., it->stage_base, dt * kA[s][j], it->slopes[j], it->stage_base, N));
+            if (s > 0) {
+                if (record) {
+                    double unused = 0;
+                    it->ck(dgh_freeze(ctx, it->state, &unused));
+                    it->ck(dgh_copy_speeds(ctx, a.speeds + ((size_t)n * S + s) * a.sz));
+                } else {
+                    it->ck(dgh_set_speeds(ctx, a.speeds + ((size_t)n * S + s) * a.sz));
+                }
+            }
+            it->ck(dgh_set_stage(ctx, it->stage_base, diag * dt));
+            it->tau = diag * dt;
+            it->old_norm = it->snorm(it->stage_base);
+            a.forward_newton += newton_stage(it);
+            if (keep) it->ck(dgh_axpby(ctx, 1., it->state, 0., it->state, a.stage_states[(n - first) * S + s], N));
+            it->ck(dgh_axpby(ctx, 1. / it->tau, it->state, -1. / it->tau, it->stage_base, it->slopes[s], N));
+        }
+        it->ck(dgh_axpby(ctx, 1., it->step_state, 0., it->step_state, u, N));
+        for (int s = 0; s < S; ++s) {
+            const double bs = S == 1 ? 1. : kB[s];
+            it->ck(dgh_axpby(ctx, 1., u, dt * bs, it->slopes[s], u, N));
+        }
+    }
+}
+
+void prepare_adjoint(dgh_integrator *it, int steps, int every) {
+    auto &a = it->adj;
+    if (a.steps == steps && a.every == every && a.speeds) return;
+    int64_t s8[8];
+    it->ck(dgh_sizes(it->ctx, s8));
+    a.steps = steps;
+    a.every = every;
+    a.stages = it->cfg.integrator == DGH_INTEGRATOR_BE ? 1 : 4;
+    a.sz = 2 * s8[4] * s8[5];
+    a.dt.assign(steps, 0.);
+    a.speeds = it->vec((int64_t)steps * a.stages * a.sz);
+    a.checkpoints.clear();
+    for (int k = 0; k < (steps + every - 1) / every; ++k) a.checkpoints.push_back(it->vec(it->N));
+    a.stage_states.clear();
+    for (int k = 0; k < every * a.stages; ++k) a.stage_states.push_back(it->vec(it->N));
+    a.ubar = it->vec(it->N);
+    a.ubs = it->vec(it->N);
+    a.psi = it->vec(it->N);
+    for (auto &p : a.kbar) p = it->vec(it->N);
+    a.u = it->vec(it->N);
+    a.step = it->vec(it->N);
+}
+}  // namespace
+
+extern "C" {
+int dgh_dirk3_adjoint(dgh_integrator *it, int steps, int checkpoint_every, const double *host_u0, double *host_grad,
+                      dgh_adjoint_stats *stats) {
+    return guarded(it, [&] {
+        if (it->method != DGH_METHOD_DG) throw Failure{DGH_ERR_INVALID, "The discrete adjoint runs on the DG operator"};
+        if (steps <= 0 || checkpoint_every <= 0) throw Failure{DGH_ERR_INVALID, "Invalid step or checkpoint count"};
+        prepare_adjoint(it, steps, checkpoint_every);
+        auto &a = it->adj;
+        dgh_ctx *ctx = it->ctx;
+        const int64_t N = it->N;
+        const int S = a.stages;
+        a.forward_newton = a.adjoint_krylov = a.recomputed = 0;
+        it->ck(dgh_upload(ctx, a.u, host_u0, N));
+        forward(it, a.u, 0, steps, true, false, true);
+        double objective = 0;
+        it->ck(dgh_rho2(ctx, a.u, &objective, a.ubar));
+        double final_time = 0;
+        for (double d : a.dt) final_time += d;
+        const int segments = (steps + checkpoint_every - 1) / checkpoint_every;
+        for (int seg = segments - 1; seg >= 0; --seg) {
+            const int c0 = seg * checkpoint_every, c1 = std::min(steps, c0 + checkpoint_every);
+            it->ck(dgh_axpby(ctx, 1., a.checkpoints[seg], 0., a.checkpoints[seg], a.step, N));
+            forward(it, a.step, c0, c1, false, true, false);  // recompute the segment's stage states
+            a.recomputed += c1 - c0;
+            for (int n = c1 - 1; n >= c0; --n) {
+                const double dt = a.dt[n];
+                for (int s = 0; s < S; ++s) {
+                    const double bs = S == 1 ? 1. : kB[s];
+                    it->ck(dgh_axpby(ctx, dt * bs, a.ubar, 0., a.ubar, a.kbar[s], N));
+                }
+                for (int s = S - 1; s >= 0; --s) {
+                    const double tau = (S == 1 ? 1. : kA[s][s]) * dt;
+                    double *us = a.stage_states[(n - c0) * S + s];
+                    it->ck(dgh_set_speeds(ctx, a.speeds + ((size_t)n * S + s) * a.sz));
+                    it->ck(dgh_set_stage(ctx, us, tau));
+                    it->ck(dgh_dg_refresh(ctx, us));
+                    it->ck(dgh_block_jacobi_refresh(ctx, DGH_OP_DG));
+                    int iters = 0;
+                    double rel = 0;
+                    it->ck(dgh_gmres(ctx, DGH_OP_DG_T, a.kbar[s], a.psi, it->cfg.max_linear, it->cfg.linear_tolerance,
+                                     &iters, &rel));
+                    a.adjoint_krylov += iters;
+                    it->ck(dgh_mass_axpby(ctx, 1. / (tau * tau), a.psi, -1. / tau, a.kbar[s], a.ubs));
+                    it->ck(dgh_axpby(ctx, 1., a.ubar, 1., a.ubs, a.ubar, N));
+                    for (int j = 0; j < s; ++j)
+                        it->ck(dgh_axpby(ctx, 1., a.kbar[j], dt * kA[s][j], a.ubs, a.kbar[j], N));
+                }
+            }
+        }
+        it->ck(dgh_download(ctx, host_grad, a.ubar, N));
+        if (stats) {
+            stats->objective = objective;
+            stats->final_time = final_time;
+            stats->steps = steps;
+            stats->checkpoints = segments;
+            stats->forward_newton = a.forward_newton;
+            stats->adjoint_krylov = a.adjoint_krylov;
+            stats->recomputed_steps = a.recomputed;
+        }
+    });
+}
+
+int dgh_dirk3_replay(dgh_integrator *it, const double *host_u0, double *objective) {
+    return guarded(it, [&] {
+        auto &a = it->adj;
+        if (!a.speeds) throw Failure{DGH_ERR_INVALID, "Run dgh_dirk3_adjoint first to record a trajectory"};
+        it->ck(dgh_upload(it->ctx, a.u, host_u0, it->N));
+        forward(it, a.u, 0, a.steps, false, false, false);
+        it->ck(dgh_rho2(it->ctx, a.u, objective, nullptr));
+    });
+}
 }  // extern "C"

@@ -19,7 +19,7 @@ METHODS = {"dg": 0, "hdg": 1, "both": 2}
 INTEGRATORS = {"ssp-dirk3": 0, "be": 1}
 TESTCASES = {"diagonal": 0, "wave": 1, "axis": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
-OPS = {"dg": 0, "hdg": 1}
+OPS = {"dg": 0, "hdg": 1, "dg_t": 2}
 
 
 class DGHError(RuntimeError):
@@ -180,6 +180,11 @@ class Solver:
         self._call("dgh_dg_apply", _ptr(v), _ptr(out))
         return out
 
+    def dg_apply_T(self, w):
+        out = self.vec()
+        self._call("dgh_dg_apply_T", _ptr(w), _ptr(out))
+        return out
+
     def dg_block(self, row: int, col: int) -> np.ndarray:
         out = np.zeros(self.block * self.block)
         self._call("dgh_dg_block", row, col, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
@@ -190,7 +195,7 @@ class Solver:
         self._call("dgh_block_jacobi_refresh", OPS[op])
 
     def precond_apply(self, op: str, x):
-        z = self.vec(self.size if op == "dg" else self.trace_size)
+        z = self.vec(self.trace_size if op == "hdg" else self.size)
         self._call("dgh_precond_apply", OPS[op], _ptr(x), _ptr(z))
         return z
 
@@ -227,7 +232,7 @@ class Solver:
     # ---- GMRES
     def gmres(self, op: str, rhs, limit: int, tol: float):
         """Returns (x, iterations, relative residual, true residual)."""
-        x = self.vec(self.size if op == "dg" else self.trace_size)
+        x = self.vec(self.trace_size if op == "hdg" else self.size)
         it, rel = ctypes.c_int(), ctypes.c_double()
         self._call("dgh_gmres", OPS[op], _ptr(rhs), _ptr(x), limit, ctypes.c_double(tol), ctypes.byref(it),
                    ctypes.byref(rel))

@@ -52,7 +52,9 @@ enum { DGH_TEST_DIAGONAL = 0, DGH_TEST_WAVE = 1, DGH_TEST_AXIS = 2 };
 /* Precision of the block-Jacobi factors and their solves.  Residuals, J*v, the Schur apply,
  * the HDG condensation, Arnoldi and the least-squares problem are always FP64. */
 enum { DGH_PRECISION_FP64 = 0, DGH_PRECISION_MIXED = 1 };
-enum { DGH_OP_DG = 0, DGH_OP_HDG = 1 };
+/* Operators for the preconditioner and GMRES: the DG Jacobian J, the condensed Schur operator,
+ * and the DG adjoint J^T (with the transposed block-Jacobi preconditioner). */
+enum { DGH_OP_DG = 0, DGH_OP_HDG = 1, DGH_OP_DG_T = 2 };
 
 /* config.hpp:7-18 plus the precision and the operators to allocate. */
 typedef struct dgh_config {
@@ -125,16 +127,28 @@ int dgh_state_norm(dgh_ctx *ctx, const double *u, double *out);    /* sqrt(u^T M
 int dgh_integral(dgh_ctx *ctx, const double *u, double out[4]);    /* discretization.cpp:237-243 */
 int dgh_l2_error(dgh_ctx *ctx, const double *u, double time, double out[4]); /* initial_and_error.cpp:55-73 */
 int dgh_speeds(dgh_ctx *ctx, double *host_ab);                     /* frozen (a,b) per face node */
+/* Device copies of the frozen speeds, and replaying recorded ones (they replace Problem::freeze's
+ * speeds without touching old/step; used to hold the speeds fixed in the discrete adjoint). */
+int dgh_copy_speeds(dgh_ctx *ctx, double *dev_ab);
+int dgh_set_speeds(dgh_ctx *ctx, const double *dev_ab);
+/* out = a M x + b y with the diagonal mass matrix (discretization.cpp:9-13). */
+int dgh_mass_axpby(dgh_ctx *ctx, double a, const double *x, double b, const double *y, double *out);
+/* value = sum over nodes of M rho^2 (the adjoint objective); grad (may be NULL) = 2 M rho. */
+int dgh_rho2(dgh_ctx *ctx, const double *u, double *value, double *grad);
 
 /* ---- DGOperator (dg_operator.hpp:5-17) ------------------------------------------------------ */
 int dgh_dg_refresh(dgh_ctx *ctx, const double *u);                 /* dg_operator.cpp:6-9 */
 int dgh_dg_apply(dgh_ctx *ctx, const double *v, double *jv);       /* dg_operator.cpp:10-21 */
+/* Adjoint J^T w of the DG residual's Jacobian at the same linearisation (no counterpart in the
+ * reference: the transpose of dg_operator.cpp:10-21 and volume_jacobian.cpp:59-71). */
+int dgh_dg_apply_T(dgh_ctx *ctx, const double *w, double *jtw);
 /* Diagonal block (row == col), copied to the host row-major m x m (dg_operator.cpp:22-48). */
 int dgh_dg_block(dgh_ctx *ctx, int row, int col, double *host_block);
 
 /* ---- BlockJacobi (block_jacobi.hpp:7-47) ---------------------------------------------------- */
 /* op DGH_OP_DG: assemble and factor the E cell blocks from the current DG linearisation;
- * op DGH_OP_HDG: the 2E face blocks of the current condensed operator. */
+ * op DGH_OP_HDG: the 2E face blocks of the current condensed operator.  dgh_precond_apply with
+ * DGH_OP_DG_T applies the transposed cell-block solves (A^{-T}) from the DG factors. */
 int dgh_block_jacobi_refresh(dgh_ctx *ctx, int op);
 int dgh_precond_apply(dgh_ctx *ctx, int op, const double *x, double *z);
 
@@ -185,6 +199,23 @@ int dgh_newton_update(dgh_integrator *it, dgh_update_stats *stats);
 int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_stats *stats);
 /* Device pointer to the integrator's current Newton state (size dgh_sizes()[0]). */
 double *dgh_integrator_state(dgh_integrator *it);
+
+/* ---- Discrete adjoint of the DG time integration (no counterpart in the reference) -------------
+ * Objective J = sum over nodes of M rho^2 at the end of `steps` fixed steps (dt = cfl / rate of
+ * each step's start state) of the context's integrator (SSP-DIRK3 or BE), DG method.  The
+ * forward run records dt and the frozen wave speeds of every stage and checkpoints the state
+ * every `checkpoint_every` steps; the reverse sweep recomputes each segment's stage states from
+ * its checkpoint and solves J_s^T psi = Kbar_s per stage with GMRES on DGH_OP_DG_T.  dt and the
+ * speeds are held fixed (the derivative of the recorded trajectory), and dgh_dirk3_replay
+ * re-runs the forward model with exactly those values, for finite-difference checks.
+ * host_grad receives dJ/dU(0) (size dgh_sizes()[0]). */
+typedef struct dgh_adjoint_stats {
+    double objective, final_time;
+    int steps, checkpoints, forward_newton, adjoint_krylov, recomputed_steps;
+} dgh_adjoint_stats;
+int dgh_dirk3_adjoint(dgh_integrator *it, int steps, int checkpoint_every, const double *host_u0,
+                      double *host_grad, dgh_adjoint_stats *stats);
+int dgh_dirk3_replay(dgh_integrator *it, const double *host_u0, double *objective);
 
 /* ---- Allocation-free residual ---------------------------------------------------------------
  * No counterpart in the reference.  R(u) exactly as dgh_residual computes it, for callers that

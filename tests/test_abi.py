@@ -13,7 +13,7 @@ HEADER = ROOT / "include" / "dgh_gpu.h"
 
 def declared_functions():
     text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
-    names = re.findall(r"\b(dgh_[a-z0-9_]+)\s*\(", text)
+    names = re.findall(r"\b(dgh_[A-Za-z0-9_]+)\s*\(", text)
     return sorted(set(names))
 
 
