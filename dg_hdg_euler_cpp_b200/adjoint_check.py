@@ -5,8 +5,9 @@
 Objective J = sum over nodes of M rho^2 after `steps` SSP-DIRK3 steps of the DG solve (the
 rotated simple wave, gamma = 3, CFL-limited dt).  Parameters: 8 Fourier coefficients theta of
 a density perturbation added to the projected initial state at the nodes,
-rho_0 += sum_k theta_k cos/sin(2 pi (mx x / lx + my y / ly)) for (mx, my) in
-{(1,0), (0,1), (1,1), (1,-1)}.  The gradient comes from one discrete-adjoint solve
+rho_0 += sum_k theta_k cos/sin(2 pi m (x / lx + y / ly)) for m = 1..4: the modes along the
+wave's direction of variation (the base state depends on x + y only, so modes with kx != ky are
+orthogonal to it and have zero gradient by symmetry).  The gradient comes from one discrete-adjoint solve
 (dgh_dirk3_adjoint: J^T GMRES per stage, checkpoints every `every` steps, recompute in between)
 and is compared with central finite differences (step h) of the same trajectory with dt and the
 frozen speeds replayed (dgh_dirk3_replay).  Prints one JSON line.
@@ -20,7 +21,7 @@ import time
 
 import numpy as np
 
-MODES = [(1, 0), (0, 1), (1, 1), (1, -1)]
+MODES = [(1, 1), (2, 2), (3, 3), (4, 4)]
 
 
 def fourier_modes(s, nx: int, ny: int, k: int) -> np.ndarray:
@@ -83,13 +84,14 @@ def main() -> None:
     t0 = time.perf_counter()
     g_fd = np.array([(objective(u0 + args.h * phi) - objective(u0 - args.h * phi)) / (2 * args.h) for phi in phis])
     t_fd = time.perf_counter() - t0
-    rel = np.abs(g_ad - g_fd) / np.maximum(np.abs(g_ad), 1e-300)
+    rel = np.abs(g_ad - g_fd) / np.max(np.abs(g_ad))
     out = {
         "config": f"{args.nx}x{args.nx} k={args.k} DIRK3 CFL {args.cfl} steps {args.steps} checkpoints every "
                   f"{args.every}", "objective": st.objective, "final_time": st.final_time,
         "forward_newton_updates": st.forward_newton, "adjoint_krylov": st.adjoint_krylov,
         "recomputed_steps": st.recomputed_steps, "gradient_adjoint": g_ad.tolist(), "gradient_fd": g_fd.tolist(),
-        "max_rel_error": float(rel.max()), "fd_step": args.h, "adjoint_seconds": t_adj,
+        "max_error_rel_to_max_gradient": float(rel.max()),
+        "per_mode_rel_error": (np.abs(g_ad - g_fd) / np.abs(g_ad)).tolist(), "fd_step": args.h, "adjoint_seconds": t_adj,
         "fd_seconds_16_forward_runs": t_fd, "within_1e-6": bool(rel.max() <= 1e-6),
     }
     print(json.dumps(out))
