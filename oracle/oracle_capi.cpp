@@ -41,6 +41,7 @@ void out(const Vec &v, double *p) { std::memcpy(p, v.data(), v.size() * sizeof(d
 
 extern "C" {
 const char *oracle_error() { return last_error.c_str(); }
+void oracle_set_error(const char *m) { last_error = m; }
 void oracle_set_threads(int t) { set_threads(t); }
 int oracle_run(int argc, char **argv) { return run_main(argc, argv); }
 

@@ -3,7 +3,7 @@
 
 The reference (YueWu2002/DG_HDG_Euler_Cpp) ships its own run outputs under
 code_test/, accuracy_test/ and speed_test/.  These files are reference OUTPUT data, not source;
-this script copies the small ones that pin the 2D hot path so the tests can run where the
+this script copies the small ones that pin the 2D and 1D hot paths so the tests can run where the
 reference tree is not mounted.  Run it once in a container that has the reference:
 
     python tests/golden/make_golden.py [/path/to/reference]
@@ -42,6 +42,18 @@ for k in range(9):
         FILES.append((f"{SPD}/k{k}_{m}_iterations.csv", f"speed256_k{k}_{m}_iterations.csv"))
         FILES.append((f"{SPD}/k{k}_{m}_summary.csv", f"speed256_k{k}_{m}_summary.csv"))
 FILES.append((f"{SPD}/k8_dg.command.json", "speed256_k8_dg.command.json"))
+# 1D production-path checks (code_test/1d/test_solver.py): 32 cells k=3 one BE step and
+# 16 cells k=2 DIRK3 to T=0.02, DG and HDG, block-Jacobi GMRES, with their commands
+ONE = "code_test/1d/results/intel_final_20261019"
+for case in ("be_update", "dirk_smoke"):
+    for part in ("iterations", "summary", "solution", "difference"):
+        FILES.append((f"{ONE}/{case}_{part}.csv", f"d1_{case}_{part}.csv"))
+    FILES.append((f"{ONE}/{case}.command.json", f"d1_{case}.command.json"))
+# 1D k=8, 32 cells, one BE step (command not archived; the summary holds its parameters)
+for part in ("iterations", "summary", "solution", "difference"):
+    FILES.append((f"code_test/1d/results/k8_n32_check_{part}.csv", f"d1_k8_n32_{part}.csv"))
+# 1D accuracy family, k=2 DIRK3 CFL2 T0.2, N = 32..512 (config N=64 k=2)
+FILES.append(("accuracy_test/results/1d_intel_20261019/convergence_intel_20261019.csv", "d1_convergence.csv"))
 
 
 def main() -> None:
