@@ -12,6 +12,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "lib" / "libdgh_gpu.so"
 BIN_PATH = PKG / "bin" / "dgh2d"
+BIN1D_PATH = PKG / "bin" / "dgh1d"
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -27,6 +28,7 @@ class dgh_config(ctypes.Structure):
         ("nonlinear_tolerance", ctypes.c_double), ("linear_tolerance", ctypes.c_double),
         ("method", ctypes.c_int), ("integrator", ctypes.c_int), ("testcase", ctypes.c_int),
         ("precision", ctypes.c_int), ("check_update", ctypes.c_int), ("device", ctypes.c_int),
+        ("dim", ctypes.c_int),
     ]
 
 

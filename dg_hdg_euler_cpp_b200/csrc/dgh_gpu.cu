@@ -1,6 +1,10 @@
 // C ABI of the B200 DG / condensed-HDG Euler solver: context, memory pools, kernel launches,
-// the block-Jacobi preconditioners and the device-resident GMRES(m).
+// the block-Jacobi preconditioners and the device-resident GMRES(m).  A context solves either
+// the 2D problem (dg_hdg_2d) or, with dgh_config.dim = 1, the 1D problem (dg_hdg_1d); the two
+// share the GMRES, the Arnoldi kernels, the vector helpers and the host integrator, and differ
+// in their discretisation kernels (dgh_kernels_dg/hdg.cuh versus dgh_kernels_1d.cuh).
 #include "dgh_gpu.h"
+#include "dgh_kernels_1d.cuh"
 #include "dgh_kernels_dg.cuh"
 #include "dgh_kernels_hdg.cuh"
 #include "dgh_kernels_init.cuh"
@@ -71,7 +75,11 @@ constexpr int RED_BLOCKS_PER_SM = 4;
 
 struct dgh_ctx {
     dgh_config cfg{};
+    int dim = 2, Q = 0;  // Q: quadrature points per direction (1D may over-integrate)
     int n = 0, P = 0, m = 0, cells = 0, faces = 0, fw = 0, t = 0, restart = 0;
+    size_t nspeeds = 0;  // doubles of the frozen speeds: 2 per face node (2D) or per face (1D)
+    Basis1Q b1{};        // 1D reference element with its quadrature rule
+    Grid1 g1{};
     long long N = 0, NT = 0;
     Grid g{};
     Basis1D basis{};
@@ -150,6 +158,7 @@ struct dgh_ctx {
     }
     void sync() { ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
     bool mixed() const { return cfg.precision == DGH_PRECISION_MIXED; }
+    bool d1() const { return dim == 1; }
     bool has_dg() const { return cfg.method == DGH_METHOD_DG || cfg.method == DGH_METHOD_BOTH; }
     bool has_hdg() const { return cfg.method == DGH_METHOD_HDG || cfg.method == DGH_METHOD_BOTH; }
     int team_blocks(int cpb) const { return (cells + cpb - 1) / cpb; }
@@ -176,6 +185,7 @@ struct dgh_ctx {
             if (s & ST_SHOCK) fail(DGH_ERR_STATE, "Simple wave reaches shock time");
             if (s & ST_SINGULAR) fail(DGH_ERR_SINGULAR, "Singular block Jacobi factor");
             if (s & ST_SINGULAR_HDG) fail(DGH_ERR_SINGULAR, "Singular or nonfinite LU factors");
+            if (s & ST_LU_INPUT) fail(DGH_ERR_SINGULAR, "Nonfinite block LU input");
             fail(DGH_ERR_CUDA, "unknown device status");
         }
     }
@@ -234,7 +244,17 @@ struct Timed {
     }
 
 // ---- launch helpers ---------------------------------------------------------------------------
+constexpr int K1_THREADS = 128;
+inline unsigned grid1(long long n, int t = K1_THREADS) { return (unsigned)((n + t - 1) / t); }
 void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
+    if (c->d1()) {
+        DGH_DISPATCH_N(c->n, {
+            if (check) k1_traces<N, true><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(u, tr, c->b1, c->g1, c->ok);
+            else k1_traces<N, false><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(u, tr, c->b1, c->g1, c->ok);
+        });
+        c->launched();
+        return;
+    }
     DGH_DISPATCH_N(c->n, {
         using T = Team<N>;
         if (check) k_face_trace<N, true><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, tr, c->basis, c->g, c->ok);
@@ -290,8 +310,33 @@ void launch_solve_t(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, 
     c->launched();
 }
 
+// 1D blocks (m <= 27 and 3 x 3): one warp per block, four warps per CTA.
+template <typename TF>
+void launch_small_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, bool backsolve) {
+    const int grid = std::min((count + 3) / 4, c->sms * 16);
+    k1_small_lu<TF><<<grid, 128, 0, c->stream>>>(pool, stride, m, ld, count, perm, c->status, ST_LU_INPUT,
+                                                 ST_SINGULAR_HDG, backsolve ? 1 : 0);
+    c->launched();
+}
+template <typename TF>
+void launch_small_solve(dgh_ctx *c, const TF *pool, const int *perm, int m, int count, const double *x, double *z,
+                        bool transpose) {
+    const int grid = std::min((count + 3) / 4, c->sms * 16);
+    k1_small_solve<TF><<<grid, 128, 0, c->stream>>>(pool, perm, m, count, x, z, transpose ? 1 : 0);
+    c->launched();
+}
+
 void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     Timed tm(c, DGH_TIMER_PRECOND);
+    if (c->d1()) {
+        const bool dg = op != DGH_OP_HDG;
+        need(dg ? c->dg_factored : c->face_factored, "Refresh the block-Jacobi preconditioner before applying it");
+        const void *pool = dg ? c->dg_pool : c->face_pool;
+        const int *perm = dg ? c->dg_perm : c->face_perm, m = dg ? c->m : c->fw;
+        if (c->mixed()) launch_small_solve<float>(c, (const float *)pool, perm, m, c->cells, x, z, op == DGH_OP_DG_T);
+        else launch_small_solve<double>(c, (const double *)pool, perm, m, c->cells, x, z, op == DGH_OP_DG_T);
+        return;
+    }
     if (op == DGH_OP_DG_T) {
         need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->m * c->m;
@@ -314,6 +359,14 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
 
 void dg_apply(dgh_ctx *c, const double *v, double *out) {
     need(c->linearised, "Refresh the volume Jacobian before applying it");
+    if (c->d1()) {
+        DGH_DISPATCH_N(c->n, {
+            k1_dg_apply<N><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(v, c->vol, c->fcache, out, c->b1, c->g1,
+                                                                          c->inv_step);
+        });
+        c->launched();
+        return;
+    }
     launch_trace(c, v, c->traces2, false);
     DGH_DISPATCH_N(c->n, {
         using T = Team<N>;
@@ -323,6 +376,7 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
     c->launched();
 }
 void dg_apply_t(dgh_ctx *c, const double *w, double *out) {
+    need(!c->d1(), "The adjoint J^T w is built for the 2D operator only");
     need(c->linearised, "Refresh the volume Jacobian before applying it");
     launch_trace(c, w, c->traces2, false);
     DGH_DISPATCH_N(c->n, {
@@ -335,6 +389,11 @@ void dg_apply_t(dgh_ctx *c, const double *w, double *out) {
 }
 void hdg_apply(dgh_ctx *c, const double *lam, double *out) {
     need(c->condensed, "Condense the HDG operator before applying it");
+    if (c->d1()) {
+        k1_hdg_apply<<<grid1(c->NT), K1_THREADS, 0, c->stream>>>(c->S, c->speeds, lam, out, c->g1);
+        c->launched();
+        return;
+    }
     DGH_DISPATCH_N(c->n, { k_hdg_apply<N><<<c->faces, 256, 0, c->stream>>>(c->S, c->speeds, lam, out, c->basis, c->g); });
     c->launched();
 }
@@ -520,6 +579,125 @@ __global__ void k_fill_trace_mass(double *inv_tm, Basis1D b, Grid g, int n, long
     const int fw = 4 * n, face = (int)(i / fw), q = (int)(i % fw) % n;
     inv_tm[i] = 1 / face_weight(g, b, face, q);
 }
+
+// Sizes, reference element and pools of a 1D context (dg_hdg_1d/src/discretization.cpp:4-14,
+// nodal_basis.hpp:34-65 with its separate quadrature rule).  Called after the stream exists.
+void create1(dgh_ctx *c, const dgh_config &k) {
+    const int n = k.degree + 1, Q = k.quadrature ? k.quadrature : n;
+    c->dim = 1;
+    c->n = n;
+    c->Q = Q;
+    c->P = n;
+    c->m = NV1 * n;
+    c->cells = k.nx;
+    c->faces = k.nx;
+    c->fw = NV1;
+    c->t = T1;
+    c->N = (long long)c->cells * c->m;
+    c->NT = (long long)c->faces * NV1;
+    c->nspeeds = 2 * (size_t)c->faces;
+    c->cs.kind = 2;  // the unrotated simple wave: exact_state's axis case with y unused
+    c->cs.cosine = 1.;
+    c->cs.sine = 0.;
+    c->cs.lx = 2.;
+    c->cs.ly = 1.;
+    c->cs.gamma = 3.;
+    c->g1.cells = c->cells;
+    c->g1.h = 2.0 / c->cells;
+    c->g1.gamma = 3.;
+    c->g.nx = c->cells;
+    c->g.ny = 1;
+    c->g.cells = c->cells;
+    c->g.hx = c->g1.h;
+    c->g.hy = 1.;
+    c->g.gamma = 3.;
+    std::vector<double> x, w, qx, qw;
+    gauss_rule(n, x, w);
+    gauss_rule(Q, qx, qw);
+    c->xnodes = x;
+    std::vector<double> bary(n, 1.), D(n * n, 0.);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            if (i != j) bary[i] /= x[i] - x[j];
+    for (int i = 0; i < n; ++i) {
+        double s = 0;
+        for (int j = 0; j < n; ++j)
+            if (i != j) {
+                D[i * n + j] = bary[j] / (bary[i] * (x[i] - x[j]));
+                s += D[i * n + j];
+            }
+        D[i * n + i] = -s;
+    }
+    auto eL = lagrange(x, -1.), eR = lagrange(x, 1.);
+    Basis1Q &b = c->b1;
+    b.n = n;
+    b.Q = Q;
+    b.colloc = Q == n;
+    for (int i = 0; i < n; ++i) {
+        b.w[i] = c->basis.w[i] = w[i];
+        b.eL[i] = c->basis.eL[i] = eL[i];
+        b.eR[i] = c->basis.eR[i] = eR[i];
+    }
+    for (int q = 0; q < Q; ++q) {
+        const auto v = lagrange(x, qx[q]);
+        for (int i = 0; i < n; ++i) b.values[q * n + i] = b.colloc ? (q == i ? 1. : 0.) : v[i];
+    }
+    for (int q = 0; q < Q; ++q)
+        for (int i = 0; i < n; ++i) {
+            double s = 0;
+            for (int j = 0; j < n; ++j) s += b.values[q * n + j] * D[j * n + i];
+            b.wd[q * n + i] = qw[q] * s;
+        }
+    c->old = c->alloc<double>(c->N);
+    c->mass = c->alloc<double>(c->N);
+    c->inv_mass = c->alloc<double>(c->N);
+    c->inv_trace_mass = c->alloc<double>(c->NT);
+    c->speeds = c->alloc<double>(c->nspeeds);
+    c->traces = c->alloc<double>((size_t)c->cells * T1);
+    c->traces2 = c->alloc<double>((size_t)c->cells * T1);
+    c->partial = c->alloc<double>((size_t)std::max<long long>(KR_MAXK * c->red_grid, 4LL * c->cells + 64));
+    c->red = c->alloc<double>(4 * KR_MAXK);
+    c->vol = c->alloc<double>((size_t)c->cells * Q * 9);
+    c->fcache = c->alloc<double>((size_t)c->faces * 18);
+    c->status = c->alloc<int>(1);
+    c->ok = c->alloc<int>(1);
+    ck(cudaMemset(c->status, 0, sizeof(int)), "memset");
+    build_rule(c);
+    k1_fill_mass<<<grid1(c->N, 256), 256, 0, c->stream>>>(c->mass, c->inv_mass, c->inv_trace_mass, c->b1, c->g1, n);
+    c->launched();
+    const size_t tsz = c->mixed() ? sizeof(float) : sizeof(double);
+    if (c->has_dg()) {
+        c->dg_pool = c->alloc<char>((size_t)c->cells * c->m * c->m * tsz);
+        c->dg_perm = c->alloc<int>((size_t)c->cells * c->m);
+    }
+    if (c->has_hdg()) {
+        c->S = c->alloc<double>((size_t)c->cells * T1 * T1);
+        c->X = c->alloc<double>((size_t)c->cells * c->m * T1);
+        c->Y = c->alloc<double>((size_t)c->cells * c->m);
+        c->cy = c->alloc<double>((size_t)c->cells * T1);
+        c->hrhs = c->alloc<double>(c->NT);
+        const size_t per_cell = (size_t)c->m * (c->m + T1 + 1) * sizeof(double);
+        const size_t budget = (size_t)8 << 30;
+        c->aug_cells = (int)std::max<size_t>(1, std::min<size_t>(c->cells, budget / per_cell));
+        c->aug = c->alloc<double>((size_t)c->aug_cells * c->m * (c->m + T1 + 1));
+        c->aug_perm = c->alloc<int>((size_t)c->aug_cells * c->m);
+        c->face_pool = c->alloc<char>((size_t)c->faces * NV1 * NV1 * tsz);
+        c->face_perm = c->alloc<int>((size_t)c->faces * NV1);
+    }
+    const long long vn = std::max(c->has_dg() ? c->N : 0LL, c->has_hdg() ? c->NT : 0LL);
+    c->vld = ((vn + 31) / 32) * 32;
+    c->restart = k.restart;
+    c->V = c->alloc<double>((size_t)c->vld * (k.restart + 1));
+    c->gw = c->alloc<double>(vn);
+    c->gz = c->alloc<double>(vn);
+    if (c->has_dg()) {
+        c->gres[DGH_OP_DG] = c->alloc<double>(c->N);
+        c->gres[DGH_OP_DG_T] = c->alloc<double>(c->N);
+    }
+    if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
+    c->gcoef = c->alloc<double>(KR_MAXK);
+    c->sync();
+}
 }  // namespace
 
 // ============================================================================ C ABI
@@ -533,7 +711,7 @@ void dgh_config_default(dgh_config *c) {
     c->cfl = 2.; c->final_time = .2; c->safety = 1.1;
     c->nonlinear_tolerance = 1e-12; c->linear_tolerance = 1e-12;
     c->method = DGH_METHOD_BOTH; c->integrator = DGH_INTEGRATOR_DIRK3; c->testcase = DGH_TEST_DIAGONAL;
-    c->precision = DGH_PRECISION_FP64; c->check_update = 0; c->device = 0;
+    c->precision = DGH_PRECISION_FP64; c->check_update = 0; c->device = 0; c->dim = 2;
 }
 
 static thread_local std::string g_create_error;
@@ -545,10 +723,15 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
     c->cfg = *cfg;
     const int rc = guard(c, [&] {
         const dgh_config &k = *cfg;
-        // config.cpp:6-22
-        need(k.nx >= 3 && k.ny >= 3 && k.degree >= 0 && k.degree <= 8 && k.quadrature >= 0, "Invalid mesh or degree");
+        need(k.dim == 1 || k.dim == 2, "Invalid dimension (1 or 2)");
+        // config.cpp:6-22 (dg_hdg_1d/src/config.cpp:6-21 in 1D)
+        need(k.nx >= 3 && (k.dim == 1 || k.ny >= 3) && k.degree >= 0 && k.degree <= 8 && k.quadrature >= 0,
+             "Invalid mesh or degree");
         need(k.quadrature == 0 || k.quadrature >= k.degree + 1, "Quadrature must be >= degree+1");
-        need(k.quadrature == 0 || k.quadrature == k.degree + 1, "Over-integration (--quad > k+1) is not supported");
+        if (k.dim == 2)
+            need(k.quadrature == 0 || k.quadrature == k.degree + 1, "Over-integration (--quad > k+1) is not supported");
+        else
+            need(k.quadrature <= MAXQ1, "Quadrature above 20 points is not supported on the device");
         need(k.restart > 0 && k.max_linear > 0 && k.max_newton > 0 && k.steps >= 0, "Invalid iteration limit");
         need(k.newton_steps >= 0 && k.warmup_updates >= 0, "Invalid timing update count");
         need(std::isfinite(k.cfl) && k.cfl > 0 && std::isfinite(k.final_time) && k.final_time >= 0,
@@ -558,7 +741,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
                  k.linear_tolerance < 1,
              "Invalid solver tolerance or wave-speed safety");
         need(k.method >= 0 && k.method <= 2, "Method must be dg, hdg, or both");
-        need(k.testcase >= 0 && k.testcase <= 2, "Invalid testcase");
+        need(k.dim == 1 || (k.testcase >= 0 && k.testcase <= 2), "Invalid testcase");
         need(k.precision == 0 || k.precision == 1, "Invalid precision");
         need(k.restart <= KR_MAXK - 1, "restart must be at most 31 on the device GMRES");
         int ndev = 0;
@@ -571,6 +754,10 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->red_grid = c->sms * RED_BLOCKS_PER_SM;
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaMallocHost((void **)&c->pinned, 4096), "cudaMallocHost");
+        if (k.dim == 1) {
+            create1(c, k);
+            return;
+        }
 
         c->n = k.degree + 1;
         c->P = c->n * c->n;
@@ -581,6 +768,8 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->t = NFACES * c->fw;
         c->N = (long long)c->cells * c->m;
         c->NT = (long long)c->faces * c->fw;
+        c->Q = c->n;
+        c->nspeeds = 2 * (size_t)c->faces * c->n;
         // example.hpp:9-14
         const double pi = std::acos(-1.);
         c->cs.kind = k.testcase == DGH_TEST_DIAGONAL ? 0 : (k.testcase == DGH_TEST_WAVE ? 1 : 2);
@@ -715,7 +904,7 @@ int dgh_get_config(const dgh_ctx *c, dgh_config *out) {
 }
 int dgh_geometry(const dgh_ctx *c, double out[4]) {
     if (!c || !out) return DGH_ERR_INVALID;
-    out[0] = c->g.hx; out[1] = c->g.hy; out[2] = c->cs.lx; out[3] = c->cs.ly;
+    out[0] = c->g.hx; out[1] = c->g.hy; out[2] = c->cs.lx; out[3] = c->cs.ly;  // 1D: h, 1, 2, 1
     return DGH_OK;
 }
 int dgh_nodes(const dgh_ctx *c, double *x, double *w) {
@@ -779,7 +968,13 @@ int dgh_axpby(dgh_ctx *c, double a, const double *x, double b, const double *y, 
 int dgh_initial(dgh_ctx *c, double *u) {
     return guard(c, [&] {
         need(u, "null state");
-        DGH_DISPATCH_N(c->n, { k_initial<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, c->status); });
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, {
+                k1_initial<N><<<grid1(c->cells, 64), 64, 0, c->stream>>>(u, c->rule, c->b1, c->g1, c->cs, c->status);
+            });
+        } else {
+            DGH_DISPATCH_N(c->n, { k_initial<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, c->status); });
+        }
         c->launched();
         c->check_status();
         // initial_and_error.cpp:53 — the projected state must be admissible
@@ -800,6 +995,25 @@ int dgh_freeze(dgh_ctx *c, const double *u, double *rate) {
         need(u && rate, "null argument");
         ck(cudaMemcpyAsync(c->old, u, c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
         launch_trace(c, u, c->traces, false);
+        if (c->d1()) {
+            // dg_hdg_1d/src/discretization.cpp:75-92
+            const unsigned nb = grid1(c->cells, 256);
+            k1_speeds<<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(c->traces, c->speeds, c->g1, c->cfg.safety,
+                                                                     c->status);
+            DGH_DISPATCH_N(c->n, { k1_rate<N><<<nb, 256, 0, c->stream>>>(u, c->speeds, c->partial, c->b1, c->g1); });
+            c->launched(2);
+            c->check_status();
+            std::vector<double> part(nb);
+            ck(cudaMemcpyAsync(part.data(), c->partial, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+            c->sync();
+            double r = 0;
+            for (double p : part) r = r < p ? p : r;
+            if (!(std::isfinite(r) && r > 0)) fail(DGH_ERR_STATE, "Invalid CFL rate");
+            *rate = r;
+            c->frozen = true;
+            c->linearised = c->dg_factored = c->condensed = c->face_factored = false;
+            return;
+        }
         DGH_DISPATCH_N(c->n, {
             const int tot = 2 * c->cells * N;
             k_speeds<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, c->g, c->cfg.safety, c->status);
@@ -839,6 +1053,14 @@ int dgh_residual(dgh_ctx *c, const double *u, double *r) {
         need(c->frozen, "Freeze the wave speeds before evaluating the residual");
         Timed tm(c, DGH_TIMER_RESIDUAL);
         launch_trace(c, u, c->traces, false);
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, {
+                k1_residual<N><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(u, c->old, c->traces, c->speeds, r, c->b1,
+                                                                              c->g1, 1. / c->step_size);
+            });
+            c->launched();
+            return;
+        }
         DGH_DISPATCH_N(c->n, {
             using T = Team<N>;
             k_residual<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->old, c->traces, c->speeds, r,
@@ -865,6 +1087,11 @@ int dgh_trace(dgh_ctx *c, const double *u, double *lam) {
     return guard(c, [&] {
         need(c->frozen, "Freeze the wave speeds first");
         launch_trace(c, u, c->traces, false);
+        if (c->d1()) {
+            k1_trace_lambda<<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(c->traces, c->speeds, lam, c->g1);
+            c->launched();
+            return;
+        }
         DGH_DISPATCH_N(c->n, {
             const int tot = 2 * c->cells * N;
             k_trace_lambda<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, lam, c->g);
@@ -882,10 +1109,14 @@ int dgh_state_norm(dgh_ctx *c, const double *u, double *out) {
 
 int dgh_integral(dgh_ctx *c, const double *u, double out[4]) {
     return guard(c, [&] {
-        DGH_DISPATCH_N(c->n, {
-            const int tot = c->cells * NVAR;
-            k_integral<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(u, c->basis, c->g, c->partial);
-        });
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, { k1_integral<N><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(u, c->b1, c->g1, c->partial); });
+        } else {
+            DGH_DISPATCH_N(c->n, {
+                const int tot = c->cells * NVAR;
+                k_integral<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(u, c->basis, c->g, c->partial);
+            });
+        }
         c->launched();
         std::vector<double> part((size_t)c->cells * 4);
         ck(cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
@@ -898,9 +1129,16 @@ int dgh_integral(dgh_ctx *c, const double *u, double out[4]) {
 
 int dgh_l2_error(dgh_ctx *c, const double *u, double time, double out[4]) {
     return guard(c, [&] {
-        DGH_DISPATCH_N(c->n, {
-            k_l2_error<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, time, c->partial, c->status);
-        });
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, {
+                k1_l2_error<N><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(u, c->rule, c->g1, c->cs, time, c->partial,
+                                                                              c->status);
+            });
+        } else {
+            DGH_DISPATCH_N(c->n, {
+                k_l2_error<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, time, c->partial, c->status);
+            });
+        }
         c->launched();
         c->check_status();
         std::vector<double> part((size_t)c->cells * 4);
@@ -916,13 +1154,13 @@ int dgh_l2_error(dgh_ctx *c, const double *u, double time, double out[4]) {
 int dgh_copy_speeds(dgh_ctx *c, double *dev_ab) {
     return guard(c, [&] {
         need(c->frozen, "Freeze the wave speeds first");
-        ck(cudaMemcpyAsync(dev_ab, c->speeds, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToDevice,
+        ck(cudaMemcpyAsync(dev_ab, c->speeds, c->nspeeds * sizeof(double), cudaMemcpyDeviceToDevice,
                            c->stream), "copy");
     });
 }
 int dgh_set_speeds(dgh_ctx *c, const double *dev_ab) {
     return guard(c, [&] {
-        ck(cudaMemcpyAsync(c->speeds, dev_ab, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToDevice,
+        ck(cudaMemcpyAsync(c->speeds, dev_ab, c->nspeeds * sizeof(double), cudaMemcpyDeviceToDevice,
                            c->stream), "copy");
         c->frozen = true;
         c->linearised = c->dg_factored = c->condensed = c->face_factored = false;
@@ -936,6 +1174,7 @@ int dgh_mass_axpby(dgh_ctx *c, double a, const double *x, double b, const double
 }
 int dgh_rho2(dgh_ctx *c, const double *u, double *value, double *grad) {
     return guard(c, [&] {
+        need(!c->d1(), "The adjoint objective is built for the 2D problem only");
         k_rho2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(u, c->mass, c->P, c->N, grad, c->partial);
         k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, c->red);
         c->launched(2);
@@ -946,7 +1185,7 @@ int dgh_rho2(dgh_ctx *c, const double *u, double *value, double *grad) {
 }
 int dgh_speeds(dgh_ctx *c, double *host_ab) {
     return guard(c, [&] {
-        ck(cudaMemcpyAsync(host_ab, c->speeds, 2 * (size_t)c->faces * c->n * sizeof(double), cudaMemcpyDeviceToHost,
+        ck(cudaMemcpyAsync(host_ab, c->speeds, c->nspeeds * sizeof(double), cudaMemcpyDeviceToHost,
                            c->stream), "copy");
         c->sync();
     });
@@ -958,6 +1197,16 @@ void linearise(dgh_ctx *c, const double *u) {
     need(c->frozen, "Freeze the wave speeds before refreshing the Jacobian");
     need(c->step_size > 0, "Set the time step before refreshing the Jacobian");
     launch_trace(c, u, c->traces, false);
+    if (c->d1()) {
+        DGH_DISPATCH_N(c->n, {
+            k1_linearise<N><<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(u, c->traces, c->speeds, c->vol, c->fcache,
+                                                                           c->b1, c->g1);
+        });
+        c->launched();
+        c->linearised = true;
+        c->dg_factored = c->condensed = c->face_factored = false;
+        return;
+    }
     DGH_DISPATCH_N(c->n, {
         const long long tv = (long long)c->cells * N * N;
         k_volume_cache<N><<<(unsigned)((tv + 255) / 256), 256, 0, c->stream>>>(u, c->vol, c->g);
@@ -984,10 +1233,17 @@ int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
         need(c->linearised, "Refresh the volume Jacobian before assembling a block");
         need(row == col && row >= 0 && row < c->cells, "Only diagonal cell blocks are exposed on the device");
         double *tmp = c->alloc<double>((size_t)c->m * c->m);
-        DGH_DISPATCH_N(c->n, {
-            k_dg_assemble<N, double><<<1, 256, 0, c->stream>>>(tmp, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step,
-                                                                row, 1);
-        });
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, {
+                k1_dg_assemble<N, double><<<grid1((long long)c->m * c->m), K1_THREADS, 0, c->stream>>>(
+                    tmp, c->vol, c->fcache, c->b1, c->g1, c->inv_step, row, 1);
+            });
+        } else {
+            DGH_DISPATCH_N(c->n, {
+                k_dg_assemble<N, double><<<1, 256, 0, c->stream>>>(tmp, c->vol, c->fcache, c->speeds, c->basis, c->g,
+                                                                    c->inv_step, row, 1);
+            });
+        }
         c->launched();
         ck(cudaMemcpyAsync(host_block, tmp, (size_t)c->m * c->m * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
         c->sync();
@@ -1001,6 +1257,38 @@ int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
 int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
     return guard(c, [&] {
         Timed tm(c, op == DGH_OP_DG ? DGH_TIMER_FACTOR : DGH_TIMER_FACE_FACTOR);
+        if (c->d1()) {
+            // BlockPreconditioner of the block-Jacobi kind (common/src/linalg/block_ilu.cpp:48-61): the
+            // DenseLU of every diagonal block, whose require() texts report a failure.
+            const bool dg = op == DGH_OP_DG;
+            need(dg ? c->dg_pool != nullptr : c->face_pool != nullptr,
+                 dg ? "context has no DG operator" : "context has no HDG operator");
+            need(dg ? c->linearised : c->condensed, dg ? "Refresh the volume Jacobian before assembling a block"
+                                                       : "Condense the HDG operator before refreshing its preconditioner");
+            const long long tot = dg ? (long long)c->cells * c->m * c->m : (long long)c->cells * 9;
+            if (c->mixed()) {
+                if (dg) DGH_DISPATCH_N(c->n, {
+                        k1_dg_assemble<N, float><<<grid1(tot), K1_THREADS, 0, c->stream>>>(
+                            (float *)c->dg_pool, c->vol, c->fcache, c->b1, c->g1, c->inv_step, 0, c->cells);
+                    })
+                else k1_face_blocks<float><<<grid1(tot), K1_THREADS, 0, c->stream>>>(c->S, c->speeds, (float *)c->face_pool, c->g1);
+                c->launched();
+                if (dg) launch_small_lu<float>(c, (float *)c->dg_pool, (size_t)c->m * c->m, c->m, c->m, c->cells, c->dg_perm, false);
+                else launch_small_lu<float>(c, (float *)c->face_pool, 9, 3, 3, c->cells, c->face_perm, false);
+            } else {
+                if (dg) DGH_DISPATCH_N(c->n, {
+                        k1_dg_assemble<N, double><<<grid1(tot), K1_THREADS, 0, c->stream>>>(
+                            (double *)c->dg_pool, c->vol, c->fcache, c->b1, c->g1, c->inv_step, 0, c->cells);
+                    })
+                else k1_face_blocks<double><<<grid1(tot), K1_THREADS, 0, c->stream>>>(c->S, c->speeds, (double *)c->face_pool, c->g1);
+                c->launched();
+                if (dg) launch_small_lu<double>(c, (double *)c->dg_pool, (size_t)c->m * c->m, c->m, c->m, c->cells, c->dg_perm, false);
+                else launch_small_lu<double>(c, (double *)c->face_pool, 9, 3, 3, c->cells, c->face_perm, false);
+            }
+            c->check_status();
+            (dg ? c->dg_factored : c->face_factored) = true;
+            return;
+        }
         if (op == DGH_OP_DG) {
             need(c->dg_pool, "context has no DG operator");
             need(c->linearised, "Refresh the volume Jacobian before assembling a block");
@@ -1059,6 +1347,28 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
         Timed tm(c, DGH_TIMER_CONDENSE);
         linearise(c, u);
         const int ld = c->m + c->t + 1;
+        if (c->d1()) {
+            // dg_hdg_1d/src/hybrid.cpp:39-84: [A | B | r] per cell, LU + back substitution, S and C y
+            for (int first = 0; first < c->cells; first += c->aug_cells) {
+                const int count = std::min(c->aug_cells, c->cells - first);
+                DGH_DISPATCH_N(c->n, {
+                    k1_hdg_assemble<N><<<grid1((long long)count * c->m * ld), K1_THREADS, 0, c->stream>>>(
+                        c->aug, c->vol, c->traces, c->speeds, r, c->b1, c->g1, c->inv_step, first, count);
+                });
+                c->launched();
+                launch_small_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, true);
+                DGH_DISPATCH_N(c->n, {
+                    k1_hdg_schur<N><<<grid1((long long)count * T1 * (T1 + 1)), K1_THREADS, 0, c->stream>>>(
+                        c->aug, c->traces, c->speeds, c->S, c->X, c->Y, c->cy, c->b1, c->g1, first, count);
+                });
+                c->launched();
+            }
+            k1_hdg_rhs<<<grid1(c->NT), K1_THREADS, 0, c->stream>>>(c->cy, c->hrhs, c->g1);
+            c->launched();
+            c->check_status();
+            c->condensed = true;
+            return;
+        }
         for (int first = 0; first < c->cells; first += c->aug_cells) {
             const int count = std::min(c->aug_cells, c->cells - first);
             const int grid = std::min(count, c->sms * 8);
@@ -1100,9 +1410,13 @@ int dgh_hdg_block(dgh_ctx *c, int row, int col, double *host_block) {
         need(row == col && row >= 0 && row < c->faces, "Only diagonal face blocks are exposed on the device");
         const long long tot = (long long)c->faces * c->fw * c->fw;
         double *tmp = c->alloc<double>(tot);
-        DGH_DISPATCH_N(c->n, {
-            k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, tmp, c->basis, c->g);
-        });
+        if (c->d1()) {
+            k1_face_blocks<double><<<grid1(tot), K1_THREADS, 0, c->stream>>>(c->S, c->speeds, tmp, c->g1);
+        } else {
+            DGH_DISPATCH_N(c->n, {
+                k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, tmp, c->basis, c->g);
+            });
+        }
         c->launched();
         ck(cudaMemcpyAsync(host_block, tmp + (size_t)row * c->fw * c->fw, (size_t)c->fw * c->fw * sizeof(double),
                            cudaMemcpyDeviceToHost, c->stream), "copy");
@@ -1115,13 +1429,24 @@ int dgh_hdg_block(dgh_ctx *c, int row, int col, double *host_block) {
 int dgh_hdg_recover(dgh_ctx *c, const double *dl, double *du) {
     return guard(c, [&] {
         need(c->condensed, "Condense the HDG operator first");
-        DGH_DISPATCH_N(c->n, { k_hdg_recover<N><<<c->cells, 256, 0, c->stream>>>(c->X, c->Y, dl, du, c->g); });
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, { k1_hdg_recover<N><<<grid1(c->N), K1_THREADS, 0, c->stream>>>(c->X, c->Y, dl, du, c->g1); });
+        } else {
+            DGH_DISPATCH_N(c->n, { k_hdg_recover<N><<<c->cells, 256, 0, c->stream>>>(c->X, c->Y, dl, du, c->g); });
+        }
         c->launched();
     });
 }
 int dgh_hdg_recovered_residual(dgh_ctx *c, const double *e, double *out) {
     return guard(c, [&] {
         need(c->condensed, "Condense the HDG operator first");
+        if (c->d1()) {
+            DGH_DISPATCH_N(c->n, {
+                k1_hdg_recovered_residual<N><<<grid1(c->N), K1_THREADS, 0, c->stream>>>(e, c->speeds, out, c->b1, c->g1);
+            });
+            c->launched();
+            return;
+        }
         DGH_DISPATCH_N(c->n, {
             const long long tot = (long long)c->cells * N * N;
             k_hdg_recovered_residual<N><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(e, c->speeds, out, c->basis, c->g);

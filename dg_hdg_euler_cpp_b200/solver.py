@@ -32,7 +32,8 @@ def make_config(**kw) -> _lib.dgh_config:
     lib = _lib.load()
     cfg = _lib.dgh_config()
     lib.dgh_config_default(ctypes.byref(cfg))
-    aliases = {"k": "degree", "ntol": "nonlinear_tolerance", "ltol": "linear_tolerance", "T": "final_time"}
+    aliases = {"k": "degree", "ntol": "nonlinear_tolerance", "ltol": "linear_tolerance", "T": "final_time",
+               "cells": "nx", "quad": "quadrature"}
     for key, val in kw.items():
         key = aliases.get(key, key)
         if key == "method":
@@ -54,7 +55,9 @@ def _ptr(t) -> ctypes.c_void_p:
 
 
 class Solver:
-    """One GPU context: the Problem plus the DG and/or HDG operators of one configuration."""
+    """One GPU context: the Problem plus the DG and/or HDG operators of one configuration.
+    Solver(dim=1, cells=..., k=...) is the 1D problem of dg_hdg_1d (three variables per node,
+    NVAR values per face trace)."""
 
     def __init__(self, **kw):
         import torch
@@ -74,6 +77,8 @@ class Solver:
         g = (ctypes.c_double * 4)()
         self._rc(self.lib.dgh_geometry(self.h, g))
         self.hx, self.hy, self.lx, self.ly = list(g)
+        self.dim = int(self.cfg.dim)
+        self.nvar = 3 if self.dim == 1 else 4
         self.device = torch.device("cuda", self.cfg.device)
 
     def close(self):
@@ -159,15 +164,15 @@ class Solver:
     def integral(self, u) -> np.ndarray:
         out = (ctypes.c_double * 4)()
         self._call("dgh_integral", _ptr(u), out)
-        return np.array(out[:])
+        return np.array(out[:self.nvar])
 
     def l2_error(self, u, time: float) -> np.ndarray:
         out = (ctypes.c_double * 4)()
         self._call("dgh_l2_error", _ptr(u), ctypes.c_double(time), out)
-        return np.array(out[:])
+        return np.array(out[:self.nvar])
 
     def speeds(self) -> np.ndarray:
-        ab = np.zeros(2 * self.faces * self.n)
+        ab = np.zeros(2 * self.faces * (1 if self.dim == 1 else self.n))
         self._call("dgh_speeds", ab.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         return ab.reshape(-1, 2)
 

@@ -56,9 +56,12 @@ enum { DGH_PRECISION_FP64 = 0, DGH_PRECISION_MIXED = 1 };
  * and the DG adjoint J^T (with the transposed block-Jacobi preconditioner). */
 enum { DGH_OP_DG = 0, DGH_OP_HDG = 1, DGH_OP_DG_T = 2 };
 
-/* config.hpp:7-18 plus the precision and the operators to allocate. */
+/* config.hpp:7-18 plus the precision and the operators to allocate.  dim = 1 selects the 1D
+ * solver of dg_hdg_1d/ (config.hpp:7-19 there): nx is the number of cells, ny is ignored,
+ * NVAR = 3, two faces per cell, and quadrature may exceed degree+1 (over-integration, up to
+ * 20 points).  In 2D the quadrature is collocated (0 or degree+1). */
 typedef struct dgh_config {
-    int nx, ny, degree, quadrature; /* quadrature 0 or degree+1 (collocated Gauss)       */
+    int nx, ny, degree, quadrature;
     int restart, max_linear, max_newton, steps, newton_steps, warmup_updates;
     double cfl, final_time, safety, nonlinear_tolerance, linear_tolerance;
     int method;       /* DGH_METHOD_*: which operators the context allocates               */
@@ -67,10 +70,12 @@ typedef struct dgh_config {
     int precision;    /* DGH_PRECISION_*                                                   */
     int check_update; /* HDG: independent DG J*v check of every update (time_integrator.cpp:153-162) */
     int device;       /* CUDA device ordinal                                               */
+    int dim;          /* 2 (dg_hdg_2d, the default) or 1 (dg_hdg_1d)                       */
 } dgh_config;
 
 /* config.hpp:7-18 defaults: nx=ny=8, k=3, restart 30, max_linear 1500, max_newton 30,
- * cfl 2, T 0.2, safety 1.1, ntol = ltol = 1e-12, ssp-dirk3, diagonal test case, both methods. */
+ * cfl 2, T 0.2, safety 1.1, ntol = ltol = 1e-12, ssp-dirk3, diagonal test case, both methods,
+ * dim 2.  (The 1D program's defaults differ only in cells = 32.) */
 void dgh_config_default(dgh_config *cfg);
 
 /* ---- context ----------------------------------------------------------------------------- */
@@ -83,7 +88,8 @@ int dgh_sizes(const dgh_ctx *ctx, int64_t sizes[8]);
 /* The configuration the context was created with. */
 int dgh_get_config(const dgh_ctx *ctx, dgh_config *out);
 void *dgh_stream(const dgh_ctx *ctx);       /* the cudaStream_t all work is ordered on */
-/* out[0..3] = hx, hy, lx, ly (discretization.cpp:4-8, example.hpp:9-14) */
+/* out[0..3] = hx, hy, lx, ly (discretization.cpp:4-8, example.hpp:9-14); in 1D h, 1, 2, 1 so
+ * that the physical rms norm / sqrt(lx ly) is dg_hdg_1d's norm / sqrt(2). */
 int dgh_geometry(const dgh_ctx *ctx, double out[4]);
 /* Gauss nodes and weights on [-1,1] (n values each; either pointer may be NULL) */
 int dgh_nodes(const dgh_ctx *ctx, double *x, double *w);
@@ -124,9 +130,10 @@ int dgh_admissible(dgh_ctx *ctx, const double *u, int *ok);        /* discretiza
 int dgh_trace(dgh_ctx *ctx, const double *u, double *lambda);      /* discretization.cpp:196-210 */
 int dgh_dual_norm(dgh_ctx *ctx, const double *r, double *out);     /* sqrt(r^T M^-1 r), time_integrator.cpp:42 */
 int dgh_state_norm(dgh_ctx *ctx, const double *u, double *out);    /* sqrt(u^T M u), time_integrator.cpp:45 */
+/* Conservation integrals and L2 errors per variable; in 1D (rho, momentum, energy, 0). */
 int dgh_integral(dgh_ctx *ctx, const double *u, double out[4]);    /* discretization.cpp:237-243 */
 int dgh_l2_error(dgh_ctx *ctx, const double *u, double time, double out[4]); /* initial_and_error.cpp:55-73 */
-int dgh_speeds(dgh_ctx *ctx, double *host_ab);                     /* frozen (a,b) per face node */
+int dgh_speeds(dgh_ctx *ctx, double *host_ab);                     /* frozen (a,b) per face node (per face in 1D) */
 /* Device copies of the frozen speeds, and replaying recorded ones (they replace Problem::freeze's
  * speeds without touching old/step; used to hold the speeds fixed in the discrete adjoint). */
 int dgh_copy_speeds(dgh_ctx *ctx, double *dev_ab);
@@ -134,14 +141,14 @@ int dgh_set_speeds(dgh_ctx *ctx, const double *dev_ab);
 /* out = a M x + b y with the diagonal mass matrix (discretization.cpp:9-13). */
 int dgh_mass_axpby(dgh_ctx *ctx, double a, const double *x, double b, const double *y, double *out);
 /* value = sum over nodes of M rho^2 (the adjoint objective); grad (may be NULL) = 2 M rho. */
-int dgh_rho2(dgh_ctx *ctx, const double *u, double *value, double *grad);
+int dgh_rho2(dgh_ctx *ctx, const double *u, double *value, double *grad);  /* 2D only */
 
 /* ---- DGOperator (dg_operator.hpp:5-17) ------------------------------------------------------ */
 int dgh_dg_refresh(dgh_ctx *ctx, const double *u);                 /* dg_operator.cpp:6-9 */
 int dgh_dg_apply(dgh_ctx *ctx, const double *v, double *jv);       /* dg_operator.cpp:10-21 */
 /* Adjoint J^T w of the DG residual's Jacobian at the same linearisation (no counterpart in the
  * reference: the transpose of dg_operator.cpp:10-21 and volume_jacobian.cpp:59-71). */
-int dgh_dg_apply_T(dgh_ctx *ctx, const double *w, double *jtw);
+int dgh_dg_apply_T(dgh_ctx *ctx, const double *w, double *jtw);    /* 2D only */
 /* Diagonal block (row == col), copied to the host row-major m x m (dg_operator.cpp:22-48). */
 int dgh_dg_block(dgh_ctx *ctx, int row, int col, double *host_block);
 

@@ -63,6 +63,42 @@ def test_invalid_configuration_is_rejected_before_any_device_work(lib):
     assert b"Invalid mesh or degree" in lib.dgh_last_error(None)
 
 
+@pytest.mark.parametrize("fields,message", [
+    ({"dim": 3}, "Invalid dimension"),
+    ({"dim": 1, "nx": 2}, "Invalid mesh or degree"),
+    ({"dim": 1, "degree": 3, "quadrature": 3}, "Quadrature must be >= degree+1"),
+    ({"dim": 1, "degree": 3, "quadrature": 21}, "Quadrature above 20 points"),
+    ({"dim": 2, "degree": 3, "quadrature": 6}, "Over-integration (--quad > k+1) is not supported"),
+])
+def test_dimension_and_quadrature_validation(lib, fields, message):
+    """dg_hdg_1d/src/config.cpp:6-21 and the device limits, checked before any device work."""
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    cfg = _lib.dgh_config()
+    lib.dgh_config_default(ctypes.byref(cfg))
+    assert cfg.dim == 2
+    for k, v in fields.items():
+        setattr(cfg, k, v)
+    h = ctypes.c_void_p()
+    assert lib.dgh_ctx_create(ctypes.byref(cfg), ctypes.byref(h)) == 1 and not h.value
+    assert message.encode() in lib.dgh_last_error(None)
+
+
+def test_1d_cli_validates_flags_before_device_work():
+    """The 1D front end parses dg_hdg_1d's flags and refuses the paths it does not build."""
+    import subprocess
+
+    from dg_hdg_euler_cpp_b200 import BIN1D_PATH
+
+    if not BIN1D_PATH.exists():
+        pytest.skip("dgh1d not built")
+    for args, msg in [(["--precond", "block-ilu0"], "block-jacobi only"), (["--linear", "direct"], "CPU-only"),
+                      (["--T", ".1", "--steps", "2"], "Choose either --T or --steps"),
+                      (["--integrator", "rk4"], "Invalid integrator"), (["--bogus"], "Unknown option")]:
+        res = subprocess.run([str(BIN1D_PATH), *args], capture_output=True, text=True, timeout=60)
+        assert res.returncode == 1 and msg in res.stderr, (args, res.stderr)
+
+
 def test_no_cpu_fallback_without_gpu(lib):
     import torch
 
