@@ -25,11 +25,13 @@ template <> struct SlabVec<double> {
     using V = double2;
     static constexpr int W = 2;
     __device__ static double dot(const V &a, const double *y) { return a.x * y[0] + a.y * y[1]; }
+    __device__ static double dotv(const V &a, const V &y) { return a.x * y.x + a.y * y.y; }
 };
 template <> struct SlabVec<float> {
     using V = float4;
     static constexpr int W = 4;
     __device__ static float dot(const V &a, const float *y) { return a.x * y[0] + a.y * y[1] + a.z * y[2] + a.w * y[3]; }
+    __device__ static float dotv(const V &a, const V &y) { return a.x * y.x + a.y * y.y + a.z * y.z + a.w * y.w; }
 };
 template <typename T> __device__ inline size_t slab_at(int nt, int i, int j) {
     constexpr int W = SlabVec<T>::W;
@@ -305,6 +307,8 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     T *y = reinterpret_cast<T *>(smraw) + (size_t)wib * m;
+    // m * sizeof(T) is a multiple of 16 (m = 4n^2 or 4n), so every warp's y is 16-byte aligned
+    const V *yv = reinterpret_cast<const V *>(y);
     const int warps = gridDim.x * (SOLVE_THREADS / 32);
     const int slabs = (m + 31) / 32;
     for (int blk = blockIdx.x * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
@@ -319,18 +323,21 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
             const T *S = A + (size_t)r0 * m;
             const V *Sv = reinterpret_cast<const V *>(S);
             const bool act = lane < nt;
-            T acc0 = 0, acc1 = 0;
+            T acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
             if (act) {
                 const int groups = r0 / W;
                 int g = 0;
-                for (; g + 2 <= groups; g += 2) {
-                    const V a = Sv[(size_t)g * nt + lane], c = Sv[(size_t)(g + 1) * nt + lane];
-                    acc0 += SV::dot(a, y + g * W);
-                    acc1 += SV::dot(c, y + (g + 1) * W);
+                for (; g + 4 <= groups; g += 4) {  // four independent 16-byte loads in flight per lane
+                    const V a0 = Sv[(size_t)g * nt + lane], a1 = Sv[(size_t)(g + 1) * nt + lane];
+                    const V a2 = Sv[(size_t)(g + 2) * nt + lane], a3 = Sv[(size_t)(g + 3) * nt + lane];
+                    acc0 += SV::dotv(a0, yv[g]);
+                    acc1 += SV::dotv(a1, yv[g + 1]);
+                    acc2 += SV::dotv(a2, yv[g + 2]);
+                    acc3 += SV::dotv(a3, yv[g + 3]);
                 }
-                for (; g < groups; ++g) acc0 += SV::dot(Sv[(size_t)g * nt + lane], y + g * W);
+                for (; g < groups; ++g) acc0 += SV::dotv(Sv[(size_t)g * nt + lane], yv[g]);
             }
-            T t = act ? y[r0 + lane] - (acc0 + acc1) : T(0);
+            T t = act ? y[r0 + lane] - ((acc0 + acc1) + (acc2 + acc3)) : T(0);
             for (int jj = 0; jj < nt; ++jj) {
                 const T l = (act && lane > jj) ? S[slab_at<T>(nt, lane, r0 + jj)] : T(0);
                 const T yj = __shfl_sync(0xffffffffu, t, jj);
@@ -345,18 +352,21 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
             const T *S = A + (size_t)r0 * m;
             const V *Sv = reinterpret_cast<const V *>(S);
             const bool act = lane < nt;
-            T acc0 = 0, acc1 = 0;
+            T acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
             if (act) {
                 const int g1 = m / W;
                 int g = hi / W;
-                for (; g + 2 <= g1; g += 2) {
-                    const V a = Sv[(size_t)g * nt + lane], c = Sv[(size_t)(g + 1) * nt + lane];
-                    acc0 += SV::dot(a, y + g * W);
-                    acc1 += SV::dot(c, y + (g + 1) * W);
+                for (; g + 4 <= g1; g += 4) {
+                    const V a0 = Sv[(size_t)g * nt + lane], a1 = Sv[(size_t)(g + 1) * nt + lane];
+                    const V a2 = Sv[(size_t)(g + 2) * nt + lane], a3 = Sv[(size_t)(g + 3) * nt + lane];
+                    acc0 += SV::dotv(a0, yv[g]);
+                    acc1 += SV::dotv(a1, yv[g + 1]);
+                    acc2 += SV::dotv(a2, yv[g + 2]);
+                    acc3 += SV::dotv(a3, yv[g + 3]);
                 }
-                for (; g < g1; ++g) acc0 += SV::dot(Sv[(size_t)g * nt + lane], y + g * W);
+                for (; g < g1; ++g) acc0 += SV::dotv(Sv[(size_t)g * nt + lane], yv[g]);
             }
-            T t = act ? y[r0 + lane] - (acc0 + acc1) : T(0);
+            T t = act ? y[r0 + lane] - ((acc0 + acc1) + (acc2 + acc3)) : T(0);
             for (int jj = nt - 1; jj >= 0; --jj) {
                 const T u = act ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
                 if (lane == jj) t = t / u;
