@@ -10,6 +10,7 @@
 #include "dgh_kernels_init.cuh"
 #include "dgh_kernels_krylov.cuh"
 #include "dgh_kernels_lu.cuh"
+#include "dgh_kernels_lu2.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -110,6 +111,9 @@ struct dgh_ctx {
     int aug_cells = 0;
     void *face_pool = nullptr;
     int *face_perm = nullptr;
+    // left-looking FP64 LU: per-CTA scratch of the panels' L_qq^{-1}, U_qq^{-1}
+    double *lu_tri = nullptr;
+    int lu_grid = 0;
     // GMRES
     double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[3] = {nullptr, nullptr, nullptr}, *gcoef = nullptr;
     long long vld = 0;
@@ -281,6 +285,17 @@ void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, in
     const int grid = std::min(count, c->sms * std::max(1, per_sm));
     k_lu<TF, LU_NB, TC><<<grid, LU_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, perm, c->status, bit,
                                                                slab_out ? 1 : 0);
+    c->launched();
+}
+// The left-looking FP64 LU (dgh_kernels_lu2.cuh): grid = resident CTAs, each with its scratch.
+template <bool AUG>
+void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out) {
+    need(m <= 2 * LL_THREADS && m % 4 == 0, "LU block width unsupported by the left-looking kernel");
+    const size_t smem = lu_left_smem_bytes(m);
+    ck(cudaFuncSetAttribute(k_lu_left<AUG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "lu_left attr");
+    const int grid = std::min(count, c->lu_grid);
+    k_lu_left<AUG><<<grid, LL_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, c->lu_tri, perm, c->status, bit,
+                                                          slab_out ? 1 : 0);
     c->launched();
 }
 // One warp per block; enough warps for every SM to keep its warp slots (and their loads) busy.
@@ -863,6 +878,15 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         }
         if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
         c->gcoef = c->alloc<double>(KR_MAXK);
+        if ((c->has_dg() && !c->mixed()) || c->has_hdg()) {
+            const size_t smem = lu_left_smem_bytes(c->m);
+            ck(cudaFuncSetAttribute(k_lu_left<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+            int per_sm = 0;
+            ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_left<true>, LL_THREADS, smem), "occupancy");
+            c->lu_grid = c->sms * std::max(1, per_sm);
+            const int P = (c->m + LL_NB - 1) / LL_NB;
+            c->lu_tri = c->alloc<double>((size_t)c->lu_grid * P * LL_TRI);
+        }
         c->sync();
     });
     if (rc != DGH_OK) {
@@ -1307,7 +1331,7 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
                                                                           c->basis, c->g, c->inv_step, 0, c->cells);
                 });
                 c->launched();
-                launch_lu<double>(c, (double *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR, true);
+                launch_lu_left<false>(c, (double *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR, true);
             }
             c->check_status();
             c->dg_factored = true;
@@ -1377,9 +1401,7 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
                                                                        c->inv_step, first, count);
             });
             c->launched();
-            launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
-            k_backsolve<double><<<std::min(count, c->sms * 2), LU_THREADS, 0, c->stream>>>(c->aug, (size_t)c->m * ld, c->m, ld, count);
-            c->launched();
+            launch_lu_left<true>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
             DGH_DISPATCH_N(c->n, {
                 k_hdg_schur<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y, c->cy, c->basis,
                                                                     c->g, first, count);

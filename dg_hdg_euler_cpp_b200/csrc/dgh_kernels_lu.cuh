@@ -107,6 +107,127 @@ __device__ void panel_factor(T *P, int rows, int nb, int *swp, T *Li, T *cand_v,
     __syncthreads();
 }
 
+// Trailing update of one column tile with FFMA register tiles: each thread owns 4 rows x 4
+// columns, the rows one pass ahead in registers (FP32 factors).
+template <typename T, int NB, int TC>
+__device__ __forceinline__ void trailing_ffma(T *__restrict__ A, int ld, int k0, int nb, int R, int c0, int tc,
+                                              const int *src, const T *P, const T *U) {
+    constexpr int PP = NB + 1;
+    const int tid = threadIdx.x;
+    const int tx = tid % (TC / 4), ty = tid / (TC / 4);
+    constexpr int TY = LU_THREADS / (TC / 4);
+    T nxt[4][4];
+    auto load_pass = [&](int rb) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int r = min(rb + ty + TY * k, R - 1);
+            const T *rowp = A + (size_t)(k0 + src[nb + r]) * ld + c0 + 4 * tx;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) nxt[k][j] = (4 * tx + j < tc) ? rowp[j] : T(0);
+        }
+    };
+    if (R > 0) load_pass(0);
+    for (int rb = 0; rb < R; rb += 4 * TY) {
+        T acc[4][4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[k][j] = nxt[k][j];
+        if (rb + 4 * TY < R) load_pass(rb + 4 * TY);
+        const T *lrow[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) lrow[k] = P + (size_t)(nb + min(rb + ty + TY * k, R - 1)) * PP;
+        const T *ucol = U + 4 * tx;
+#pragma unroll 4
+        for (int l = 0; l < nb; ++l) {
+            T uu[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) uu[j] = ucol[l * TC + j];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const T lv = lrow[k][l];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[k][j] -= lv * uu[j];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int r = rb + ty + TY * k;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = 4 * tx + j;
+                if (r < R && c < tc) A[(size_t)(k0 + nb + r) * ld + c0 + c] = acc[k][j];
+            }
+        }
+    }
+}
+
+// FP64 DMMA m8n8k4: d = a b + d on one 8x8 tile, a the 8x4 and b the 4x8 operand fragment
+// (lane l holds a[l/4][l%4], b[l%4][l/4] and d[l/4][2(l%4) .. 2(l%4)+1]).
+__device__ __forceinline__ void dmma8x8x4(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// Trailing update of one 32-column tile on the FP64 tensor pipe: each warp owns 32 rows x 32
+// columns (4 x 4 DMMA tiles, 32 accumulators per lane), loads its rows through the panel's
+// gather src[], runs nb/4 k-steps against -L21 (shared panel) and U12 (shared tile), and
+// stores the updated rows in place.
+template <int NB>
+__device__ __forceinline__ void trailing_dmma(double *__restrict__ A, int ld, int k0, int nb, int R, int c0, int tc,
+                                              const int *src, const double *P, const double *U) {
+    constexpr int PP = NB + 1, TC = 32, NW = LU_THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lr = lane >> 2, lc = lane & 3;
+    for (int rb = warp * 32; rb < R; rb += NW * 32) {
+        double c[4][4][2];
+        int srow[4];
+        bool valid[4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            const int r = rb + mt * 8 + lr;
+            valid[mt] = r < R;
+            srow[mt] = valid[mt] ? k0 + src[nb + r] : 0;
+        }
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int col = nt * 8 + 2 * lc + e;
+                    c[mt][nt][e] = (valid[mt] && col < tc) ? A[(size_t)srow[mt] * ld + c0 + col] : 0.;
+                }
+        for (int kk = 0; kk < nb; kk += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) {
+                const int r = rb + mt * 8 + lr;
+                a[mt] = valid[mt] ? -P[(size_t)(nb + r) * PP + kk + lc] : 0.;
+            }
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) b[nt] = U[(kk + lc) * TC + nt * 8 + lr];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) dmma8x8x4(c[mt][nt], a[mt], b[nt]);
+        }
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            if (!valid[mt]) continue;
+            double *row = A + (size_t)(k0 + nb + rb + mt * 8 + lr) * ld + c0;
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int col = nt * 8 + 2 * lc + e;
+                    if (col < tc) row[col] = c[mt][nt][e];
+                }
+        }
+    }
+}
+
 // Right-looking blocked LU.  Row interchanges are never executed one at a time: the columns
 // right of the panel are read through the panel's row permutation when its U12 tile and the
 // trailing rows are formed (a row moved by the panel's pivoting comes from the panel's top
@@ -180,54 +301,9 @@ k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restr
                     for (int q = 0; q < RPT; ++q) U[(rg + RG * q) * TC + c] = out[q];
                 }
                 __syncthreads();
-                // trailing rows: A[k0+nb+r] = A[k0+src[nb+r]] - L21 U12 (loads one pass ahead)
-                const int R = rows - nb;
-                const int tx = tid % (TC / 4), ty = tid / (TC / 4);
-                constexpr int TY = LU_THREADS / (TC / 4);
-                T nxt[4][4];
-                auto load_pass = [&](int rb) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int r = min(rb + ty + TY * k, R - 1);
-                        const T *rowp = A + (size_t)(k0 + src[nb + r]) * ld + c0 + 4 * tx;
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) nxt[k][j] = (4 * tx + j < tc) ? rowp[j] : T(0);
-                    }
-                };
-                if (R > 0) load_pass(0);
-                for (int rb = 0; rb < R; rb += 4 * TY) {
-                    T acc[4][4];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) acc[k][j] = nxt[k][j];
-                    if (rb + 4 * TY < R) load_pass(rb + 4 * TY);
-                    const T *lrow[4];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) lrow[k] = P + (size_t)(nb + min(rb + ty + TY * k, R - 1)) * PP;
-                    const T *ucol = U + 4 * tx;
-#pragma unroll 4
-                    for (int l = 0; l < nb; ++l) {
-                        T uu[4];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) uu[j] = ucol[l * TC + j];
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const T lv = lrow[k][l];
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) acc[k][j] -= lv * uu[j];
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int r = rb + ty + TY * k;
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int c = 4 * tx + j;
-                            if (r < R && c < tc) A[(size_t)(k0 + nb + r) * ld + c0 + c] = acc[k][j];
-                        }
-                    }
-                }
+                // trailing rows: A[k0+nb+r] = A[k0+src[nb+r]] - L21 U12
+                if constexpr (sizeof(T) == 8 && TC == 32) trailing_dmma<NB>(A, ld, k0, nb, rows - nb, c0, tc, src, P, U);
+                else trailing_ffma<T, NB, TC>(A, ld, k0, nb, rows - nb, c0, tc, src, P, U);
                 __syncthreads();
                 for (int i = tid / TC; i < nb; i += LU_THREADS / TC) {
                     const int c = tid % TC;
@@ -538,6 +614,84 @@ k_backsolve(T *__restrict__ pool, size_t stride, int m, int ld, int count) {
                 for (int idx = tid; idx < nt * ct; idx += LU_THREADS) {
                     const int r = idx / ct, c = idx % ct;
                     A[(size_t)(r0 + r) * ld + m + cb + c] = Xs[r][c];
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// FP64 multi-RHS back substitution on the tensor pipe: the same blocking as k_backsolve (32-row
+// blocks from the bottom, 64 right-hand-side columns at a time), with the update
+// X[r0 rows] -= U[r0 rows, l >= hi] X[l rows] done by DMMA: warp w owns the 8 columns
+// 8w..8w+7 of the column block and all 32 rows (4 tiles), k-chunks of 32 are staged in shared
+// memory with pitches 36 and 68 (4 mod 16) so the fragment loads are conflict-free.
+constexpr int BS_RT = 32, BS_CT = 64, BS_KC = 32, BS_UP = 36, BS_XP = 68;
+constexpr size_t backsolve_smem_bytes() {
+    return sizeof(double) * ((size_t)BS_RT * BS_UP + (size_t)BS_KC * BS_XP + (size_t)BS_RT * (BS_CT + 1) +
+                             (size_t)BS_RT * (BS_RT + 1));
+}
+__global__ void __launch_bounds__(LU_THREADS)
+k_backsolve_dmma(double *__restrict__ pool, size_t stride, int m, int ld, int count) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double *Us = reinterpret_cast<double *>(smraw);        // [BS_RT][BS_UP]
+    double *Xk = Us + BS_RT * BS_UP;                        // [BS_KC][BS_XP]
+    double *Xs = Xk + BS_KC * BS_XP;                        // [BS_RT][BS_CT + 1]
+    double *Ud = Xs + BS_RT * (BS_CT + 1);                  // [BS_RT][BS_RT + 1]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, lr = lane >> 2, lc = lane & 3;
+    const int nrhs = ld - m;
+    for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
+        double *A = pool + (size_t)blk * stride;
+        for (int cb = 0; cb < nrhs; cb += BS_CT) {
+            const int ct = min(BS_CT, nrhs - cb);
+            const int last = ((m - 1) / BS_RT) * BS_RT;
+            for (int r0 = last; r0 >= 0; r0 -= BS_RT) {
+                const int nt = min(BS_RT, m - r0), hi = r0 + nt;
+                double c[4][2];
+#pragma unroll
+                for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int r = mt * 8 + lr, col = warp * 8 + 2 * lc + e;
+                        c[mt][e] = (r < nt && col < ct) ? A[(size_t)(r0 + r) * ld + m + cb + col] : 0.;
+                    }
+                for (int l0 = hi; l0 < m; l0 += BS_KC) {
+                    const int kc = min(BS_KC, m - l0);
+                    for (int idx = tid; idx < BS_RT * BS_KC; idx += LU_THREADS) {
+                        const int r = idx / BS_KC, l = idx % BS_KC;
+                        Us[r * BS_UP + l] = (r < nt && l < kc) ? A[(size_t)(r0 + r) * ld + l0 + l] : 0.;
+                    }
+                    for (int idx = tid; idx < BS_KC * BS_CT; idx += LU_THREADS) {
+                        const int l = idx / BS_CT, col = idx % BS_CT;
+                        Xk[l * BS_XP + col] = (l < kc && col < ct) ? A[(size_t)(l0 + l) * ld + m + cb + col] : 0.;
+                    }
+                    __syncthreads();
+                    for (int kk = 0; kk < kc; kk += 4) {
+                        const double b = Xk[(kk + lc) * BS_XP + warp * 8 + lr];
+#pragma unroll
+                        for (int mt = 0; mt < 4; ++mt) dmma8x8x4(c[mt], -Us[(mt * 8 + lr) * BS_UP + kk + lc], b);
+                    }
+                    __syncthreads();
+                }
+#pragma unroll
+                for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) Xs[(mt * 8 + lr) * (BS_CT + 1) + warp * 8 + 2 * lc + e] = c[mt][e];
+                for (int idx = tid; idx < BS_RT * BS_RT; idx += LU_THREADS) {
+                    const int r = idx / BS_RT, col = idx % BS_RT;
+                    Ud[r * (BS_RT + 1) + col] = (r < nt && col < nt) ? A[(size_t)(r0 + r) * ld + r0 + col] : 0.;
+                }
+                __syncthreads();
+                if (tid < ct)
+                    for (int i = nt - 1; i >= 0; --i) {
+                        double val = Xs[i * (BS_CT + 1) + tid];
+                        for (int l = i + 1; l < nt; ++l) val -= Ud[i * (BS_RT + 1) + l] * Xs[l * (BS_CT + 1) + tid];
+                        Xs[i * (BS_CT + 1) + tid] = val / Ud[i * (BS_RT + 1) + i];
+                    }
+                __syncthreads();
+                for (int idx = tid; idx < nt * ct; idx += LU_THREADS) {
+                    const int r = idx / ct, col = idx % ct;
+                    A[(size_t)(r0 + r) * ld + m + cb + col] = Xs[r * (BS_CT + 1) + col];
                 }
                 __syncthreads();
             }
