@@ -111,9 +111,10 @@ struct dgh_ctx {
     int aug_cells = 0;
     void *face_pool = nullptr;
     int *face_perm = nullptr;
-    // left-looking FP64 LU: per-CTA scratch of the panels' L_qq^{-1}, U_qq^{-1}
-    double *lu_tri = nullptr;
-    int lu_grid = 0;
+    // left-looking FP64 LU: per-CTA scratch of the panels' L_qq^{-1}, U_qq^{-1}; FP64 workspace
+    // for the mixed-precision DG blocks (factored in FP64 in chunks, stored as FP32 slabs)
+    double *lu_tri = nullptr, *dg_ws = nullptr;
+    int lu_grid = 0, dg_ws_cells = 0;
     // GMRES
     double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[3] = {nullptr, nullptr, nullptr}, *gcoef = nullptr;
     long long vld = 0;
@@ -289,13 +290,14 @@ void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, in
 }
 // The left-looking FP64 LU (dgh_kernels_lu2.cuh): grid = resident CTAs, each with its scratch.
 template <bool AUG>
-void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out) {
+void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out,
+                    float *out32 = nullptr) {
     need(m <= 2 * LL_THREADS && m % 4 == 0, "LU block width unsupported by the left-looking kernel");
     const size_t smem = lu_left_smem_bytes(m);
     ck(cudaFuncSetAttribute(k_lu_left<AUG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "lu_left attr");
     const int grid = std::min(count, c->lu_grid);
     k_lu_left<AUG><<<grid, LL_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, c->lu_tri, perm, c->status, bit,
-                                                          slab_out ? 1 : 0);
+                                                          slab_out ? 1 : 0, out32);
     c->launched();
 }
 // One warp per block; enough warps for every SM to keep its warp slots (and their loads) busy.
@@ -878,7 +880,13 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         }
         if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
         c->gcoef = c->alloc<double>(KR_MAXK);
-        if ((c->has_dg() && !c->mixed()) || c->has_hdg()) {
+        if (c->has_dg() && c->mixed()) {
+            const size_t per_cell = (size_t)c->m * c->m * sizeof(double);
+            const size_t budget = (size_t)8 << 30;  // FP64 factor workspace: at most 8 GiB
+            c->dg_ws_cells = (int)std::max<size_t>(1, std::min<size_t>(c->cells, budget / per_cell));
+            c->dg_ws = c->alloc<double>((size_t)c->dg_ws_cells * c->m * c->m);
+        }
+        if (c->has_dg() || c->has_hdg()) {
             const size_t smem = lu_left_smem_bytes(c->m);
             ck(cudaFuncSetAttribute(k_lu_left<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
             int per_sm = 0;
@@ -1319,12 +1327,17 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             const size_t stride = (size_t)c->m * c->m;
             const int grid = std::min(c->cells, c->sms * 8);
             if (c->mixed()) {
-                DGH_DISPATCH_N(c->n, {
-                    k_dg_assemble<N, float><<<grid, 256, 0, c->stream>>>((float *)c->dg_pool, c->vol, c->fcache, c->speeds,
-                                                                         c->basis, c->g, c->inv_step, 0, c->cells);
-                });
-                c->launched();
-                launch_lu<float>(c, (float *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR, true);
+                // factor in FP64 chunk by chunk, store FP32 slabs
+                for (int first = 0; first < c->cells; first += c->dg_ws_cells) {
+                    const int count = std::min(c->dg_ws_cells, c->cells - first);
+                    DGH_DISPATCH_N(c->n, {
+                        k_dg_assemble<N, double><<<std::min(count, c->sms * 8), 256, 0, c->stream>>>(
+                            c->dg_ws, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step, first, count);
+                    });
+                    c->launched();
+                    launch_lu_left<false>(c, c->dg_ws, stride, c->m, c->m, count, c->dg_perm + (size_t)first * c->m,
+                                          ST_SINGULAR, false, (float *)c->dg_pool + (size_t)first * stride);
+                }
             } else {
                 DGH_DISPATCH_N(c->n, {
                     k_dg_assemble<N, double><<<grid, 256, 0, c->stream>>>((double *)c->dg_pool, c->vol, c->fcache, c->speeds,

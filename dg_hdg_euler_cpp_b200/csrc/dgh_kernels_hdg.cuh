@@ -147,8 +147,8 @@ template <int N>
 __global__ void __launch_bounds__(256)
 k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
             double *__restrict__ out, Basis1D b, Grid g) {
-    constexpr int FW = NVAR * N, T = NFACES * FW;
-    __shared__ double loc[2][T];
+    constexpr int FW = NVAR * N, T = NFACES * FW, T2 = T / 2, PASSES = (T2 + 31) / 32;
+    __shared__ __align__(16) double loc[2][T];
     const int face = blockIdx.x;
     const int axis = face >= g.cells, first = face - axis * g.cells, next = neighbor(g, first, 2 * axis + 1);
     for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
@@ -158,11 +158,20 @@ k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, con
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double2 *l0 = reinterpret_cast<const double2 *>(loc[0]), *l1 = reinterpret_cast<const double2 *>(loc[1]);
     for (int row = warp; row < FW; row += 8) {
-        const double *s1 = S + (size_t)first * T * T + (size_t)((2 * axis + 1) * FW + row) * T;
-        const double *s2 = S + (size_t)next * T * T + (size_t)((2 * axis) * FW + row) * T;
+        // rows of S_K are T = 16N doubles (an even count), so every row starts 16-byte aligned
+        const double2 *s1 = reinterpret_cast<const double2 *>(S + (size_t)first * T * T + (size_t)((2 * axis + 1) * FW + row) * T);
+        const double2 *s2 = reinterpret_cast<const double2 *>(S + (size_t)next * T * T + (size_t)((2 * axis) * FW + row) * T);
         double acc = 0;
-        for (int j = lane; j < T; j += 32) acc += s1[j] * loc[0][j] + s2[j] * loc[1][j];
+#pragma unroll
+        for (int t = 0; t < PASSES; ++t) {
+            const int j = lane + 32 * t;
+            if (j < T2) {
+                const double2 a = s1[j], b = s2[j], x = l0[j], y = l1[j];
+                acc += a.x * x.x + a.y * x.y + b.x * y.x + b.y * y.y;
+            }
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) {

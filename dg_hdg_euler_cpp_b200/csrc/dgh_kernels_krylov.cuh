@@ -2,7 +2,9 @@
 // classical Gram-Schmidt applied twice and a weighted inner product (gmres.cpp:17-86).
 // Reductions are deterministic: a fixed grid writes per-block partial sums, and k_reduce adds
 // them in a fixed tree order.  The two CGS2 passes are fused so the basis is swept three times
-// per iteration instead of four: dot | axpy+dot | axpy+norm.
+// per iteration instead of four: dot | axpy+dot | axpy+norm.  The sweeps read 16-byte pairs
+// (the basis rows, the work vectors and the metric are 16-byte aligned device buffers); an odd
+// last element is handled by thread 0 of block 0.
 #pragma once
 #include "dgh_common.cuh"
 
@@ -40,7 +42,20 @@ k_mdot(const double *__restrict__ V, size_t ldv, int K, const double *__restrict
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0;
-    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+    const long long n2 = n >> 1;
+    const double2 *x2 = reinterpret_cast<const double2 *>(x), *W2 = reinterpret_cast<const double2 *>(W);
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n2; i += (long long)gridDim.x * KR_THREADS) {
+        const double2 xv = x2[i], wv = W2[i];
+        const double wx0 = wv.x * xv.x, wx1 = wv.y * xv.y;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const double2 v = reinterpret_cast<const double2 *>(V + k * ldv)[i];
+            acc[k] += v.x * wx0;
+            acc[k] += v.y * wx1;
+        }
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long long i = n - 1;
         const double wx = W[i] * x[i];
 #pragma unroll
         for (int k = 0; k < NV; ++k) acc[k] += V[k * ldv + i] * wx;
@@ -60,7 +75,7 @@ k_maxpy_reduce(const double *__restrict__ V, size_t ldv, int K, const double *__
     double acc[MODE == 0 ? NV : 1];
 #pragma unroll
     for (int k = 0; k < (MODE == 0 ? NV : 1); ++k) acc[k] = 0;
-    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+    auto one = [&](long long i) {
         double v[NV];
         double s = 0;
 #pragma unroll
@@ -77,7 +92,37 @@ k_maxpy_reduce(const double *__restrict__ V, size_t ldv, int K, const double *__
         } else {
             acc[0] += xn * wx;
         }
+    };
+    const long long n2 = n >> 1;
+    double2 *x2 = reinterpret_cast<double2 *>(x);
+    const double2 *W2 = reinterpret_cast<const double2 *>(W);
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n2; i += (long long)gridDim.x * KR_THREADS) {
+        double2 v[NV];
+        double s0 = 0, s1 = 0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            v[k] = reinterpret_cast<const double2 *>(V + k * ldv)[i];
+            s0 += v[k].x * hs[k];
+            s1 += v[k].y * hs[k];
+        }
+        double2 xv = x2[i];
+        xv.x -= s0;
+        xv.y -= s1;
+        x2[i] = xv;
+        const double2 wv = W2[i];
+        const double wx0 = wv.x * xv.x, wx1 = wv.y * xv.y;
+        if (MODE == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                acc[k] += v[k].x * wx0;
+                acc[k] += v[k].y * wx1;
+            }
+        } else {
+            acc[0] += xv.x * wx0;
+            acc[0] += xv.y * wx1;
+        }
     }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) one(n - 1);
     block_reduce_store<MODE == 0 ? NV : 1>(acc, MODE == 0 ? K : 1, partial, gridDim.x);
 }
 
@@ -106,11 +151,22 @@ k_lincomb(const double *__restrict__ V, size_t ldv, int K, const double *__restr
     __shared__ double cs[KR_MAXK];
     if (threadIdx.x < K) cs[threadIdx.x] = c[threadIdx.x];
     __syncthreads();
-    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * KR_THREADS) {
+    const long long n2 = n >> 1;
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n2; i += (long long)gridDim.x * KR_THREADS) {
+        double s0 = 0, s1 = 0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const double2 v = reinterpret_cast<const double2 *>(V + k * ldv)[i];
+            s0 += v.x * cs[k];
+            s1 += v.y * cs[k];
+        }
+        reinterpret_cast<double2 *>(out)[i] = make_double2(s0, s1);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         double s = 0;
 #pragma unroll
-        for (int k = 0; k < NV; ++k) s += V[k * ldv + i] * cs[k];
-        out[i] = s;
+        for (int k = 0; k < NV; ++k) s += V[k * ldv + n - 1] * cs[k];
+        out[n - 1] = s;
     }
 }
 

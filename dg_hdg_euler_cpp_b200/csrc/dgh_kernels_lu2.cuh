@@ -158,13 +158,16 @@ __device__ __forceinline__ void ll_prefetch(const double *__restrict__ A, int ld
 // Batched LU.  AUG = false: pool holds m x m blocks (ld = m); on exit row i of each block is
 // position i of the factors (unit L below, U on and above the diagonal), perm_out[i] = its
 // original row, and with slab_out the block is rewritten in the slab layout of k_lu_solve.
+// With out32 != nullptr the factors are instead written, rounded to FP32, in the FP32 slab
+// layout to out32 (m x m per block) and pool is left in original-row order: the mixed
+// precision preconditioner factors in FP64 and stores FP32.
 // AUG = true: pool holds [A | B | r] with ld > m; on exit columns m..ld-1 hold A^{-1}[B r]
 // (row i = unknown i); the A part holds the factors in original-row order (not used later).
 // tri: per-CTA scratch of ceil(m/32) * LL_TRI doubles.
 template <bool AUG>
 __global__ void __launch_bounds__(LL_THREADS, 2)
 k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, double *__restrict__ tri_all,
-          int *__restrict__ perm_out, int *status, int singular_bit, int slab_out) {
+          int *__restrict__ perm_out, int *status, int singular_bit, int slab_out, float *__restrict__ out32) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int mp = (m + LL_NB - 1) / LL_NB * LL_NB, P = mp / LL_NB;
     double *acc = reinterpret_cast<double *>(smraw);  // mp rows x LL_AP
@@ -450,6 +453,21 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 }
                 __syncthreads();
             }
+        } else if (out32) {
+            // ---- FP32 slabs straight from the original-row storage: stage 32 position rows
+            constexpr int W = SlabVec<float>::W;
+            double *stage = acc;  // 32 rows x m doubles fit: 32 * m <= mp * LL_AP
+            for (int r0 = 0; r0 < m; r0 += 32) {
+                const int nt = min(32, m - r0);
+                for (int idx = tid; idx < nt * m; idx += LL_THREADS)
+                    stage[idx] = A[(size_t)piv[r0 + idx / m] * ld + idx % m];
+                __syncthreads();
+                float *reg = out32 + (size_t)blk * m * m + (size_t)r0 * m;
+                for (int g = warp; g < m / W; g += NW)
+                    for (int e = lane; e < nt * W; e += 32) reg[(size_t)g * nt * W + e] = (float)stage[(e / W) * m + g * W + e % W];
+                __syncthreads();
+            }
+            for (int i = tid; i < m; i += LL_THREADS) perm_out[(size_t)blk * m + i] = piv[i];
         } else {
             // ---- gather the rows into position order, 32 columns at a time
             for (int c0 = 0; c0 < m; c0 += LL_NB) {
