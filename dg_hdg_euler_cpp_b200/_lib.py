@@ -110,6 +110,7 @@ SIGNATURES = {
     "dgh_hdg_recover": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_hdg_recovered_residual": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_gmres": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, ctypes.c_int, ctypes.c_double, _I, _D]),
+    "dgh_gmres_graph_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dgh_gmres_residual": (_VP, [_VP, ctypes.c_int]),
     "dgh_integrator_create": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_VP)]),
     "dgh_integrator_destroy": (ctypes.c_int, [_VP]),

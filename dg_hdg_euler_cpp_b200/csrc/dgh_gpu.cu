@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
@@ -117,7 +118,18 @@ struct dgh_ctx {
     int lu_grid = 0, dg_ws_cells = 0;
     // GMRES
     double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[3] = {nullptr, nullptr, nullptr}, *gcoef = nullptr;
+    double *g_rhs = nullptr, *g_x = nullptr;  // the solve's own copies of rhs and x (fixed graph operands)
+    GmresDev *gdev = nullptr;
     long long vld = 0;
+    // one captured restart cycle per operator (conditional Arnoldi steps), rebuilt when the
+    // captured stage scalar (1/tau, a kernel argument of J*v) changes
+    struct CycleGraph {
+        cudaGraphExec_t exec = nullptr;
+        double inv_step = 0;
+        int launches_fixed = 0, launches_step = 0;
+    } cycle[3];
+    bool use_graph = false;
+    cudaStream_t aux = nullptr;  // captures the conditional bodies
     // optional CUDA-event timers per kernel class (dgh_timing_enable / dgh_timing_read)
     struct TimerRec { int cat; cudaEvent_t a, b; };
     bool timing = false;
@@ -476,92 +488,193 @@ void axpby(dgh_ctx *c, double a, const double *x, double b, const double *y, dou
     c->launched();
 }
 
-// gmres.cpp:17-86 with the CGS2 passes fused as dot | axpy+dot | axpy+norm.
-void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
-    const long long n = op == DGH_OP_HDG ? c->NT : c->N;
-    const double *W = op == DGH_OP_HDG ? c->inv_trace_mass : c->inv_mass;
-    const int restart = (int)std::min<long long>(n, c->cfg.restart);
-    double *r = c->gres[op], *w = c->gw, *z = c->gz, *V = c->V;
+// gmres.cpp:17-86 with the CGS2 passes fused as dot | axpy+dot | axpy+norm.  One restart cycle
+// is three segments: start (beta, V0 = r / beta, k_gmres_init), up to `restart` Arnoldi steps
+// (preconditioner, operator, three sweeps, normalisation, k_gmres_update), and finish (back
+// substitution, x += M^{-1} V y, true residual and its norm).  The cycle is either launched step
+// by step (the host reads the device's continue flag after every step) or replayed as one CUDA
+// graph whose steps are conditional nodes; the kernels and hence the numbers are the same.
+struct GmresCall {
+    int op;
+    long long n;
+    const double *W;
+    double *r;
+    int restart;
+};
+int gmres_start(dgh_ctx *c, const GmresCall &g, cudaGraphConditionalHandle h, int use_h) {
+    k_wnorm2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(g.r, g.W, 0, g.n, c->partial);
+    k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, c->red + 2 * KR_MAXK);
+    k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(g.r, c->red + 2 * KR_MAXK, 1, c->V, g.n);
+    k_gmres_init<<<1, 32, 0, c->stream>>>(c->gdev, c->red + 2 * KR_MAXK, h, use_h);
+    c->launched(4);
+    return 4;
+}
+int gmres_step(dgh_ctx *c, const GmresCall &g, int j, cudaGraphConditionalHandle h, int use_h) {
     const size_t ld = (size_t)c->vld;
+    double *V = c->V, *w = c->gw, *z = c->gz;
     double *h1 = c->red, *h2 = c->red + KR_MAXK, *nrm = c->red + 2 * KR_MAXK;
-    std::vector<double> H((size_t)(restart + 1) * restart), cs(restart), sn(restart), g(restart + 1), y(restart);
-    auto Hc = [&](int i, int j) -> double & { return H[(size_t)j * (restart + 1) + i]; };
-    ck(cudaMemsetAsync(x, 0, n * sizeof(double), c->stream), "memset");
-    ck(cudaMemcpyAsync(r, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
-    const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(rhs, W, false, n)));
+    const int64_t before = c->launches;
+    precond_apply(c, g.op, V + (size_t)j * ld, z);
+    op_apply(c, g.op, z, w);
+    {
+        Timed tm(c, DGH_TIMER_ARNOLDI);
+        mdot(c, V, ld, j + 1, w, g.W, g.n, h1);
+        maxpy_dot(c, V, ld, j + 1, h1, w, g.W, g.n, h2);
+        maxpy_norm(c, V, ld, j + 1, h2, w, g.W, g.n, nrm);
+        k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(w, nrm, 1, V + (size_t)(j + 1) * ld, g.n);
+        c->launched();
+    }
+    k_gmres_update<<<1, 32, 0, c->stream>>>(c->gdev, c->red, j, h, use_h);
+    c->launched();
+    return (int)(c->launches - before);
+}
+int gmres_finish(dgh_ctx *c, const GmresCall &g) {
+    const int64_t before = c->launches;
+    k_gmres_backsolve<<<1, 32, 0, c->stream>>>(c->gdev, c->gcoef);
+    k_lincomb_dyn<<<c->red_grid, KR_THREADS, 0, c->stream>>>(c->V, (size_t)c->vld, &c->gdev->count, c->gcoef, c->gw, g.n);
+    c->launched(2);
+    precond_apply(c, g.op, c->gw, c->gz);
+    axpby(c, 1., c->g_x, 1., c->gz, c->g_x, g.n);
+    op_apply(c, g.op, c->g_x, c->gw);
+    axpby(c, 1., c->g_rhs, -1., c->gw, g.r, g.n);
+    k_wnorm2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(g.r, g.W, 0, g.n, c->partial);
+    k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, &c->gdev->rnorm2);
+    c->launched(2);
+    return (int)(c->launches - before);
+}
+// Captures one restart cycle of operator op: the start and finish segments on the context's
+// stream, each Arnoldi step j inside an IF node with its own conditional handle h_j (a handle
+// belongs to one conditional node), the body captured on the auxiliary stream.  The start kernel
+// sets h_0 and the step-j kernel sets h_{j+1}; every handle defaults to 0 at launch, so once a
+// step breaks (or does not run) all later steps are skipped.  The kernels capture their
+// arguments, so the graph is rebuilt when the stage scalar 1/tau of the DG operators changes.
+void build_cycle_graph(dgh_ctx *c, const GmresCall &g) {
+    auto &cg = c->cycle[g.op];
+    if (cg.exec) ck(cudaGraphExecDestroy(cg.exec), "cudaGraphExecDestroy");
+    cg.exec = nullptr;
+    if (!c->aux) ck(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking), "cudaStreamCreate");
+    const bool timing = c->timing;
+    c->timing = false;  // no event records inside a captured graph
+    const int64_t launches0 = c->launches;
+    cudaStream_t main = c->stream;
+    cudaGraph_t cap = nullptr;
+    ck(cudaGraphCreate(&cap, 0), "cudaGraphCreate");
+    std::vector<cudaGraphConditionalHandle> h(g.restart);
+    for (auto &hj : h)
+        ck(cudaGraphConditionalHandleCreate(&hj, cap, 0, cudaGraphCondAssignDefault), "cudaGraphConditionalHandleCreate");
+    ck(cudaStreamBeginCaptureToGraph(main, cap, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+       "cudaStreamBeginCaptureToGraph");
+    cudaStreamCaptureStatus st;
+    int fixed = gmres_start(c, g, h[0], 1), per_step = 0;
+    for (int j = 0; j < g.restart; ++j) {
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        ck(cudaStreamGetCaptureInfo(main, &st, nullptr, nullptr, &deps, &nd), "cudaStreamGetCaptureInfo");
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h[j];
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        ck(cudaGraphAddNode(&node, cap, deps, nd, &cp), "cudaGraphAddNode");
+        ck(cudaStreamUpdateCaptureDependencies(main, &node, 1, cudaStreamSetCaptureDependencies),
+           "cudaStreamUpdateCaptureDependencies");
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ck(cudaStreamBeginCaptureToGraph(c->aux, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+           "cudaStreamBeginCaptureToGraph");
+        c->stream = c->aux;
+        per_step = j + 1 < g.restart ? gmres_step(c, g, j, h[j + 1], 1) : gmres_step(c, g, j, h[j], 0);
+        c->stream = main;
+        ck(cudaStreamEndCapture(c->aux, &body), "cudaStreamEndCapture (body)");
+    }
+    fixed += gmres_finish(c, g);
+    ck(cudaStreamEndCapture(main, &cap), "cudaStreamEndCapture");
+    ck(cudaGraphInstantiate(&cg.exec, cap, 0), "cudaGraphInstantiate");
+    ck(cudaGraphDestroy(cap), "cudaGraphDestroy");
+    c->timing = timing;
+    c->launches = launches0;  // counted when replayed
+    cg.inv_step = c->inv_step;
+    cg.launches_fixed = fixed;
+    cg.launches_step = per_step;
+}
+
+__global__ void k_gmres_setup(GmresDev *d, double rhs_norm, double tol, int limit, int restart) {
+    if (threadIdx.x != 0) return;
+    d->rhs_norm = rhs_norm;
+    d->tol = tol;
+    d->limit = limit;
+    d->restart = restart;
+    d->iters = 0;
+    d->status = 0;
+    d->count = 0;
+}
+
+void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
+    GmresCall g;
+    g.op = op;
+    g.n = op == DGH_OP_HDG ? c->NT : c->N;
+    g.W = op == DGH_OP_HDG ? c->inv_trace_mass : c->inv_mass;
+    g.restart = (int)std::min<long long>(g.n, c->cfg.restart);
+    g.r = c->gres[op];
+    const long long n = g.n;
+    ck(cudaMemcpyAsync(c->g_rhs, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    ck(cudaMemsetAsync(c->g_x, 0, n * sizeof(double), c->stream), "memset");
+    ck(cudaMemcpyAsync(g.r, c->g_rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(c->g_rhs, g.W, false, n)));
     iters = 0;
     rel = 0;
-    if (rhs_norm == 0) return;
-    while (iters < limit) {
-        // beta = ||r||; V0 = r / beta
-        k_wnorm2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(r, W, 0, n, c->partial);
-        k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, nrm);
-        k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(r, nrm, 1, V, n);
-        c->launched(3);
-        ck(cudaMemcpyAsync(c->pinned, nrm, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
-        c->sync();
-        const double beta = std::sqrt(std::max(0.0, c->pinned[0]));
-        if (beta <= tol * rhs_norm) {
-            rel = beta / rhs_norm;
-            return;
-        }
-        std::fill(H.begin(), H.end(), 0.);
-        std::fill(g.begin(), g.end(), 0.);
-        g[0] = beta;
-        int count = 0;
-        for (int j = 0; j < restart && iters < limit; ++j) {
-            precond_apply(c, op, V + (size_t)j * ld, z);
-            op_apply(c, op, z, w);
-            {
-                Timed tm(c, DGH_TIMER_ARNOLDI);
-                mdot(c, V, ld, j + 1, w, W, n, h1);
-                maxpy_dot(c, V, ld, j + 1, h1, w, W, n, h2);
-                maxpy_norm(c, V, ld, j + 1, h2, w, W, n, nrm);
-                k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(w, nrm, 1, V + (size_t)(j + 1) * ld, n);
-                c->launched();
-            }
-            ck(cudaMemcpyAsync(c->pinned, c->red, (2 * KR_MAXK + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
-               "copy");
-            c->sync();
-            const double *hh1 = c->pinned, *hh2 = c->pinned + KR_MAXK;
-            for (int i = 0; i <= j; ++i) Hc(i, j) = (0. + hh1[i]) + hh2[i];
-            const double next = std::sqrt(std::max(0.0, c->pinned[2 * KR_MAXK]));
-            Hc(j + 1, j) = next;
-            for (int i = 0; i < j; ++i) {
-                const double a = Hc(i, j), b = Hc(i + 1, j);
-                Hc(i, j) = cs[i] * a + sn[i] * b;
-                Hc(i + 1, j) = -sn[i] * a + cs[i] * b;
-            }
-            const double d = std::hypot(Hc(j, j), Hc(j + 1, j));
-            if (!(std::isfinite(d) && d > 0)) fail(DGH_ERR_BREAKDOWN, "GMRES Arnoldi breakdown");
-            cs[j] = Hc(j, j) / d;
-            sn[j] = Hc(j + 1, j) / d;
-            Hc(j, j) = d;
-            Hc(j + 1, j) = 0;
-            g[j + 1] = -sn[j] * g[j];
-            g[j] *= cs[j];
-            ++iters;
-            count = j + 1;
-            if (std::abs(g[j + 1]) <= tol * rhs_norm || next <= std::numeric_limits<double>::min()) break;
-        }
-        for (int i = count - 1; i >= 0; --i) {
-            double value = g[i];
-            for (int j = i + 1; j < count; ++j) value -= Hc(i, j) * y[j];
-            y[i] = value / Hc(i, i);
-        }
-        std::memcpy(c->pinned, y.data(), count * sizeof(double));
-        ck(cudaMemcpyAsync(c->gcoef, c->pinned, count * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
-        lincomb(c, V, ld, count, c->gcoef, w, n);
-        precond_apply(c, op, w, z);
-        axpby(c, 1., x, 1., z, x, n);
-        op_apply(c, op, x, w);
-        axpby(c, 1., rhs, -1., w, r, n);
-        const double rn = std::sqrt(std::max(0.0, c->reduce_scalar(r, W, false, n)));
-        rel = rn / rhs_norm;
-        if (!std::isfinite(rel)) fail(DGH_ERR_NONFINITE, "Nonfinite GMRES residual");
-        if (rel <= tol) return;
+    auto copy_out = [&] { ck(cudaMemcpyAsync(x, c->g_x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy"); };
+    if (rhs_norm == 0) {
+        copy_out();
+        return;
     }
-    fail(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+    k_gmres_setup<<<1, 32, 0, c->stream>>>(c->gdev, rhs_norm, tol, limit, g.restart);
+    c->launched();
+    struct Tail {
+        double rhs_norm, tol, beta, rnorm2;
+        int iters, limit, count, cont, status, restart;
+    };
+    static_assert(sizeof(Tail) <= 4096, "pinned scratch");
+    const size_t tail_off = offsetof(GmresDev, rhs_norm);
+    for (;;) {
+        if (c->use_graph) {
+            auto &cg = c->cycle[op];
+            if (!cg.exec || (op != DGH_OP_HDG && cg.inv_step != c->inv_step)) build_cycle_graph(c, g);
+            ck(cudaGraphLaunch(cg.exec, c->stream), "cudaGraphLaunch");
+        } else {
+            gmres_start(c, g, 0, 0);
+            for (int j = 0; j < g.restart; ++j) {
+                ck(cudaMemcpyAsync(c->pinned, &c->gdev->cont, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "copy");
+                c->sync();
+                int cont = 0;
+                std::memcpy(&cont, c->pinned, sizeof(int));
+                if (!cont) break;
+                gmres_step(c, g, j, 0, 0);
+            }
+            gmres_finish(c, g);
+        }
+        ck(cudaMemcpyAsync(c->pinned, reinterpret_cast<const char *>(c->gdev) + tail_off, sizeof(Tail),
+                           cudaMemcpyDeviceToHost, c->stream), "copy");
+        c->sync();
+        Tail t;
+        std::memcpy(&t, c->pinned, sizeof(Tail));
+        if (c->use_graph)  // the graph's kernels, counted per replay
+            c->launches += c->cycle[op].launches_fixed + (int64_t)t.count * c->cycle[op].launches_step;
+        iters = t.iters;
+        if (t.status) fail(DGH_ERR_BREAKDOWN, "GMRES Arnoldi breakdown");
+        if (t.count == 0) {
+            if (t.beta <= tol * rhs_norm) {
+                rel = t.beta / rhs_norm;
+                break;
+            }
+            fail(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+        }
+        rel = std::sqrt(std::max(0.0, t.rnorm2)) / rhs_norm;
+        if (!std::isfinite(rel)) fail(DGH_ERR_NONFINITE, "Nonfinite GMRES residual");
+        if (rel <= tol) break;
+        if (iters >= limit) fail(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+    }
+    copy_out();
 }
 
 void build_rule(dgh_ctx *c) {
@@ -713,6 +826,10 @@ void create1(dgh_ctx *c, const dgh_config &k) {
     }
     if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
     c->gcoef = c->alloc<double>(KR_MAXK);
+    c->g_rhs = c->alloc<double>(vn);
+    c->g_x = c->alloc<double>(vn);
+    c->gdev = c->alloc<GmresDev>(1);
+    ck(cudaMemset(c->V, 0, sizeof(double) * (size_t)c->vld * (k.restart + 1)), "memset");
     c->sync();
 }
 }  // namespace
@@ -880,6 +997,10 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         }
         if (c->has_hdg()) c->gres[DGH_OP_HDG] = c->alloc<double>(c->NT);
         c->gcoef = c->alloc<double>(KR_MAXK);
+        c->g_rhs = c->alloc<double>(vn);
+        c->g_x = c->alloc<double>(vn);
+        c->gdev = c->alloc<GmresDev>(1);
+        ck(cudaMemset(c->V, 0, sizeof(double) * (size_t)c->vld * (k.restart + 1)), "memset");
         if (c->has_dg() && c->mixed()) {
             const size_t per_cell = (size_t)c->m * c->m * sizeof(double);
             const size_t budget = (size_t)8 << 30;  // FP64 factor workspace: at most 8 GiB
@@ -916,6 +1037,9 @@ int dgh_ctx_destroy(dgh_ctx *c) {
     for (auto e : c->spare) cudaEventDestroy(e);
     for (void *p : c->owned) cudaFree(p);
     if (c->pinned) cudaFreeHost(c->pinned);
+    for (auto &g : c->cycle)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (c->aux) cudaStreamDestroy(c->aux);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return DGH_OK;
@@ -1506,6 +1630,9 @@ int dgh_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, doubl
         if (iterations) *iterations = it;
         if (relative) *relative = rel;
     });
+}
+int dgh_gmres_graph_enable(dgh_ctx *c, int on) {
+    return guard(c, [&] { c->use_graph = on != 0; });
 }
 const double *dgh_gmres_residual(dgh_ctx *c, int op) {
     if (!c || op < 0 || op > 2) return nullptr;

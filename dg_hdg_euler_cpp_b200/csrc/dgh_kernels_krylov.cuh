@@ -216,4 +216,107 @@ k_rho2(const double *__restrict__ u, const double *__restrict__ mass, int plane,
     block_reduce_store<1>(acc, 1, partial, gridDim.x);
 }
 
+// ---- Device-resident GMRES control (gmres.cpp:24-86): the Hessenberg column, the Givens
+// rotations, the inner-loop break and the least-squares back substitution run in one-thread
+// kernels, so a whole restart cycle can be replayed as one CUDA graph whose Arnoldi steps are
+// conditional nodes (the break of gmres.cpp:65-67 sets the condition to zero).  The same kernels
+// run when the cycle is launched step by step, so both ways give the same numbers.  Each step's
+// conditional node has its own handle, set by the kernel that precedes the step.
+struct GmresDev {
+    double H[(KR_MAXK + 1) * KR_MAXK];  // column-major, leading dimension KR_MAXK + 1
+    double cs[KR_MAXK], sn[KR_MAXK], g[KR_MAXK + 1], y[KR_MAXK];
+    double rhs_norm, tol, beta, rnorm2;
+    int iters, limit, count, cont, status, restart;
+};
+
+// Cycle start: beta = ||r|| (from the reduction at nrm2), g = beta e_1, and whether to iterate
+// (gmres.cpp:25-27 and the loop condition of :33).
+__global__ void k_gmres_init(GmresDev *d, const double *nrm2, cudaGraphConditionalHandle h, int use_h) {
+    if (threadIdx.x != 0) return;
+    const double beta = sqrt(fmax(0., *nrm2));
+    d->beta = beta;
+    for (int i = 0; i < (KR_MAXK + 1) * KR_MAXK; ++i) d->H[i] = 0.;
+    for (int i = 0; i <= KR_MAXK; ++i) d->g[i] = 0.;
+    d->g[0] = beta;
+    d->count = 0;
+    const int cont = !(beta <= d->tol * d->rhs_norm) && d->restart > 0 && d->iters < d->limit;
+    d->cont = cont;
+    if (use_h) cudaGraphSetConditional(h, cont);
+}
+
+// After the CGS2 sweeps of step j: column j of H from the two projections (red[0..j],
+// red[KR_MAXK..]) and the norm (red[2 KR_MAXK]), the earlier rotations, the new rotation, the
+// rotated right-hand side and the break test (gmres.cpp:42-67).  In a captured cycle h is the
+// handle of step j+1's conditional node.
+__global__ void k_gmres_update(GmresDev *d, const double *red, int j, cudaGraphConditionalHandle h, int use_h) {
+    if (threadIdx.x != 0) return;
+    constexpr int LDH = KR_MAXK + 1;
+    double *H = d->H + (size_t)j * LDH;
+    for (int i = 0; i <= j; ++i) H[i] = (0. + red[i]) + red[KR_MAXK + i];
+    const double next = sqrt(fmax(0., red[2 * KR_MAXK]));
+    H[j + 1] = next;
+    for (int i = 0; i < j; ++i) {
+        const double a = H[i], b = H[i + 1];
+        H[i] = d->cs[i] * a + d->sn[i] * b;
+        H[i + 1] = -d->sn[i] * a + d->cs[i] * b;
+    }
+    const double dd = hypot(H[j], H[j + 1]);
+    if (!(isfinite(dd) && dd > 0)) {  // "GMRES Arnoldi breakdown", reported by the host
+        d->status = 1;
+        d->cont = 0;
+        if (use_h) cudaGraphSetConditional(h, 0);
+        return;
+    }
+    d->cs[j] = H[j] / dd;
+    d->sn[j] = H[j + 1] / dd;
+    H[j] = dd;
+    H[j + 1] = 0;
+    d->g[j + 1] = -d->sn[j] * d->g[j];
+    d->g[j] *= d->cs[j];
+    d->iters += 1;
+    d->count = j + 1;
+    const int cont = !(fabs(d->g[j + 1]) <= d->tol * d->rhs_norm || next <= 2.2250738585072014e-308) &&
+                     j + 1 < d->restart && d->iters < d->limit;
+    d->cont = cont;
+    if (use_h) cudaGraphSetConditional(h, cont);
+}
+
+// y = H(0:count, 0:count)^{-1} g (gmres.cpp:69-74); coef = y padded with zeros.
+__global__ void k_gmres_backsolve(GmresDev *d, double *coef) {
+    if (threadIdx.x != 0) return;
+    constexpr int LDH = KR_MAXK + 1;
+    const int cnt = d->count;
+    for (int i = cnt - 1; i >= 0; --i) {
+        double value = d->g[i];
+        for (int jj = i + 1; jj < cnt; ++jj) value -= d->H[(size_t)jj * LDH + i] * d->y[jj];
+        d->y[i] = value / d->H[(size_t)i * LDH + i];
+    }
+    for (int k = 0; k < KR_MAXK; ++k) coef[k] = k < cnt ? d->y[k] : 0.;
+}
+
+// out[i] = sum_{k < *count} V_k[i] c_k with the basis size read on the device.
+__global__ void __launch_bounds__(KR_THREADS)
+k_lincomb_dyn(const double *__restrict__ V, size_t ldv, const int *countp, const double *__restrict__ c,
+              double *__restrict__ out, long long n) {
+    __shared__ double cs[KR_MAXK];
+    const int K = *countp;
+    if (threadIdx.x < KR_MAXK) cs[threadIdx.x] = threadIdx.x < K ? c[threadIdx.x] : 0.;
+    __syncthreads();
+    const long long n2 = n >> 1;
+    for (long long i = (long long)blockIdx.x * KR_THREADS + threadIdx.x; i < n2; i += (long long)gridDim.x * KR_THREADS) {
+        double s0 = 0, s1 = 0;
+        for (int k = 0; k < K; ++k) {
+            const double2 v = reinterpret_cast<const double2 *>(V + k * ldv)[i];
+            s0 += v.x * cs[k];
+            s1 += v.y * cs[k];
+        }
+        reinterpret_cast<double2 *>(out)[i] = make_double2(s0, s1);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        double s = 0;
+        for (int k = 0; k < K; ++k) s += V[k * ldv + n - 1] * cs[k];
+        out[n - 1] = s;
+    }
+}
+
 }  // namespace dgh

@@ -22,6 +22,7 @@ void require(bool c, const std::string &m) {
 struct Options {
     dgh_config cfg;
     std::string method = "both", prefix = "output/run_2d", integrator = "ssp-dirk3", testcase = "diagonal";
+    bool graph = false;
     bool timing_only = false, save_solution = true, direct = false;
 };
 Options parse(int argc, char **argv) {
@@ -72,6 +73,7 @@ Options parse(int argc, char **argv) {
         else if (option == "--max-linear") c.max_linear = integer();
         else if (option == "--max-newton") c.max_newton = integer();
         else if (option == "--device") c.device = integer();
+        else if (option == "--graph") o.graph = true;
         else if (option == "--precision") {
             auto p = value();
             require(p == "fp64" || p == "mixed", "Invalid precision");
@@ -93,7 +95,7 @@ Options parse(int argc, char **argv) {
                          "--ordering natural --restart N --max-linear N --max-newton N\n"
                          "--ntol R --ltol R --safety S --prefix PATH\n"
                          "--integrator ssp-dirk3|be --newton-steps N --warmup-updates N\n"
-                         "--timing-only --check-update --no-save-solution --precision fp64|mixed --device N\n";
+                         "--graph --timing-only --check-update --no-save-solution --precision fp64|mixed --device N\n";
             std::exit(0);
         } else
             throw std::runtime_error("Unknown option: " + option);
@@ -182,6 +184,7 @@ int main(int argc, char **argv) {
             auto ck = [&](int rc) {
                 if (rc != DGH_OK) throw std::runtime_error(dgh_last_error(ctx));
             };
+            if (o.graph) ck(dgh_gmres_graph_enable(ctx, 1));
             int64_t s[8];
             ck(dgh_sizes(ctx, s));
             const int64_t N = s[0], NT = s[1];

@@ -235,6 +235,10 @@ class Solver:
         return out
 
     # ---- GMRES
+    def gmres_graph(self, on: bool = True):
+        """Replay each GMRES restart cycle as one CUDA graph (dgh_gmres_graph_enable)."""
+        self._rc(self.lib.dgh_gmres_graph_enable(self.h, 1 if on else 0))
+
     def gmres(self, op: str, rhs, limit: int, tol: float):
         """Returns (x, iterations, relative residual, true residual)."""
         x = self.vec(self.trace_size if op == "hdg" else self.size)

@@ -173,6 +173,12 @@ int dgh_hdg_recovered_residual(dgh_ctx *ctx, const double *e, double *out); /* h
 int dgh_gmres(dgh_ctx *ctx, int op, const double *rhs, double *x, int limit, double tol,
               int *iterations, double *relative);
 /* Device pointer to the true residual rhs - A x of the last dgh_gmres call on op. */
+/* Replay each GMRES restart cycle as one CUDA graph (its Arnoldi steps are conditional nodes
+ * that stop at the reference's inner-loop break, gmres.cpp:65-67) instead of launching it step
+ * by step with a host read of the continue flag after every step.  Both ways run the same
+ * kernels and give the same results; the graph removes the per-step host round trip.  Off by
+ * default.  No counterpart in the reference. */
+int dgh_gmres_graph_enable(dgh_ctx *ctx, int on);
 const double *dgh_gmres_residual(dgh_ctx *ctx, int op);
 
 /* ---- TimeIntegrator (time_integrator.hpp:21-40, time_integrator.cpp:48-213) ------------------ */
