@@ -28,7 +28,7 @@ class dgh_config(ctypes.Structure):
         ("nonlinear_tolerance", ctypes.c_double), ("linear_tolerance", ctypes.c_double),
         ("method", ctypes.c_int), ("integrator", ctypes.c_int), ("testcase", ctypes.c_int),
         ("precision", ctypes.c_int), ("check_update", ctypes.c_int), ("device", ctypes.c_int),
-        ("dim", ctypes.c_int),
+        ("dim", ctypes.c_int), ("autotune", ctypes.c_int),
     ]
 
 
@@ -110,6 +110,7 @@ SIGNATURES = {
     "dgh_hdg_recover": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_hdg_recovered_residual": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_gmres": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, ctypes.c_int, ctypes.c_double, _I, _D]),
+    "dgh_autotune_report": (ctypes.c_int, [_VP, _D]),
     "dgh_gmres_graph_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dgh_gmres_residual": (_VP, [_VP, ctypes.c_int]),
     "dgh_integrator_create": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_VP)]),

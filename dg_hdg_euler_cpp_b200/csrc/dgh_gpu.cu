@@ -17,7 +17,10 @@
 #include <cstddef>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <stdexcept>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -116,6 +119,10 @@ struct dgh_ctx {
     // for the mixed-precision DG blocks (factored in FP64 in chunks, stored as FP32 slabs)
     double *lu_tri = nullptr, *dg_ws = nullptr;
     int lu_grid = 0, dg_ws_cells = 0;
+    // per-degree autotuner: chosen factorisation variants (-1 until the first refresh) and the
+    // tuning times
+    int dg_variant = -1, hdg_variant = -1;
+    double tune_ms[4] = {0, 0, 0, 0};
     // GMRES
     double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[3] = {nullptr, nullptr, nullptr}, *gcoef = nullptr;
     double *g_rhs = nullptr, *g_x = nullptr;  // the solve's own copies of rhs and x (fixed graph operands)
@@ -1409,6 +1416,116 @@ int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
     });
 }
 
+}  // extern "C"
+
+// ---- factorisation variants and the per-degree autotuner ------------------------------------------
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int>, int> g_tune_cache;  // (kind, n, precision) -> variant
+
+// DG blocks of cells [first, first + count): assembly and LU with the given variant.
+void dg_factor(dgh_ctx *c, int variant, int first, int count) {
+    const size_t stride = (size_t)c->m * c->m;
+    const int grid = std::min(count, c->sms * 8);
+    if (c->mixed()) {
+        if (variant == 0) {  // FP64 left-looking in the workspace, FP32 slabs out, chunked
+            for (int f = first; f < first + count; f += c->dg_ws_cells) {
+                const int cnt = std::min(c->dg_ws_cells, first + count - f);
+                DGH_DISPATCH_N(c->n, {
+                    k_dg_assemble<N, double><<<std::min(cnt, c->sms * 8), 256, 0, c->stream>>>(
+                        c->dg_ws, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step, f, cnt);
+                });
+                c->launched();
+                launch_lu_left<false>(c, c->dg_ws, stride, c->m, c->m, cnt, c->dg_perm + (size_t)f * c->m, ST_SINGULAR,
+                                      false, (float *)c->dg_pool + (size_t)f * stride);
+            }
+        } else {  // FP32 right-looking in place
+            float *pool = (float *)c->dg_pool + (size_t)first * stride;
+            DGH_DISPATCH_N(c->n, {
+                k_dg_assemble<N, float><<<grid, 256, 0, c->stream>>>(pool, c->vol, c->fcache, c->speeds, c->basis, c->g,
+                                                                     c->inv_step, first, count);
+            });
+            c->launched();
+            launch_lu<float>(c, pool, stride, c->m, c->m, count, c->dg_perm + (size_t)first * c->m, ST_SINGULAR, true);
+        }
+    } else {
+        double *pool = (double *)c->dg_pool + (size_t)first * stride;
+        DGH_DISPATCH_N(c->n, {
+            k_dg_assemble<N, double><<<grid, 256, 0, c->stream>>>(pool, c->vol, c->fcache, c->speeds, c->basis, c->g,
+                                                                  c->inv_step, first, count);
+        });
+        c->launched();
+        if (variant == 0)
+            launch_lu_left<false>(c, pool, stride, c->m, c->m, count, c->dg_perm + (size_t)first * c->m, ST_SINGULAR, true);
+        else
+            launch_lu<double>(c, pool, stride, c->m, c->m, count, c->dg_perm + (size_t)first * c->m, ST_SINGULAR, true);
+    }
+}
+// Condensation of cells [first, first + count) (count <= aug_cells): [A | B | r], LU + solve
+// with the given variant, S, X, y, C y.
+void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int count) {
+    const int ld = c->m + c->t + 1, grid = std::min(count, c->sms * 8);
+    DGH_DISPATCH_N(c->n, {
+        k_hdg_assemble<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->vol, c->fcache, c->speeds, r, c->basis, c->g,
+                                                               c->inv_step, first, count);
+    });
+    c->launched();
+    if (variant == 0) {
+        launch_lu_left<true>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
+    } else {
+        launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
+        constexpr size_t bs_smem = backsolve_smem_bytes();
+        ck(cudaFuncSetAttribute(k_backsolve_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bs_smem), "attr");
+        int per_sm = 0;
+        ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backsolve_dmma, LU_THREADS, bs_smem), "occupancy");
+        k_backsolve_dmma<<<std::min(count, c->sms * std::max(1, per_sm)), LU_THREADS, bs_smem, c->stream>>>(
+            c->aug, (size_t)c->m * ld, c->m, ld, count);
+        c->launched();
+    }
+    DGH_DISPATCH_N(c->n, {
+        k_hdg_schur<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y, c->cy, c->basis,
+                                                            c->g, first, count);
+    });
+    c->launched();
+}
+// Times f(variant) for variants 0 and 1 (best of two runs each) and returns the faster one.
+template <class F> int tune_pick(dgh_ctx *c, F &&f, double *ms_out) {
+    cudaEvent_t a = c->event(), b = c->event();
+    double best[2] = {1e300, 1e300};
+    for (int rep = 0; rep < 2; ++rep)
+        for (int v = 0; v < 2; ++v) {
+            ck(cudaEventRecord(a, c->stream), "cudaEventRecord");
+            f(v);
+            ck(cudaEventRecord(b, c->stream), "cudaEventRecord");
+            ck(cudaEventSynchronize(b), "cudaEventSynchronize");
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+            best[v] = std::min(best[v], (double)ms);
+        }
+    c->spare.push_back(a);
+    c->spare.push_back(b);
+    ms_out[0] = best[0];
+    ms_out[1] = best[1];
+    return best[1] < best[0] ? 1 : 0;
+}
+// The cached or newly tuned variant of one kind (0 DG blocks, 1 condensation).
+template <class F> int tuned_variant(dgh_ctx *c, int kind, F &&time_both, double *ms_out) {
+    if (!c->cfg.autotune) return 0;
+    const auto key = std::make_tuple(kind, c->n, c->cfg.precision);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return it->second;
+    }
+    const int v = tune_pick(c, time_both, ms_out);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = v;
+    return v;
+}
+}  // namespace
+
+extern "C" {
+
 // ---- BlockJacobi -------------------------------------------------------------------------------
 int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
     return guard(c, [&] {
@@ -1448,28 +1565,12 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
         if (op == DGH_OP_DG) {
             need(c->dg_pool, "context has no DG operator");
             need(c->linearised, "Refresh the volume Jacobian before assembling a block");
-            const size_t stride = (size_t)c->m * c->m;
-            const int grid = std::min(c->cells, c->sms * 8);
-            if (c->mixed()) {
-                // factor in FP64 chunk by chunk, store FP32 slabs
-                for (int first = 0; first < c->cells; first += c->dg_ws_cells) {
-                    const int count = std::min(c->dg_ws_cells, c->cells - first);
-                    DGH_DISPATCH_N(c->n, {
-                        k_dg_assemble<N, double><<<std::min(count, c->sms * 8), 256, 0, c->stream>>>(
-                            c->dg_ws, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step, first, count);
-                    });
-                    c->launched();
-                    launch_lu_left<false>(c, c->dg_ws, stride, c->m, c->m, count, c->dg_perm + (size_t)first * c->m,
-                                          ST_SINGULAR, false, (float *)c->dg_pool + (size_t)first * stride);
-                }
-            } else {
-                DGH_DISPATCH_N(c->n, {
-                    k_dg_assemble<N, double><<<grid, 256, 0, c->stream>>>((double *)c->dg_pool, c->vol, c->fcache, c->speeds,
-                                                                          c->basis, c->g, c->inv_step, 0, c->cells);
-                });
-                c->launched();
-                launch_lu_left<false>(c, (double *)c->dg_pool, stride, c->m, c->m, c->cells, c->dg_perm, ST_SINGULAR, true);
+            if (c->dg_variant < 0) {
+                const int sample = std::min(c->cells, std::max(c->lu_grid, 1) * 4);
+                c->dg_variant = tuned_variant(c, 0, [&](int v) { dg_factor(c, v, 0, sample); }, c->tune_ms);
+                c->check_status();
             }
+            dg_factor(c, c->dg_variant, 0, c->cells);
             c->check_status();
             c->dg_factored = true;
         } else {
@@ -1530,21 +1631,13 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
             c->condensed = true;
             return;
         }
-        for (int first = 0; first < c->cells; first += c->aug_cells) {
-            const int count = std::min(c->aug_cells, c->cells - first);
-            const int grid = std::min(count, c->sms * 8);
-            DGH_DISPATCH_N(c->n, {
-                k_hdg_assemble<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->vol, c->fcache, c->speeds, r, c->basis, c->g,
-                                                                       c->inv_step, first, count);
-            });
-            c->launched();
-            launch_lu_left<true>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
-            DGH_DISPATCH_N(c->n, {
-                k_hdg_schur<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y, c->cy, c->basis,
-                                                                    c->g, first, count);
-            });
-            c->launched();
+        if (c->hdg_variant < 0) {
+            const int sample = std::min(c->aug_cells, std::max(c->lu_grid, 1) * 4);
+            c->hdg_variant = tuned_variant(c, 1, [&](int v) { hdg_condense_chunk(c, v, r, 0, sample); }, c->tune_ms + 2);
+            c->check_status();
         }
+        for (int first = 0; first < c->cells; first += c->aug_cells)
+            hdg_condense_chunk(c, c->hdg_variant, r, first, std::min(c->aug_cells, c->cells - first));
         DGH_DISPATCH_N(c->n, {
             const long long tot = c->NT;
             k_hdg_rhs<N><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->cy, c->hrhs, c->g);
@@ -1630,6 +1723,13 @@ int dgh_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, doubl
         if (iterations) *iterations = it;
         if (relative) *relative = rel;
     });
+}
+int dgh_autotune_report(const dgh_ctx *c, double out[6]) {
+    if (!c || !out) return DGH_ERR_INVALID;
+    out[0] = c->dg_variant;
+    out[1] = c->hdg_variant;
+    for (int i = 0; i < 4; ++i) out[2 + i] = c->tune_ms[i];
+    return DGH_OK;
 }
 int dgh_gmres_graph_enable(dgh_ctx *c, int on) {
     return guard(c, [&] { c->use_graph = on != 0; });

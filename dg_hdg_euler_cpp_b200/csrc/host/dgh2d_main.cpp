@@ -74,6 +74,7 @@ Options parse(int argc, char **argv) {
         else if (option == "--max-newton") c.max_newton = integer();
         else if (option == "--device") c.device = integer();
         else if (option == "--graph") o.graph = true;
+        else if (option == "--autotune") c.autotune = 1;
         else if (option == "--precision") {
             auto p = value();
             require(p == "fp64" || p == "mixed", "Invalid precision");
@@ -95,7 +96,7 @@ Options parse(int argc, char **argv) {
                          "--ordering natural --restart N --max-linear N --max-newton N\n"
                          "--ntol R --ltol R --safety S --prefix PATH\n"
                          "--integrator ssp-dirk3|be --newton-steps N --warmup-updates N\n"
-                         "--graph --timing-only --check-update --no-save-solution --precision fp64|mixed --device N\n";
+                         "--graph --autotune --timing-only --check-update --no-save-solution --precision fp64|mixed --device N\n";
             std::exit(0);
         } else
             throw std::runtime_error("Unknown option: " + option);

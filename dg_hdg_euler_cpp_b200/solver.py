@@ -234,6 +234,13 @@ class Solver:
         self._call("dgh_hdg_recovered_residual", _ptr(e), _ptr(out))
         return out
 
+    def autotune_report(self) -> dict:
+        """Factorisation variants in use and the last tuning times (dgh_autotune_report)."""
+        out = (ctypes.c_double * 6)()
+        self._rc(self.lib.dgh_autotune_report(self.h, out))
+        return {"dg_variant": int(out[0]), "hdg_variant": int(out[1]),
+                "tune_ms": {"dg": [out[2], out[3]], "hdg": [out[4], out[5]]}}
+
     # ---- GMRES
     def gmres_graph(self, on: bool = True):
         """Replay each GMRES restart cycle as one CUDA graph (dgh_gmres_graph_enable)."""

@@ -71,6 +71,7 @@ typedef struct dgh_config {
     int check_update; /* HDG: independent DG J*v check of every update (time_integrator.cpp:153-162) */
     int device;       /* CUDA device ordinal                                               */
     int dim;          /* 2 (dg_hdg_2d, the default) or 1 (dg_hdg_1d)                       */
+    int autotune;     /* 2D: time the factorisation variants on the first refresh (per degree) */
 } dgh_config;
 
 /* config.hpp:7-18 defaults: nx=ny=8, k=3, restart 30, max_linear 1500, max_newton 30,
@@ -173,6 +174,17 @@ int dgh_hdg_recovered_residual(dgh_ctx *ctx, const double *e, double *out); /* h
 int dgh_gmres(dgh_ctx *ctx, int op, const double *rhs, double *x, int limit, double tol,
               int *iterations, double *relative);
 /* Device pointer to the true residual rhs - A x of the last dgh_gmres call on op. */
+/* Per-degree autotuner (no counterpart in the reference).  With dgh_config.autotune set, the
+ * first DG block-Jacobi refresh and the first HDG condensation of a context time their
+ * factorisation variants on a sample of the context's own cells and keep the faster one; the
+ * choice is cached per (degree, precision) for the process.  Variants: DG blocks 0 = left-looking
+ * FP64 LU on the tensor pipe (FP32 slabs in the mixed form), 1 = right-looking LU (FP32 in the
+ * mixed form); condensation 0 = left-looking LU with the fused right-hand-side solve,
+ * 1 = right-looking LU then the tensor-pipe back substitution.  All variants compute the same
+ * factors up to rounding.  out[0..1] = the DG and condensation variants in use, -1 where the
+ * context has not factored yet; out[2..5] = the last tuning times in ms (DG 0, DG 1, HDG 0,
+ * HDG 1; 0 where not timed). */
+int dgh_autotune_report(const dgh_ctx *ctx, double out[6]);
 /* Replay each GMRES restart cycle as one CUDA graph (its Arnoldi steps are conditional nodes
  * that stop at the reference's inner-loop break, gmres.cpp:65-67) instead of launching it step
  * by step with a host read of the continue flag after every step.  Both ways run the same
