@@ -51,7 +51,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-graph-check", action="store_true", help="skip the GMRES graph-vs-stepped comparison")
-    p.add_argument("--graph", action="store_true", help="replay GMRES restart cycles as CUDA graphs")
+    p.add_argument("--no-batch", action="store_true", help="skip the 16-member uneven batch")
+    p.add_argument("--stepped", action="store_true",
+                   help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
     p.add_argument("--cpu-sample-nx", type=int, default=32)
     return p.parse_args()
@@ -156,7 +158,7 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
     s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=W + K + 2,
                method=method, precision=precision, restart=20, max_linear=1500, ntol=args.ltol, ltol=args.ltol,
                safety=1.1, device=local, autotune=1 if args.autotune else 0)
-    s.gmres_graph(args.graph)
+    s.gmres_graph(not args.stepped)
     it = Integrator(s, method)
     stream = torch.cuda.ExternalStream(s.stream(), device=s.device)
     u0 = s.initial()
@@ -185,33 +187,50 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
         sampler.stop()
     ms = allmax(pg, torch, e0.elapsed_time(e1))
     launches = s.launch_count() - launches0
-    timers = {}
-    for name, cat in (("precond", 0), ("operator", 1), ("arnoldi", 2), ("factor", 3), ("face_factor", 4),
-                      ("condense", 5), ("residual", 6)):
-        tot, cnt = ctypes.c_double(), ctypes.c_int64()
-        lib.dgh_timing_read(s.h, cat, ctypes.byref(tot), ctypes.byref(cnt))
-        timers[name] = {"ms": tot.value, "launches": cnt.value}
+
+    def read_timers():
+        out = {}
+        for name, cat in (("precond", 0), ("operator", 1), ("arnoldi", 2), ("factor", 3), ("face_factor", 4),
+                          ("condense", 5), ("residual", 6)):
+            tot, cnt = ctypes.c_double(), ctypes.c_int64()
+            lib.dgh_timing_read(s.h, cat, ctypes.byref(tot), ctypes.byref(cnt))
+            out[name] = {"ms": tot.value, "launches": cnt.value}
+        return out
+
+    timers = read_timers()
     lib.dgh_timing_enable(s.h, 0)
     final = np.empty(s.size)
     lib.dgh_download(s.h, final.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(it.state_ptr()), s.size)
+    # Inside the replayed cycle graphs the per-call timers see no launches: the per-kernel figures
+    # (the roofline's average launch time) come from one more update, from the same stage start,
+    # with the cycles launched step by step (the same kernels with the same arguments).
+    kernel_timers = timers
+    if not args.stepped:
+        s.gmres_graph(False)
+        it.stage_begin(u0)
+        lib.dgh_timing_enable(s.h, 1)
+        it.update()
+        kernel_timers = read_timers()
+        lib.dgh_timing_enable(s.h, 0)
+        s.gmres_graph(True)
     out = {
         "method": method, "precision": precision, "updates": K, "ms": ms, "updates_per_s": 1000.0 * K / ms,
         "ms_per_update": ms / K, "krylov": [r["krylov_iterations"] for r in rows],
         "krylov_update1": first["krylov_iterations"],
         "rms": [r["residual_physical_rms"] for r in rows], "damping": [r["damping"] for r in rows],
         "launches": launches, "timers": timers, "device_gb": s.device_bytes() / 1e9,
-        "clocks": sampler.summary() if sampler else None, "graph": bool(args.graph),
+        "clocks": sampler.summary() if sampler else None, "gmres_cycles": "stepped" if args.stepped else "cuda_graph",
         "autotune": s.autotune_report(),
     }
     # dominant per-iteration kernel of this configuration
     if method == "dg":
         kb = algorithmic_bytes("dg", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
-        tk = timers["precond"]
+        tk = kernel_timers["precond"]
         kernel = "k_lu_solve<%s> (block-Jacobi solve, one launch per Krylov iteration)" % (
             "float" if precision == "mixed" else "double")
     else:
         kb = algorithmic_bytes("hdg_schur", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
-        tk = timers["operator"]
+        tk = kernel_timers["operator"]
         kernel = "k_hdg_apply (face-owned Schur apply, one launch per Krylov iteration)"
     if tk["launches"]:
         avg_ms = tk["ms"] / tk["launches"]
@@ -219,8 +238,12 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
         out["roofline"] = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "bytes_per_launch": kb,
                            "avg_launch_ms": avg_ms, "launches": tk["launches"]}
-    else:  # graph replay: the per-call timers do not see launches inside the cycle graphs
+        if not args.stepped:
+            out["roofline"]["measured_on"] = "update 1 from the stage start, cycles launched step by step"
+    else:
         out["roofline"] = None
+    if not args.stepped:
+        out["kernel_timers_stepped_update"] = kernel_timers
     # e2e through the C ABI with host buffers
     if not args.no_e2e:
         it.stage_begin(u0)
@@ -279,6 +302,63 @@ def graph_comparison(torch, local: int):
                                        "krylov": [r["krylov_iterations"] for r in res[True][1]],
                                        "bitwise_equal_history": same}
     return out
+
+
+def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: bool = True):
+    """The uneven batch (members from seeds 0..members-1: k in {2,4,6,8}, N^2 meshes with N in
+    {32,64,96,128}, DG or HDG, amplitude-scaled initial states, BE CFL 5, GMRES(30), mixed
+    precision): `updates` Newton updates of every member run one member at a time, then all
+    members together through dgh_batch; member-updates per second for both and whether every
+    member's rows agree bitwise between the two."""
+    from dg_hdg_euler_cpp_b200.solver import Batch, batch_member, perturb
+
+    draws = [batch_member(s) for s in range(members)]
+    cfgs = [dict(d["config"], device=local) for d in draws]
+
+    def states(b, idx):
+        return [perturb(b.initial(j), cfgs[i]["nx"], cfgs[i]["ny"], cfgs[i]["k"], draws[i]["amplitude"])
+                for j, i in enumerate(idx)]
+
+    def timed(b, u0):
+        b.gmres_graph(graph)
+        b.stage_begin(u0)
+        b.update()  # warm-up update, then restart the stage
+        b.stage_begin(u0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rows = [b.update() for _ in range(updates)]
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, rows
+
+    seq_s, seq_rows = 0.0, []
+    for i in range(members):
+        b = Batch([cfgs[i]])
+        t, rows = timed(b, states(b, [i]))
+        seq_s += t
+        seq_rows.append([r[0] for r in rows])
+        b.close()
+        torch.cuda.empty_cache()
+    b = Batch(cfgs)
+    dev_gb = 0.0
+    for i in range(members):
+        by = ctypes.c_int64()
+        b.lib.dgh_device_bytes(b.member_ctx(i), ctypes.byref(by))
+        dev_gb += by.value / 1e9
+    bat_s, bat_rows = timed(b, states(b, list(range(members))))
+    b.close()
+    torch.cuda.empty_cache()
+    same = all(bat_rows[u][i][k] == seq_rows[i][u][k] for i in range(members) for u in range(updates)
+               for k in ("krylov_iterations", "residual_physical_rms", "damping"))
+    work = members * updates
+    return {"members": [{"seed": d["seed"], "k": d["config"]["k"], "n": d["config"]["nx"], "method": d["config"]["method"],
+                         "amplitude": d["amplitude"], "krylov": [seq_rows[i][u]["krylov_iterations"]
+                                                                  for u in range(updates)]}
+                        for i, d in enumerate(draws)],
+            "updates_per_member": updates, "device_gb": dev_gb,
+            "one_at_a_time_s": seq_s, "batched_s": bat_s,
+            "one_at_a_time_member_updates_per_s": work / seq_s, "batched_member_updates_per_s": work / bat_s,
+            "speedup": seq_s / bat_s, "bitwise_equal_rows": same,
+            "gmres_cycles": "cuda_graph" if graph else "stepped"}
 
 
 def cpu_baseline(args, threads: int, steps: int, warm: int):
@@ -369,6 +449,8 @@ def main():
         line["e2e"] = {"value": world * tot_upd / e2e_s, "unit": "updates/s",
                        "h2d_bytes_per_step": results[head[0]]["e2e"]["h2d_bytes_per_step"],
                        "d2h_bytes_per_step": results[head[0]]["e2e"]["d2h_bytes_per_step"]}
+    if rank == 0 and world == 1 and not args.no_batch:
+        line["breakdown"]["uneven_batch_16"] = uneven_batch(torch, local, graph=not args.stepped)
     if rank == 0 and world == 1 and not args.no_graph_check:
         line["breakdown"]["gmres_graph_vs_stepped"] = graph_comparison(torch, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -123,6 +123,13 @@ SIGNATURES = {
     "dgh_integrator_state": (_VP, [_VP]),
     "dgh_dirk3_adjoint": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.POINTER(dgh_adjoint_stats)]),
     "dgh_dirk3_replay": (ctypes.c_int, [_VP, _VP, _D]),
+    "dgh_batch_create": (ctypes.c_int, [ctypes.POINTER(dgh_config), ctypes.c_int, ctypes.POINTER(_VP)]),
+    "dgh_batch_destroy": (ctypes.c_int, [_VP]),
+    "dgh_batch_error": (ctypes.c_char_p, [_VP, ctypes.c_int]),
+    "dgh_batch_member": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+    "dgh_batch_stage_begin": (ctypes.c_int, [_VP, _VP, _D, _I]),
+    "dgh_batch_newton_update": (ctypes.c_int, [_VP, ctypes.POINTER(dgh_update_stats), _I]),
+    "dgh_batch_download": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "dgh_residual_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             _VP, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),
 }

@@ -287,13 +287,27 @@ void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
     c->launched();
 }
 
+// The dynamic shared-memory cap of a kernel is process-wide state that every context shares (and
+// the contexts of a batch run on several host threads): it only ever rises, under a lock, so no
+// launch sees a cap below the size it was launched with.
+void allow_dynamic_smem(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> cap;
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = cap[{fn, dev}];
+    if (bytes <= cur) return;
+    ck(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "shared memory attribute");
+    cur = bytes;
+}
+
 // Panel width 32; U12 tile width 32 for FP64 (two CTAs per SM fit in shared memory at m = 324)
 // and 64 for FP32.
 constexpr int LU_NB = 32;
 template <typename TF> constexpr int lu_tc() { return sizeof(TF) == 8 ? 32 : 64; }
 template <typename TF> void setup_lu_attrs(size_t smem) {
-    ck(cudaFuncSetAttribute(k_lu<TF, LU_NB, lu_tc<TF>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-       "lu attr");
+    allow_dynamic_smem((const void *)k_lu<TF, LU_NB, lu_tc<TF>()>, smem);
 }
 template <typename TF>
 void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out) {
@@ -313,24 +327,32 @@ void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int 
                     float *out32 = nullptr) {
     need(m <= 2 * LL_THREADS && m % 4 == 0, "LU block width unsupported by the left-looking kernel");
     const size_t smem = lu_left_smem_bytes(m);
-    ck(cudaFuncSetAttribute(k_lu_left<AUG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "lu_left attr");
+    allow_dynamic_smem((const void *)k_lu_left<AUG>, smem);
     const int grid = std::min(count, c->lu_grid);
     k_lu_left<AUG><<<grid, LL_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, c->lu_tri, perm, c->status, bit,
                                                           slab_out ? 1 : 0, out32);
     c->launched();
 }
 // One warp per block; enough warps for every SM to keep its warp slots (and their loads) busy.
-template <typename TF>
-void launch_solve(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
-                  double *z) {
+// FP32 blocks narrower than two slabs (the HDG face blocks) use the register-held diagonal rows.
+template <typename TF, bool DIAG>
+void launch_solve_as(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
+                     double *z) {
     constexpr int wpc = SOLVE_THREADS / 32;
     const size_t smem = sizeof(TF) * (size_t)m * wpc;
     const int want = (count + wpc - 1) / wpc;
     int resident = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve<TF>, SOLVE_THREADS, smem), "occupancy");
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve<TF, DIAG>, SOLVE_THREADS, smem), "occupancy");
     const int grid = std::min(want, c->sms * std::max(1, resident));
-    k_lu_solve<TF><<<grid, SOLVE_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
+    k_lu_solve<TF, DIAG><<<grid, SOLVE_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
     c->launched();
+}
+template <typename TF>
+void launch_solve(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
+                  double *z) {
+    if constexpr (sizeof(TF) == 4)
+        if (m < 64) return launch_solve_as<TF, true>(c, pool, perm, stride, m, count, x, z);
+    launch_solve_as<TF, false>(c, pool, perm, stride, m, count, x, z);
 }
 
 template <typename TF>
@@ -1016,7 +1038,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         }
         if (c->has_dg() || c->has_hdg()) {
             const size_t smem = lu_left_smem_bytes(c->m);
-            ck(cudaFuncSetAttribute(k_lu_left<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+            allow_dynamic_smem((const void *)k_lu_left<true>, smem);
             int per_sm = 0;
             ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_left<true>, LL_THREADS, smem), "occupancy");
             c->lu_grid = c->sms * std::max(1, per_sm);
@@ -1475,7 +1497,7 @@ void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int
     } else {
         launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
         constexpr size_t bs_smem = backsolve_smem_bytes();
-        ck(cudaFuncSetAttribute(k_backsolve_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bs_smem), "attr");
+        allow_dynamic_smem((const void *)k_backsolve_dmma, bs_smem);
         int per_sm = 0;
         ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backsolve_dmma, LU_THREADS, bs_smem), "occupancy");
         k_backsolve_dmma<<<std::min(count, c->sms * std::max(1, per_sm)), LU_THREADS, bs_smem, c->stream>>>(

@@ -369,17 +369,22 @@ k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restr
 // Block solve z = A^{-1} b with the factors of k_lu (block_jacobi.hpp:24-39): permute, unit
 // lower solve, upper solve.  One warp owns one block and streams its factors exactly once with
 // no CTA-wide barriers; lane i owns row 32 s + i of slab s and reads 16-byte column groups of
-// the slab layout above.  Off-diagonal parts are per-lane dot products; the diagonal triangles
-// of the 32-row slabs are solved with warp shuffles.  T is the factor and arithmetic precision
-// (FP32 factors accumulate in FP32); b and z are FP64.
+// the slab layout above.  Off-diagonal parts are per-lane dot products (four 16-byte loads in
+// flight per lane, four accumulators); the diagonal triangles of the 32-row slabs are solved with
+// warp shuffles.  T is the factor and arithmetic precision (FP32 factors accumulate in FP32);
+// b and z are FP64.  The forward and backward sweeps share one loop body, which keeps the
+// kernel at <= 48 registers (FP32; five 256-thread CTAs per SM) or 64 (FP64).  DIAG loads a full
+// slab's diagonal row into registers before its triangle (all its loads in flight at once): the
+// FP32 form for narrow blocks (the HDG face blocks, m = 4n), whose time is mostly triangles.
 constexpr int SOLVE_THREADS = 256;
-template <typename T>
-__global__ void __launch_bounds__(SOLVE_THREADS)
+template <typename T, bool DIAG> constexpr int solve_min_blocks() { return sizeof(T) == 4 && !DIAG ? 5 : 4; }
+template <typename T, bool DIAG>
+__global__ void __launch_bounds__(SOLVE_THREADS, (solve_min_blocks<T, DIAG>()))
 k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stride, int m, int count,
            const double *__restrict__ rhs, double *__restrict__ z) {
     using SV = SlabVec<T>;
     using V = typename SV::V;
-    constexpr int W = SV::W;
+    constexpr int W = SV::W, ND = 32 / W;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     T *y = reinterpret_cast<T *>(smraw) + (size_t)wib * m;
@@ -393,64 +398,77 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
         const double *b = rhs + (size_t)blk * m;
         for (int i = lane; i < m; i += 32) y[i] = (T)b[pm[i]];
         __syncwarp();
-        // forward: L y = P b
-        for (int s = 0; s < slabs; ++s) {
-            const int r0 = 32 * s, nt = min(32, m - r0);
-            const T *S = A + (size_t)r0 * m;
-            const V *Sv = reinterpret_cast<const V *>(S);
-            const bool act = lane < nt;
-            T acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
-            if (act) {
-                const int groups = r0 / W;
-                int g = 0;
-                for (; g + 4 <= groups; g += 4) {  // four independent 16-byte loads in flight per lane
-                    const V a0 = Sv[(size_t)g * nt + lane], a1 = Sv[(size_t)(g + 1) * nt + lane];
-                    const V a2 = Sv[(size_t)(g + 2) * nt + lane], a3 = Sv[(size_t)(g + 3) * nt + lane];
-                    acc0 += SV::dotv(a0, yv[g]);
-                    acc1 += SV::dotv(a1, yv[g + 1]);
-                    acc2 += SV::dotv(a2, yv[g + 2]);
-                    acc3 += SV::dotv(a3, yv[g + 3]);
+        // dir 0: forward, L y = P b (slabs in order, columns left of the slab); dir 1: backward,
+        // U z = y (slabs in reverse, columns right of the slab)
+        for (int dir = 0; dir < 2; ++dir) {
+            for (int si = 0; si < slabs; ++si) {
+                const int s = dir == 0 ? si : slabs - 1 - si;
+                const int r0 = 32 * s, nt = min(32, m - r0), hi = r0 + nt;
+                const T *S = A + (size_t)r0 * m;
+                const V *Sv = reinterpret_cast<const V *>(S);
+                const bool act = lane < nt;
+                T acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+                if (act) {
+                    const int g1 = dir == 0 ? r0 / W : m / W;
+                    int g = dir == 0 ? 0 : hi / W;
+                    for (; g + 4 <= g1; g += 4) {  // four independent 16-byte loads in flight per lane
+                        const V a0 = Sv[(size_t)g * nt + lane], a1 = Sv[(size_t)(g + 1) * nt + lane];
+                        const V a2 = Sv[(size_t)(g + 2) * nt + lane], a3 = Sv[(size_t)(g + 3) * nt + lane];
+                        acc0 += SV::dotv(a0, yv[g]);
+                        acc1 += SV::dotv(a1, yv[g + 1]);
+                        acc2 += SV::dotv(a2, yv[g + 2]);
+                        acc3 += SV::dotv(a3, yv[g + 3]);
+                    }
+                    for (; g < g1; ++g) acc0 += SV::dotv(Sv[(size_t)g * nt + lane], yv[g]);
                 }
-                for (; g < groups; ++g) acc0 += SV::dotv(Sv[(size_t)g * nt + lane], yv[g]);
-            }
-            T t = act ? y[r0 + lane] - ((acc0 + acc1) + (acc2 + acc3)) : T(0);
-            for (int jj = 0; jj < nt; ++jj) {
-                const T l = (act && lane > jj) ? S[slab_at<T>(nt, lane, r0 + jj)] : T(0);
-                const T yj = __shfl_sync(0xffffffffu, t, jj);
-                t -= l * yj;
-            }
-            if (act) y[r0 + lane] = t;
-            __syncwarp();
-        }
-        // backward: U z = y
-        for (int s = slabs - 1; s >= 0; --s) {
-            const int r0 = 32 * s, nt = min(32, m - r0), hi = r0 + nt;
-            const T *S = A + (size_t)r0 * m;
-            const V *Sv = reinterpret_cast<const V *>(S);
-            const bool act = lane < nt;
-            T acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
-            if (act) {
-                const int g1 = m / W;
-                int g = hi / W;
-                for (; g + 4 <= g1; g += 4) {
-                    const V a0 = Sv[(size_t)g * nt + lane], a1 = Sv[(size_t)(g + 1) * nt + lane];
-                    const V a2 = Sv[(size_t)(g + 2) * nt + lane], a3 = Sv[(size_t)(g + 3) * nt + lane];
-                    acc0 += SV::dotv(a0, yv[g]);
-                    acc1 += SV::dotv(a1, yv[g + 1]);
-                    acc2 += SV::dotv(a2, yv[g + 2]);
-                    acc3 += SV::dotv(a3, yv[g + 3]);
+                T t = act ? y[r0 + lane] - ((acc0 + acc1) + (acc2 + acc3)) : T(0);
+                if (DIAG && nt == 32) {
+                    V d[ND];
+#pragma unroll
+                    for (int q = 0; q < ND; ++q) d[q] = Sv[(size_t)(r0 / W + q) * 32 + lane];
+                    if (dir == 0) {
+#pragma unroll
+                        for (int q = 0; q < ND; ++q) {
+                            const T *e = reinterpret_cast<const T *>(&d[q]);
+#pragma unroll
+                            for (int w = 0; w < W; ++w) {
+                                const int jj = W * q + w;
+                                const T l = lane > jj ? e[w] : T(0);
+                                const T yj = __shfl_sync(0xffffffffu, t, jj);
+                                t -= l * yj;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = ND - 1; q >= 0; --q) {
+                            const T *e = reinterpret_cast<const T *>(&d[q]);
+#pragma unroll
+                            for (int w = W - 1; w >= 0; --w) {
+                                const int jj = W * q + w;
+                                const T u = e[w];
+                                if (lane == jj) t = t / u;
+                                const T yj = __shfl_sync(0xffffffffu, t, jj);
+                                if (lane < jj) t -= u * yj;
+                            }
+                        }
+                    }
+                } else if (dir == 0) {
+                    for (int jj = 0; jj < nt; ++jj) {
+                        const T l = (act && lane > jj) ? S[slab_at<T>(nt, lane, r0 + jj)] : T(0);
+                        const T yj = __shfl_sync(0xffffffffu, t, jj);
+                        t -= l * yj;
+                    }
+                } else {
+                    for (int jj = nt - 1; jj >= 0; --jj) {
+                        const T u = act ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
+                        if (lane == jj) t = t / u;
+                        const T yj = __shfl_sync(0xffffffffu, t, jj);
+                        if (lane < jj) t -= u * yj;
+                    }
                 }
-                for (; g < g1; ++g) acc0 += SV::dotv(Sv[(size_t)g * nt + lane], yv[g]);
+                if (act) y[r0 + lane] = t;
+                __syncwarp();
             }
-            T t = act ? y[r0 + lane] - ((acc0 + acc1) + (acc2 + acc3)) : T(0);
-            for (int jj = nt - 1; jj >= 0; --jj) {
-                const T u = act ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
-                if (lane == jj) t = t / u;
-                const T yj = __shfl_sync(0xffffffffu, t, jj);
-                if (lane < jj) t -= u * yj;
-            }
-            if (act) y[r0 + lane] = t;
-            __syncwarp();
         }
         for (int i = lane; i < m; i += 32) z[(size_t)blk * m + i] = (double)y[i];
         __syncwarp();

@@ -315,3 +315,145 @@ class Integrator:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Independent uneven member problems advanced together (dgh_batch_*): each member has its
+    own config (mesh, degree, method "dg" or "hdg", precision ...), context, integrator and host
+    thread, so the members' kernels overlap on the device; each member computes exactly what
+    its single-problem run computes."""
+
+    def __init__(self, members: list[dict]):
+        self.lib = _lib.load()
+        self.count = len(members)
+        self.cfgs = (_lib.dgh_config * self.count)(*[make_config(**m) for m in members])
+        h = ctypes.c_void_p()
+        rc = self.lib.dgh_batch_create(self.cfgs, self.count, ctypes.byref(h))
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_batch_error(None, 0).decode())
+        self.h = h
+        self.sizes = []
+        for i in range(self.count):
+            ctx = ctypes.c_void_p()
+            self.lib.dgh_batch_member(self.h, i, ctypes.byref(ctx), None)
+            s = (ctypes.c_int64 * 8)()
+            self.lib.dgh_sizes(ctx, s)
+            self.sizes.append(int(s[0]))
+
+    def gmres_graph(self, on: bool = True):
+        """Replay every member's GMRES restart cycles as CUDA graphs (dgh_gmres_graph_enable)."""
+        for i in range(self.count):
+            rc = self.lib.dgh_gmres_graph_enable(self.member_ctx(i), 1 if on else 0)
+            if rc != 0:
+                raise DGHError(rc, self.lib.dgh_last_error(self.member_ctx(i)).decode())
+
+    def _check(self, rc, status):
+        if rc != 0:
+            bad = [i for i in range(self.count) if status[i] != 0]
+            msg = "; ".join(f"member {i}: {self.lib.dgh_batch_error(self.h, i).decode()}" for i in bad)
+            raise DGHError(rc, msg)
+
+    def member_ctx(self, i: int) -> ctypes.c_void_p:
+        ctx = ctypes.c_void_p()
+        self.lib.dgh_batch_member(self.h, i, ctypes.byref(ctx), None)
+        return ctx
+
+    def initial(self, i: int) -> np.ndarray:
+        """Member i's projected initial state (dgh_initial), on the host."""
+        ctx = self.member_ctx(i)
+        out = np.empty(self.sizes[i])
+        dev = ctypes.POINTER(ctypes.c_double)()
+        self.lib.dgh_vec_alloc(ctx, self.sizes[i], ctypes.byref(dev))
+        try:
+            rc = self.lib.dgh_initial(ctx, dev)
+            if rc == 0:
+                rc = self.lib.dgh_download(ctx, out.ctypes.data_as(ctypes.c_void_p), dev, self.sizes[i])
+            if rc != 0:
+                raise DGHError(rc, self.lib.dgh_last_error(ctx).decode())
+        finally:
+            self.lib.dgh_vec_free(ctx, dev)
+        return out
+
+    def stage_begin(self, states=None) -> list[float]:
+        """Every member starts a backward-Euler stage from states[i] (host arrays; None = its
+        initial state); returns the members' step sizes."""
+        keep = [None if states is None or states[i] is None else np.ascontiguousarray(states[i], dtype=np.float64)
+                for i in range(self.count)]
+        ptrs = (ctypes.c_void_p * self.count)(*[None if a is None else a.ctypes.data for a in keep])
+        dt = (ctypes.c_double * self.count)()
+        status = (ctypes.c_int * self.count)()
+        rc = self.lib.dgh_batch_stage_begin(self.h, ptrs, dt, status)
+        self._check(rc, status)
+        return list(dt)
+
+    def update(self) -> list[dict]:
+        """One Newton update of every member; the members' rows."""
+        st = (_lib.dgh_update_stats * self.count)()
+        status = (ctypes.c_int * self.count)()
+        rc = self.lib.dgh_batch_newton_update(self.h, st, status)
+        self._check(rc, status)
+        return [{f: getattr(s, f) for f, _ in _lib.dgh_update_stats._fields_} for s in st]
+
+    def state(self, i: int) -> np.ndarray:
+        out = np.empty(self.sizes[i])
+        rc = self.lib.dgh_batch_download(self.h, i, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_batch_error(self.h, i).decode())
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dgh_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- the uneven-batch workload: 16 members drawn from seeds 0-15 --------------------------------
+_MASK64 = (1 << 64) - 1
+
+
+def splitmix64(state: int) -> tuple[int, int]:
+    """One step of Vigna's SplitMix64 generator: (output, next state)."""
+    state = (state + 0x9E3779B97F4A7C15) & _MASK64
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _MASK64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _MASK64
+    return z ^ (z >> 31), state
+
+
+def batch_member(seed: int, sizes=(32, 64, 96, 128), degrees=(2, 4, 6, 8), precision="mixed") -> dict:
+    """Member `seed` of the uneven batch: degree k, an N x N mesh, amplitude A in [0.05, 0.25)
+    and the method, drawn from SplitMix64 seeded by the seed index; backward Euler at CFL 5 with
+    GMRES(30)."""
+    st = seed
+    r = []
+    for _ in range(4):
+        v, st = splitmix64(st)
+        r.append(v)
+    k = degrees[r[0] % len(degrees)]
+    n = sizes[r[1] % len(sizes)]
+    amp = 0.05 + 0.2 * ((r[2] >> 11) / float(1 << 53))
+    method = ("dg", "hdg")[r[3] % 2]
+    return {"config": dict(nx=n, ny=n, k=k, cfl=5.0, integrator="be", steps=1, restart=30, max_linear=1500,
+                           method=method, precision=precision),
+            "amplitude": amp, "seed": seed}
+
+
+def perturb(u: np.ndarray, nx: int, ny: int, k: int, amplitude: float) -> np.ndarray:
+    """The member's initial state with every conserved variable scaled by
+    1 + A sin(2 pi X) sin(2 pi Y), X and Y the mesh-relative node coordinates (periodic, and
+    positive density and pressure for A < 1)."""
+    n = k + 1
+    xi, _ = np.polynomial.legendre.leggauss(n)
+    s = (xi + 1) / 2
+    X = (np.arange(nx)[:, None] + s[None, :]) / nx   # [cx][i]
+    Y = (np.arange(ny)[:, None] + s[None, :]) / ny   # [cy][j]
+    f = 1 + amplitude * np.sin(2 * np.pi * Y)[:, None, :, None] * np.sin(2 * np.pi * X)[None, :, None, :]
+    # f[cy][cx][j][i] -> per cell (cell = cy * nx + cx), per node (j, i), same for all 4 variables
+    f = f.reshape(ny * nx, 1, n, n)
+    return (u.reshape(ny * nx, 4, n, n) * f).reshape(-1)

@@ -225,6 +225,27 @@ int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_st
 /* Device pointer to the integrator's current Newton state (size dgh_sizes()[0]). */
 double *dgh_integrator_state(dgh_integrator *it);
 
+/* ---- Batched uneven problems (no counterpart in the reference) ---------------------------------
+ * Independent member problems, each with its own dgh_config (mesh, degree, method DG or HDG,
+ * precision, restart ...), advanced together on one device.  Every member owns a context and an
+ * integrator and is driven by its own host thread, so the members' kernels overlap on the device
+ * (each context has its own stream); every member computes exactly what its single-problem run
+ * computes.  Calls on a batch are not thread-safe; per-member statuses go to status[] (may be
+ * NULL) and the return value is the first failing member's status.
+ *   dgh_batch_stage_begin: member i starts a backward-Euler stage from host_states[i] (its
+ *     dgh_initial state when host_states or host_states[i] is NULL); dt[i] receives its step.
+ *   dgh_batch_newton_update: one Newton update of every member; stats[i] its row. */
+typedef struct dgh_batch dgh_batch;
+int dgh_batch_create(const dgh_config *members, int count, dgh_batch **out);
+int dgh_batch_destroy(dgh_batch *batch);
+/* Message of member i's last failure; with batch == NULL the last dgh_batch_create failure. */
+const char *dgh_batch_error(const dgh_batch *batch, int member);
+int dgh_batch_member(dgh_batch *batch, int member, dgh_ctx **ctx, dgh_integrator **it);
+int dgh_batch_stage_begin(dgh_batch *batch, const double *const *host_states, double *dt, int *status);
+int dgh_batch_newton_update(dgh_batch *batch, dgh_update_stats *stats, int *status);
+/* Member i's current Newton state, copied to the host (size dgh_sizes()[0] of its context). */
+int dgh_batch_download(dgh_batch *batch, int member, double *host_state);
+
 /* ---- Discrete adjoint of the DG time integration (no counterpart in the reference) -------------
  * Objective J = sum over nodes of M rho^2 at the end of `steps` fixed steps (dt = cfl / rate of
  * each step's start state) of the context's integrator (SSP-DIRK3 or BE), DG method.  The

@@ -117,3 +117,46 @@ def test_kernels_are_built_for_sm100a():
     log = (ROOT / "dg_hdg_euler_cpp_b200" / "lib" / "ptxas.log").read_text()
     assert "sm_100a" in log
     assert "k_lu" in log and "k_dg_apply" in log and "k_hdg_apply" in log
+
+
+def test_batch_rejects_members_without_a_single_method(lib):
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    cfgs = (_lib.dgh_config * 2)()
+    for c in cfgs:
+        lib.dgh_config_default(ctypes.byref(c))
+        c.method = 0
+    cfgs[1].method = 2  # both: a batch member runs one method
+    h = ctypes.c_void_p()
+    assert lib.dgh_batch_create(cfgs, 2, ctypes.byref(h)) == 1
+    assert not h.value
+    assert "batch member" in lib.dgh_batch_error(None, 0).decode()
+    assert lib.dgh_batch_create(cfgs, 0, ctypes.byref(h)) == 1
+
+
+def test_uneven_batch_workload_draws():
+    """The 16-member uneven batch (seeds 0-15, SplitMix64): degree, mesh, method and amplitude."""
+    from dg_hdg_euler_cpp_b200.solver import batch_member
+
+    draws = [batch_member(s) for s in range(16)]
+    got = [(d["config"]["k"], d["config"]["nx"], d["config"]["method"]) for d in draws]
+    assert got == [(8, 32, "dg"), (4, 128, "hdg"), (6, 96, "dg"), (4, 64, "hdg"), (6, 32, "dg"), (6, 32, "hdg"),
+                   (2, 64, "dg"), (8, 32, "hdg"), (6, 64, "dg"), (2, 96, "dg"), (6, 96, "dg"), (4, 64, "dg"),
+                   (8, 128, "hdg"), (8, 64, "hdg"), (6, 96, "dg"), (4, 32, "hdg")]
+    assert all(0.05 <= d["amplitude"] < 0.25 for d in draws)
+    assert abs(draws[0]["amplitude"] - 0.0553) < 1e-4
+    # SplitMix64 known answer for state 0 (Vigna's reference generator)
+    from dg_hdg_euler_cpp_b200.solver import splitmix64
+
+    assert splitmix64(0)[0] == 0xE220A8397B1DCDAF
+
+
+def test_perturbation_keeps_states_positive():
+    import numpy as np
+
+    from dg_hdg_euler_cpp_b200.solver import perturb
+
+    u = np.ones(3 * 2 * 4 * 9)
+    p = perturb(u, 3, 2, 2, 0.25)
+    assert p.min() >= 0.75 - 1e-12 and p.max() <= 1.25 + 1e-12
+    assert not np.allclose(p, 1)
