@@ -460,7 +460,10 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
                     }
                 } else {
                     for (int jj = nt - 1; jj >= 0; --jj) {
-                        const T u = act ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
+                        // row `lane` uses U(lane, jj) only on and right of its diagonal: the
+                        // lower half of the diagonal block was read by the forward sweep and is
+                        // not fetched again
+                        const T u = (act && lane <= jj) ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
                         if (lane == jj) t = t / u;
                         const T yj = __shfl_sync(0xffffffffu, t, jj);
                         if (lane < jj) t -= u * yj;
