@@ -5,6 +5,7 @@
 // in their discretisation kernels (dgh_kernels_dg/hdg.cuh versus dgh_kernels_1d.cuh).
 #include "dgh_gpu.h"
 #include "dgh_kernels_1d.cuh"
+#include "dgh_kernels_ilu1d.cuh"
 #include "dgh_kernels_dg.cuh"
 #include "dgh_kernels_hdg.cuh"
 #include "dgh_kernels_init.cuh"
@@ -88,6 +89,7 @@ struct dgh_ctx {
     long long N = 0, NT = 0;
     Grid g{};
     Basis1D basis{};
+    Basis1D *basis_dev = nullptr;  // device copy, for tables indexed per thread
     Case cs{};
     double step_size = 0, inv_step = 0;
     int sms = 148, red_grid = 592;
@@ -115,6 +117,15 @@ struct dgh_ctx {
     int aug_cells = 0;
     void *face_pool = nullptr;
     int *face_perm = nullptr;
+    // 1D block ILU(0): the periodic block pattern, its symbolic update schedule, the pattern
+    // blocks (row-major, slot order) and the diagonal blocks' permutations, per operator
+    struct IluPlan {
+        int rows = 0, m = 0, nnz = 0;
+        int *row_ptr = nullptr, *col = nullptr, *diag = nullptr, *slot_row = nullptr;
+        int *upd_off = nullptr, *upd_target = nullptr, *upd_upper = nullptr, *perm = nullptr;
+        void *vals = nullptr;
+    } ilu_dg, ilu_hdg;
+    bool ilu() const { return cfg.preconditioner == 1; }
     // left-looking FP64 LU: per-CTA scratch of the panels' L_qq^{-1}, U_qq^{-1}; FP64 workspace
     // for the mixed-precision DG blocks (factored in FP64 in chunks, stored as FP32 slabs)
     double *lu_tri = nullptr, *dg_ws = nullptr;
@@ -333,6 +344,19 @@ void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int 
                                                           slab_out ? 1 : 0, out32);
     c->launched();
 }
+// Narrow blocks (m <= 64): one warp per block in shared memory.
+template <typename TF>
+void launch_lu_narrow(dgh_ctx *c, TF *pool, int m, int count, int *perm, int bit) {
+    need(m <= 64 && m % 4 == 0, "block width unsupported by the narrow LU");
+    const size_t smem = lu_narrow_smem_bytes<TF>(m);
+    allow_dynamic_smem((const void *)k_lu_narrow<TF>, smem);
+    int resident = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_narrow<TF>, NARROW_THREADS, smem), "occupancy");
+    constexpr int wpc = NARROW_THREADS / 32;
+    const int grid = std::min((count + wpc - 1) / wpc, c->sms * std::max(1, resident));
+    k_lu_narrow<TF><<<grid, NARROW_THREADS, smem, c->stream>>>(pool, m, count, perm, c->status, bit);
+    c->launched();
+}
 // One warp per block; enough warps for every SM to keep its warp slots (and their loads) busy.
 // FP32 blocks narrower than two slabs (the HDG face blocks) use the register-held diagonal rows.
 template <typename TF, bool DIAG>
@@ -389,6 +413,18 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     if (c->d1()) {
         const bool dg = op != DGH_OP_HDG;
         need(dg ? c->dg_factored : c->face_factored, "Refresh the block-Jacobi preconditioner before applying it");
+        if (c->ilu()) {
+            need(op != DGH_OP_DG_T, "The transposed block ILU(0) is not built");
+            const auto &pl = dg ? c->ilu_dg : c->ilu_hdg;
+            if (c->mixed())
+                k1_ilu_apply<float><<<1, ILU_THREADS, 0, c->stream>>>((const float *)pl.vals, pl.perm, pl.row_ptr, pl.col,
+                                                                    pl.diag, pl.rows, pl.m, x, z);
+            else
+                k1_ilu_apply<double><<<1, ILU_THREADS, 0, c->stream>>>((const double *)pl.vals, pl.perm, pl.row_ptr,
+                                                                     pl.col, pl.diag, pl.rows, pl.m, x, z);
+            c->launched();
+            return;
+        }
         const void *pool = dg ? c->dg_pool : c->face_pool;
         const int *perm = dg ? c->dg_perm : c->face_perm, m = dg ? c->m : c->fw;
         if (c->mixed()) launch_small_solve<float>(c, (const float *)pool, perm, m, c->cells, x, z, op == DGH_OP_DG_T);
@@ -429,7 +465,7 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
     DGH_DISPATCH_N(c->n, {
         using T = Team<N>;
         k_dg_apply<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(v, c->traces2, c->vol, c->fcache, c->speeds,
-                                                                            out, c->basis, c->g, c->inv_step);
+                                                                            out, c->basis_dev, c->g, c->inv_step);
     });
     c->launched();
 }
@@ -739,6 +775,63 @@ __global__ void k_fill_trace_mass(double *inv_tm, Basis1D b, Grid g, int n, long
     inv_tm[i] = 1 / face_weight(g, b, face, q);
 }
 
+// block_ilu.cpp:15-45 on BlockGraph::periodic(rows) (block_graph.cpp:7-19,30-35): each row's
+// columns {row-1, row, row+1} sorted and unique, the diagonal slots and, for every block left of
+// the diagonal, the (target, upper) pairs its elimination updates; uploaded once.
+void build_ilu_plan(dgh_ctx *c, dgh_ctx::IluPlan &pl, int rows, int m) {
+    std::vector<int> row_ptr(rows + 1, 0), col, diag(rows), slot_row;
+    for (int r = 0; r < rows; ++r) {
+        std::vector<int> cols = {(r + rows - 1) % rows, r, (r + 1) % rows};
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        for (int cc : cols) {
+            col.push_back(cc);
+            slot_row.push_back(r);
+        }
+        row_ptr[r + 1] = (int)col.size();
+    }
+    auto find = [&](int r, int cc) {
+        for (int p = row_ptr[r]; p < row_ptr[r + 1]; ++p)
+            if (col[p] == cc) return p;
+        return -1;
+    };
+    std::vector<int> off(col.size() + 1, 0), target, upper;
+    for (int r = 0; r < rows; ++r) {
+        diag[r] = find(r, r);
+        for (int slot = row_ptr[r]; slot < row_ptr[r + 1]; ++slot) {
+            off[slot] = (int)target.size();
+            const int elim = col[slot];
+            if (elim >= r) continue;
+            for (int u = row_ptr[elim]; u < row_ptr[elim + 1]; ++u) {
+                if (col[u] <= elim) continue;
+                const int t = find(r, col[u]);
+                if (t >= 0) {
+                    target.push_back(t);
+                    upper.push_back(u);
+                }
+            }
+        }
+    }
+    off.back() = (int)target.size();
+    auto upload = [&](const std::vector<int> &h) {
+        int *d = c->alloc<int>(std::max<size_t>(h.size(), 1));
+        if (!h.empty()) ck(cudaMemcpy(d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice), "upload pattern");
+        return d;
+    };
+    pl.rows = rows;
+    pl.m = m;
+    pl.nnz = (int)col.size();
+    pl.row_ptr = upload(row_ptr);
+    pl.col = upload(col);
+    pl.diag = upload(diag);
+    pl.slot_row = upload(slot_row);
+    pl.upd_off = upload(off);
+    pl.upd_target = upload(target);
+    pl.upd_upper = upload(upper);
+    pl.perm = c->alloc<int>((size_t)rows * m);
+    pl.vals = c->alloc<char>((size_t)pl.nnz * m * m * (c->mixed() ? sizeof(float) : sizeof(double)));
+}
+
 // Sizes, reference element and pools of a 1D context (dg_hdg_1d/src/discretization.cpp:4-14,
 // nodal_basis.hpp:34-65 with its separate quadrature rule).  Called after the stream exists.
 void create1(dgh_ctx *c, const dgh_config &k) {
@@ -843,6 +936,10 @@ void create1(dgh_ctx *c, const dgh_config &k) {
         c->face_pool = c->alloc<char>((size_t)c->faces * NV1 * NV1 * tsz);
         c->face_perm = c->alloc<int>((size_t)c->faces * NV1);
     }
+    if (c->ilu()) {
+        if (c->has_dg()) build_ilu_plan(c, c->ilu_dg, c->cells, c->m);
+        if (c->has_hdg()) build_ilu_plan(c, c->ilu_hdg, c->faces, NV1);
+    }
     const long long vn = std::max(c->has_dg() ? c->N : 0LL, c->has_hdg() ? c->NT : 0LL);
     c->vld = ((vn + 31) / 32) * 32;
     c->restart = k.restart;
@@ -887,6 +984,8 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
     const int rc = guard(c, [&] {
         const dgh_config &k = *cfg;
         need(k.dim == 1 || k.dim == 2, "Invalid dimension (1 or 2)");
+        need(k.preconditioner == 0 || k.preconditioner == 1, "Invalid block preconditioner");
+        need(k.preconditioner == 0 || k.dim == 1, "2D currently supports block-jacobi only");
         // config.cpp:6-22 (dg_hdg_1d/src/config.cpp:6-21 in 1D)
         need(k.nx >= 3 && (k.dim == 1 || k.ny >= 3) && k.degree >= 0 && k.degree <= 8 && k.quadrature >= 0,
              "Invalid mesh or degree");
@@ -991,6 +1090,8 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->ok = c->alloc<int>(1);
         ck(cudaMemset(c->status, 0, sizeof(int)), "memset");
         build_rule(c);
+        c->basis_dev = c->alloc<Basis1D>(1);
+        ck(cudaMemcpy(c->basis_dev, &c->basis, sizeof(Basis1D), cudaMemcpyHostToDevice), "upload basis");
         const int tb = 256;
         k_fill_mass<<<(unsigned)((c->N + tb - 1) / tb), tb, 0, c->stream>>>(c->mass, c->inv_mass, c->basis, c->g, n, c->N);
         k_fill_trace_mass<<<(unsigned)((c->NT + tb - 1) / tb), tb, 0, c->stream>>>(c->inv_trace_mass, c->basis, c->g, n, c->NT);
@@ -1561,6 +1662,30 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             need(dg ? c->linearised : c->condensed, dg ? "Refresh the volume Jacobian before assembling a block"
                                                        : "Condense the HDG operator before refreshing its preconditioner");
             const long long tot = dg ? (long long)c->cells * c->m * c->m : (long long)c->cells * 9;
+            if (c->ilu()) {
+                // BlockPreconditioner::refresh (block_ilu.hpp:14-19): every pattern block, then
+                // the sequential ILU(0) factorisation
+                auto &pl = dg ? c->ilu_dg : c->ilu_hdg;
+                const long long nb = (long long)pl.nnz * pl.m * pl.m;
+                auto run = [&](auto *vals) {
+                    using TF = std::remove_pointer_t<decltype(vals)>;
+                    if (dg) DGH_DISPATCH_N(c->n, {
+                            k1_ilu_dg_blocks<N, TF><<<grid1(nb), K1_THREADS, 0, c->stream>>>(
+                                vals, pl.slot_row, pl.col, pl.nnz, c->vol, c->fcache, c->b1, c->g1, c->inv_step);
+                        })
+                    else k1_ilu_face_blocks<TF><<<grid1(nb), K1_THREADS, 0, c->stream>>>(vals, pl.slot_row, pl.col, pl.nnz,
+                                                                                         c->S, c->speeds, c->g1);
+                    k1_ilu_factor<TF><<<1, ILU_THREADS, 0, c->stream>>>(vals, pl.perm, pl.row_ptr, pl.col, pl.diag,
+                                                                        pl.upd_off, pl.upd_target, pl.upd_upper, pl.rows,
+                                                                        pl.m, c->status);
+                    c->launched(2);
+                };
+                if (c->mixed()) run((float *)pl.vals);
+                else run((double *)pl.vals);
+                c->check_status();
+                (dg ? c->dg_factored : c->face_factored) = true;
+                return;
+            }
             if (c->mixed()) {
                 if (dg) DGH_DISPATCH_N(c->n, {
                         k1_dg_assemble<N, float><<<grid1(tot), K1_THREADS, 0, c->stream>>>(
@@ -1606,14 +1731,14 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
                                                                                                  c->basis, c->g);
                 });
                 c->launched();
-                launch_lu<float>(c, (float *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR, true);
+                launch_lu_narrow<float>(c, (float *)c->face_pool, c->fw, c->faces, c->face_perm, ST_SINGULAR);
             } else {
                 DGH_DISPATCH_N(c->n, {
                     k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (double *)c->face_pool,
                                                                                                   c->basis, c->g);
                 });
                 c->launched();
-                launch_lu<double>(c, (double *)c->face_pool, stride, c->fw, c->fw, c->faces, c->face_perm, ST_SINGULAR, true);
+                launch_lu_narrow<double>(c, (double *)c->face_pool, c->fw, c->faces, c->face_perm, ST_SINGULAR);
             }
             c->check_status();
             c->face_factored = true;

@@ -231,10 +231,13 @@ __global__ void k_face_cache(const double *__restrict__ traces, const double *__
 // ---- matrix-free J·v (volume_jacobian.cpp:59-71 + dg_operator.cpp:10-21) ---------------------
 // Needs the face traces of the direction d (k_face_trace on d).
 template <int N>
-__global__ void __launch_bounds__(Team<N>::THREADS)
+__global__ void __launch_bounds__(Team<N>::THREADS, 65536 / (Team<N>::THREADS * 72))
 k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const double *__restrict__ vol,
            const double *__restrict__ fcache, const double *__restrict__ speeds, double *__restrict__ out,
-           Basis1D b, Grid g, double inv_step) {
+           const Basis1D *__restrict__ bp, Grid g, double inv_step) {
+    // the basis tables are indexed per thread: read them through L1 from a device copy rather
+    // than from the kernel's parameter bank, where lane-varying indices serialise
+    const Basis1D &b = *bp;
     using T = Team<N>;
     __shared__ double fx[T::CPB][NVAR * T::P], fy[T::CPB][NVAR * T::P];
     __shared__ double ff[T::CPB][NFACES * N * NVAR];

@@ -366,6 +366,93 @@ k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restr
     }
 }
 
+// LU with row partial pivoting of narrow blocks (m <= 64, ld == m: the HDG face blocks, m = 4n)
+// with one warp per block in shared memory, written out in the slab layout of k_lu_solve.  The
+// pivot rule and the singularity test are k_lu's (first largest |a|; a NaN column keeps its
+// diagonal; a non-finite or subnormal-or-zero U diagonal sets singular_bit); lane r owns rows r
+// and r + 32 and eliminates them column by column.  Shared memory per warp: m (m + 1) T.
+constexpr int NARROW_THREADS = 128;
+template <typename T> constexpr size_t lu_narrow_smem_bytes(int m) {
+    return (size_t)(NARROW_THREADS / 32) * m * (m + 1) * sizeof(T);
+}
+template <typename T>
+__global__ void __launch_bounds__(NARROW_THREADS)
+k_lu_narrow(T *__restrict__ pool, int m, int count, int *__restrict__ perm_out, int *status, int singular_bit) {
+    constexpr int W = SlabVec<T>::W;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, pitch = m + 1;
+    T *S = reinterpret_cast<T *>(smraw) + (size_t)wib * m * pitch;
+    const int warps = gridDim.x * (NARROW_THREADS / 32);
+    for (int blk = blockIdx.x * (NARROW_THREADS / 32) + wib; blk < count; blk += warps) {
+        T *A = pool + (size_t)blk * m * m;
+        for (int e = lane; e < m * m; e += 32) S[(e / m) * pitch + e % m] = A[e];
+        int orig0 = lane, orig1 = lane + 32;  // original rows now at positions lane, lane + 32
+        __syncwarp();
+        for (int j = 0; j < m; ++j) {
+            T best = T(-1);
+            int bi = 0x7fffffff;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = lane + 32 * h;
+                if (r >= j && r < m) {
+                    const T a = tabs(S[r * pitch + j]);
+                    if (a > best) { best = a; bi = r; }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            const int p = (bi == 0x7fffffff || !(best == best)) ? j : bi;
+            if (p != j) {
+                for (int c = lane; c < m; c += 32) {
+                    const T t = S[j * pitch + c];
+                    S[j * pitch + c] = S[p * pitch + c];
+                    S[p * pitch + c] = t;
+                }
+                // the original row indices follow the rows
+                const int oj = __shfl_sync(0xffffffffu, j < 32 ? orig0 : orig1, j & 31);
+                const int op = __shfl_sync(0xffffffffu, p < 32 ? orig0 : orig1, p & 31);
+                if (lane == (j & 31)) { if (j < 32) orig0 = op; else orig1 = op; }
+                if (lane == (p & 31)) { if (p < 32) orig0 = oj; else orig1 = oj; }
+            }
+            __syncwarp();
+            const T pivot = S[j * pitch + j];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = lane + 32 * h;
+                if (r > j && r < m) {
+                    T l = S[r * pitch + j];
+                    if (pivot != T(0)) l = l / pivot;
+                    S[r * pitch + j] = l;
+                    for (int c = j + 1; c < m; ++c) S[r * pitch + c] -= l * S[j * pitch + c];
+                }
+            }
+            __syncwarp();
+        }
+        bool bad = false;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = lane + 32 * h;
+            if (r < m) {
+                const double dd = (double)S[r * pitch + r];
+                if (!isfinite(dd) || !(fabs(dd) > 2.2250738585072014e-308)) bad = true;
+                perm_out[(size_t)blk * m + r] = h ? orig1 : orig0;
+            }
+        }
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, singular_bit);
+        // slab layout: element (r, c) of slab s = r / 32 at 32 s m + (c / W) nt W + (r % 32) W + c % W
+        for (int e = lane; e < m * m; e += 32) {
+            const int s = e / (32 * m), off = e - s * 32 * m, nt = min(32, m - 32 * s);
+            const int g = off / (nt * W), rem = off - g * nt * W, i = rem / W, w = rem % W;
+            A[e] = S[(32 * s + i) * pitch + g * W + w];
+        }
+        __syncwarp();
+    }
+}
+
 // Block solve z = A^{-1} b with the factors of k_lu (block_jacobi.hpp:24-39): permute, unit
 // lower solve, upper solve.  One warp owns one block and streams its factors exactly once with
 // no CTA-wide barriers; lane i owns row 32 s + i of slab s and reads 16-byte column groups of

@@ -72,6 +72,8 @@ typedef struct dgh_config {
     int device;       /* CUDA device ordinal                                               */
     int dim;          /* 2 (dg_hdg_2d, the default) or 1 (dg_hdg_1d)                       */
     int autotune;     /* 2D: time the factorisation variants on the first refresh (per degree) */
+    int preconditioner; /* 0 block Jacobi; 1 block ILU(0), natural ordering (1D only,        */
+                        /* common/src/linalg/block_ilu.cpp:15-84)                            */
 } dgh_config;
 
 /* config.hpp:7-18 defaults: nx=ny=8, k=3, restart 30, max_linear 1500, max_newton 30,
@@ -153,7 +155,7 @@ int dgh_dg_apply_T(dgh_ctx *ctx, const double *w, double *jtw);    /* 2D only */
 /* Diagonal block (row == col), copied to the host row-major m x m (dg_operator.cpp:22-48). */
 int dgh_dg_block(dgh_ctx *ctx, int row, int col, double *host_block);
 
-/* ---- BlockJacobi (block_jacobi.hpp:7-47) ---------------------------------------------------- */
+/* ---- BlockJacobi / BlockPreconditioner (block_jacobi.hpp:7-47) ---------------------------------------------------- */
 /* op DGH_OP_DG: assemble and factor the E cell blocks from the current DG linearisation;
  * op DGH_OP_HDG: the 2E face blocks of the current condensed operator.  dgh_precond_apply with
  * DGH_OP_DG_T applies the transposed cell-block solves (A^{-T}) from the DG factors. */

@@ -649,6 +649,23 @@ struct Jacobi {
         for (int i = 0; i < blocks; ++i) lus[i].solve(&rhs[(size_t)i * width], &out[(size_t)i * width]);
     }
 };
+// BlockPreconditioner on BlockGraph::periodic(cells) (dg_hdg_1d/src/time_integrator.cpp:31-36):
+// block Jacobi or block ILU(0) in the natural ordering.
+struct Precond1D {
+    Jacobi jacobi;
+    std::unique_ptr<oracle::BlockILU0> ilu;
+    Precond1D(int blocks, int width, bool use_ilu) : jacobi(blocks, width) {
+        if (use_ilu) ilu = std::make_unique<oracle::BlockILU0>(oracle::periodic_adjacency(blocks), width);
+    }
+    template <class F> void refresh(F &&provider) {
+        if (ilu) ilu->refresh(provider);
+        else jacobi.refresh(provider);
+    }
+    void apply(const Vec &rhs, Vec &out) const {
+        if (ilu) ilu->apply(rhs, out);
+        else jacobi.apply(rhs, out);
+    }
+};
 }  // namespace
 
 oracle::RunStatistics advance(Problem &p, Method method, Vec &solution) {
@@ -656,7 +673,7 @@ oracle::RunStatistics advance(Problem &p, Method method, Vec &solution) {
     const int N = p.size(), NT = p.cells * NVAR;
     const bool dg = method == Method::DG;
     require(!c.direct, "The dense direct solve is not restated in the oracle");
-    require(!c.ilu, "Block ILU(0) is not restated in the oracle");
+    require(!(c.ilu && c.colamd), "The block COLAMD ordering is not restated in the oracle");
     Vec state(N), trial(N), residual(N), trial_residual(N), direction(N), rhs(dg ? N : NT);
     Vec trace_direction(NT), equation_error(N), independent(N), step_state(N), stage_base(N);
     std::vector<Vec> slopes(4, Vec(N));
@@ -666,7 +683,7 @@ oracle::RunStatistics advance(Problem &p, Method method, Vec &solution) {
     if (dg) dgop = std::make_unique<DGOperator>(p);
     else hybrid = std::make_unique<HybridOperator>(p);
     if (!dg && c.check_update) diagnostic = std::make_unique<DGOperator>(p);
-    Jacobi precond(p.cells, dg ? p.block : NVAR);
+    Precond1D precond(p.cells, dg ? p.block : NVAR, c.ilu);
     oracle::GMRES gmres(dg ? N : NT, c.restart, weights);
     auto dual_norm = [&](const Vec &x) {
         double s = 0;
@@ -733,7 +750,7 @@ oracle::RunStatistics advance(Problem &p, Method method, Vec &solution) {
                     for (int i = 0; i < N; ++i) rhs[i] = -residual[i];
                     precond.refresh([&](int row, int col, double *out) { dgop->block(row, col, out); });
                     linear = gmres.solve(oracle::Action{dgop.get(), bind_apply<DGOperator>},
-                                         oracle::Action{&precond, bind_apply<Jacobi>}, rhs, direction, c.max_linear,
+                                         oracle::Action{&precond, bind_apply<Precond1D>}, rhs, direction, c.max_linear,
                                          c.linear_tolerance);
                     for (int i = 0; i < N; ++i) equation_error[i] = -gmres.residual()[i];
                 } else {
@@ -745,7 +762,7 @@ oracle::RunStatistics advance(Problem &p, Method method, Vec &solution) {
                     for (int attempt = 0; attempt < 4; ++attempt) {
                         const oracle::LinearResult cur =
                             gmres.solve(oracle::Action{hybrid.get(), bind_apply<HybridOperator>},
-                                        oracle::Action{&precond, bind_apply<Jacobi>}, rhs, trace_direction,
+                                        oracle::Action{&precond, bind_apply<Precond1D>}, rhs, trace_direction,
                                         c.max_linear, tolerance);
                         linear.iterations += cur.iterations;
                         linear.relative_residual = cur.relative_residual;

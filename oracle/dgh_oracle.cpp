@@ -951,6 +951,106 @@ void DenseLU::solve(const double *b, double *x) const {
     }
     for (int i = 0; i < m; ++i) x[i] = t[i];
 }
+// dense_lu.hpp:42-49: row by row, solve with U^T (lower, U's diagonal), then L^T (unit upper),
+// then apply P^T.
+void DenseLU::right_solve(double *x) const {
+    Vec s(m);
+    for (int r = 0; r < m; ++r) {
+        for (int i = 0; i < m; ++i) s[i] = x[(size_t)i * m + r];
+        for (int i = 0; i < m; ++i) {
+            double v = s[i];
+            for (int k = 0; k < i; ++k) v -= lu[(size_t)i * m + k] * s[k];  // U(k, i) = lu[i*m + k]
+            s[i] = v / lu[(size_t)i * m + i];
+        }
+        for (int i = m - 1; i >= 0; --i) {
+            double v = s[i];
+            for (int k = i + 1; k < m; ++k) v -= lu[(size_t)i * m + k] * s[k];  // L(k, i) = lu[i*m + k]
+            s[i] = v;
+        }
+        for (int i = 0; i < m; ++i) x[(size_t)perm[i] * m + r] = s[i];
+    }
+}
+std::vector<std::vector<int>> periodic_adjacency(int cells) {
+    std::vector<std::vector<int>> adj(cells);
+    for (int c = 0; c < cells; ++c) adj[c] = {(c + cells - 1) % cells, c, (c + 1) % cells};
+    return adj;
+}
+BlockILU0::BlockILU0(const std::vector<std::vector<int>> &adjacency, int w)
+    : rows((int)adjacency.size()), width(w), row_ptr(rows + 1, 0), diag(rows), lus(rows) {
+    for (int r = 0; r < rows; ++r) {
+        auto row = adjacency[r];
+        row.push_back(r);
+        std::sort(row.begin(), row.end());
+        row.erase(std::unique(row.begin(), row.end()), row.end());
+        col_idx.insert(col_idx.end(), row.begin(), row.end());
+        row_ptr[r + 1] = (int)col_idx.size();
+    }
+    values.assign(col_idx.size() * (size_t)w * w, 0.);
+    upd_off.assign(col_idx.size() + 1, 0);
+    for (int row = 0; row < rows; ++row) {
+        diag[row] = find(row, row);
+        for (int slot = row_ptr[row]; slot < row_ptr[row + 1]; ++slot) {
+            upd_off[slot] = (int)upd_target.size();
+            const int elim = col_idx[slot];
+            if (elim >= row) continue;
+            for (int upper = row_ptr[elim]; upper < row_ptr[elim + 1]; ++upper) {
+                const int column = col_idx[upper];
+                if (column <= elim) continue;
+                const int target = find(row, column);
+                if (target >= 0) {
+                    upd_target.push_back(target);
+                    upd_upper.push_back(upper);
+                }
+            }
+        }
+    }
+    upd_off.back() = (int)upd_target.size();
+}
+int BlockILU0::find(int row, int col) const {
+    for (int p = row_ptr[row]; p < row_ptr[row + 1]; ++p)
+        if (col_idx[p] == col) return p;
+    return -1;
+}
+// block_ilu.cpp:48-61 (factorize) after the provider filled every pattern block.
+void BlockILU0::refresh(const std::function<void(int, int, double *)> &provider) {
+    for (int row = 0; row < rows; ++row)
+        for (int p = row_ptr[row]; p < row_ptr[row + 1]; ++p) provider(row, col_idx[p], block(p));
+    const int w = width;
+    for (int i = 0; i < rows; ++i) {
+        for (int p = row_ptr[i]; p < diag[i]; ++p) {
+            lus[col_idx[p]].right_solve(block(p));
+            for (int u = upd_off[p]; u < upd_off[p + 1]; ++u) {
+                // dense_lu.hpp:53-57: destination.col(j) -= right(k, j) * left.col(k)
+                double *dst = block(upd_target[u]);
+                const double *left = block(p), *right = block(upd_upper[u]);
+                for (int j = 0; j < w; ++j)
+                    for (int k = 0; k < w; ++k) {
+                        const double r = right[(size_t)j * w + k];
+                        for (int q = 0; q < w; ++q) dst[(size_t)j * w + q] -= r * left[(size_t)k * w + q];
+                    }
+            }
+        }
+        lus[i].compute(block(diag[i]), w);
+    }
+}
+// block_ilu.cpp:62-84 (apply, natural order)
+void BlockILU0::apply(const Vec &rhs, Vec &result) const {
+    const int w = width;
+    Vec work(rhs.begin(), rhs.end());
+    auto gemv_sub = [&](const double *blk, int row, int col) {
+        for (int k = 0; k < w; ++k) {
+            const double xk = work[(size_t)col * w + k];
+            for (int q = 0; q < w; ++q) work[(size_t)row * w + q] -= blk[(size_t)k * w + q] * xk;
+        }
+    };
+    for (int i = 0; i < rows; ++i)
+        for (int p = row_ptr[i]; p < diag[i]; ++p) gemv_sub(block(p), i, col_idx[p]);
+    for (int i = rows - 1; i >= 0; --i) {
+        for (int p = diag[i] + 1; p < row_ptr[i + 1]; ++p) gemv_sub(block(p), i, col_idx[p]);
+        lus[i].solve(&work[(size_t)i * w], &work[(size_t)i * w]);
+    }
+    result = work;
+}
 BlockJacobi::BlockJacobi(int b, int w) : blocks(b), width(w), lus(b) {}
 void BlockJacobi::refresh(const std::function<void(int, int, double *)> &provider) {
     std::string failure;

@@ -153,7 +153,27 @@ struct DenseLU {
     std::vector<int> perm;   // P: (P b)[i] = b[perm[i]]
     void compute(const double *a, int width);   // throws on non-finite / singular
     void solve(const double *b, double *x) const;  // x may alias b
+    void right_solve(double *x) const;             // X <- X A^{-1}, X column-major m x m
 };
+// block_ilu.cpp:15-84 with the natural ordering (block_graph.cpp:7-19 pattern: each row's
+// columns sorted, the diagonal included): the ILU(0) kind of BlockPreconditioner.  Blocks are
+// column-major width x width; the provider fills block (row, col).
+class BlockILU0 {
+  public:
+    BlockILU0(const std::vector<std::vector<int>> &adjacency, int width);
+    void refresh(const std::function<void(int, int, double *)> &provider);
+    void apply(const Vec &rhs, Vec &result) const;
+    int rows, width;
+    std::vector<int> row_ptr, col_idx, diag;
+    std::vector<int> upd_off, upd_target, upd_upper;  // block_ilu.cpp:24-45 symbolic schedule
+    Vec values;
+    std::vector<DenseLU> lus;
+    double *block(int slot) { return &values[(size_t)slot * width * width]; }
+    const double *block(int slot) const { return &values[(size_t)slot * width * width]; }
+    int find(int row, int col) const;
+};
+// BlockGraph::periodic(cells) adjacency (block_graph.cpp:30-35)
+std::vector<std::vector<int>> periodic_adjacency(int cells);
 class BlockJacobi {
   public:
     BlockJacobi(int blocks, int width);

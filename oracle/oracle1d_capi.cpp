@@ -18,6 +18,7 @@ struct Handle1 {
     std::unique_ptr<DGOperator> dg;
     std::unique_ptr<HybridOperator> hdg;
     std::vector<oracle::DenseLU> pc_dg, pc_hdg;
+    std::unique_ptr<oracle::BlockILU0> ilu_dg, ilu_hdg;  // --precond block-ilu0
 };
 template <class F> int guard(F &&f) {
     try {
@@ -131,11 +132,23 @@ int oracle1d_dg_block(void *h, int row, int col, double *o) {
 }
 int oracle1d_dg_precond_refresh(void *h) {
     return guard([&] {
-        factor(H(h)->pc_dg, H(h)->p->cells, H(h)->p->block, [&](int r, int c, double *o) { H(h)->dg->block(r, c, o); });
+        Handle1 *k = H(h);
+        auto provider = [&](int r, int c, double *o) { k->dg->block(r, c, o); };
+        if (k->p->config.ilu) {
+            k->ilu_dg = std::make_unique<oracle::BlockILU0>(oracle::periodic_adjacency(k->p->cells), k->p->block);
+            k->ilu_dg->refresh(provider);
+        } else {
+            factor(k->pc_dg, k->p->cells, k->p->block, provider);
+        }
     });
 }
 int oracle1d_dg_precond_apply(void *h, const double *x, double *z) {
-    return guard([&] { Vec o; solve_all(H(h)->pc_dg, H(h)->p->block, vec(x, H(h)->p->size()), o); out(o, z); });
+    return guard([&] {
+        Vec o;
+        if (H(h)->ilu_dg) H(h)->ilu_dg->apply(vec(x, H(h)->p->size()), o);
+        else solve_all(H(h)->pc_dg, H(h)->p->block, vec(x, H(h)->p->size()), o);
+        out(o, z);
+    });
 }
 int oracle1d_hdg_refresh(void *h, const double *u, const double *r) {
     return guard([&] { H(h)->hdg->refresh_projected(vec(u, H(h)->p->size()), vec(r, H(h)->p->size())); });
@@ -156,11 +169,23 @@ int oracle1d_hdg_recovered_residual(void *h, const double *dl, double *o) {
 }
 int oracle1d_hdg_precond_refresh(void *h) {
     return guard([&] {
-        factor(H(h)->pc_hdg, H(h)->p->cells, NVAR, [&](int r, int c, double *o) { H(h)->hdg->block(r, c, o); });
+        Handle1 *k = H(h);
+        auto provider = [&](int r, int c, double *o) { k->hdg->block(r, c, o); };
+        if (k->p->config.ilu) {
+            k->ilu_hdg = std::make_unique<oracle::BlockILU0>(oracle::periodic_adjacency(k->p->cells), NVAR);
+            k->ilu_hdg->refresh(provider);
+        } else {
+            factor(k->pc_hdg, k->p->cells, NVAR, provider);
+        }
     });
 }
 int oracle1d_hdg_precond_apply(void *h, const double *x, double *z) {
-    return guard([&] { Vec o; solve_all(H(h)->pc_hdg, NVAR, vec(x, (size_t)H(h)->p->cells * NVAR), o); out(o, z); });
+    return guard([&] {
+        Vec o;
+        if (H(h)->ilu_hdg) H(h)->ilu_hdg->apply(vec(x, (size_t)H(h)->p->cells * NVAR), o);
+        else solve_all(H(h)->pc_hdg, NVAR, vec(x, (size_t)H(h)->p->cells * NVAR), o);
+        out(o, z);
+    });
 }
 // op 0: DG J*v with block Jacobi, weights M^-1; op 1: Schur apply with face blocks, weights 1
 // (dg_hdg_1d/src/time_integrator.cpp:27).
@@ -172,11 +197,13 @@ int oracle1d_gmres(void *h, int op, int restart, const double *rhs, double *x, i
         oracle::GMRES g(n, restart, op == 0 ? k->p->inverse_mass : Vec(n, 1.));
         Vec xv;
         oracle::LinearResult res;
-        struct Pc { const std::vector<oracle::DenseLU> *lus; int width; };
-        Pc pc{op == 0 ? &k->pc_dg : &k->pc_hdg, op == 0 ? k->p->block : NVAR};
+        struct Pc { const std::vector<oracle::DenseLU> *lus; int width; const oracle::BlockILU0 *ilu; };
+        Pc pc{op == 0 ? &k->pc_dg : &k->pc_hdg, op == 0 ? k->p->block : NVAR,
+              op == 0 ? k->ilu_dg.get() : k->ilu_hdg.get()};
         const oracle::Action M{&pc, [](const void *c, const Vec &a, Vec &b) {
                                    const Pc *q = static_cast<const Pc *>(c);
-                                   solve_all(*q->lus, q->width, a, b);
+                                   if (q->ilu) q->ilu->apply(a, b);
+                                   else solve_all(*q->lus, q->width, a, b);
                                }};
         if (op == 0)
             res = g.solve(oracle::Action{k->dg.get(), [](const void *c, const Vec &a, Vec &b) {

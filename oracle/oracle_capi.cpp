@@ -3,6 +3,8 @@
 // Functions return 0 on success and 1 on a thrown require(); oracle_error() gives the text.
 #include "dgh_oracle.hpp"
 
+#include <map>
+
 #include <cstring>
 #include <memory>
 #include <sstream>
@@ -251,6 +253,51 @@ int oracle_advance(void *hv, int method, double *u, double *stats8, double *upda
             std::memcpy(updates + 13 * k, row, sizeof(row));
         }
         *n_updates = (int)st.updates.size();
+    });
+}
+// The exactness property the reference's own check asserts for block ILU(0)
+// (dg_hdg_1d/check/check_1d.cpp:109-138): on a block path graph (natural ordering) and on a
+// full block graph ILU(0) has no dropped fill, so one application solves A x = A exact.
+// Off-diagonal blocks 0.03 * uniform[-1, 1) from a fixed LCG, diagonal blocks the cyclic
+// shift with entries 3 + v.  Returns max |x - exact| in *err.
+int oracle_ilu_exactness(int count, int width, int full, double *err) {
+    return guard([&] {
+        std::vector<std::vector<int>> adj(count);
+        for (int i = 0; i < count; ++i)
+            for (int j = 0; j < count; ++j)
+                if (full || std::abs(i - j) <= 1) adj[i].push_back(j);
+        unsigned long long state = 12345;
+        auto uniform = [&] {
+            state = state * 6364136223846793005ULL + 1442695040888963407ULL;
+            return (double)(state >> 11) / 9007199254740992.0 * 2 - 1;
+        };
+        const size_t w2 = (size_t)width * width;
+        std::map<std::pair<int, int>, Vec> blocks;
+        for (int i = 0; i < count; ++i)
+            for (int j : adj[i]) {
+                Vec b(w2, 0.);
+                if (i == j) {
+                    for (int v = 0; v < width; ++v) b[(size_t)((v + 1) % width) * width + v] = 3 + v;
+                } else {
+                    for (auto &x : b) x = .03 * uniform();
+                }
+                blocks[{i, j}] = b;
+            }
+        Vec exact((size_t)count * width), rhs((size_t)count * width, 0.), x;
+        for (size_t i = 0; i < exact.size(); ++i) exact[i] = std::sin(1.0 + 0.37 * (double)i);
+        for (auto &[key, b] : blocks)
+            for (int c = 0; c < width; ++c)
+                for (int r = 0; r < width; ++r)
+                    rhs[(size_t)key.first * width + r] += b[(size_t)c * width + r] * exact[(size_t)key.second * width + c];
+        oracle::BlockILU0 ilu(adj, width);
+        ilu.refresh([&](int r, int c, double *o) {
+            const Vec &b = blocks.at({r, c});
+            std::copy(b.begin(), b.end(), o);
+        });
+        ilu.apply(rhs, x);
+        double e = 0;
+        for (size_t i = 0; i < x.size(); ++i) e = std::max(e, std::abs(x[i] - exact[i]));
+        *err = e;
     });
 }
 }

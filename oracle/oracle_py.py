@@ -418,3 +418,12 @@ def run_cli_1d(args: list[str], cwd: str | None = None) -> subprocess.CompletedP
     if not CLI1D_PATH.exists():
         build()
     return subprocess.run([str(CLI1D_PATH), *args], cwd=cwd, capture_output=True, text=True)
+
+
+def ilu_exactness(count: int, width: int, full: bool) -> float:
+    """max |x - exact| of one block ILU(0) application on the path (full=False) or full block
+    graph of the reference's own check (check_1d.cpp:109-138)."""
+    err = ctypes.c_double()
+    if lib().oracle_ilu_exactness(count, width, 1 if full else 0, ctypes.byref(err)) != 0:
+        raise OracleError(lib().oracle_error().decode())
+    return err.value

@@ -112,6 +112,25 @@ def test_mixed_precision_precond(oracle_mod, nx, ny, k):
     assert rel(zg, zo) <= 1e-4
 
 
+@pytest.mark.parametrize("nx,ny,k", [(4, 4, 2), (3, 4, 4), (3, 3, 8)])
+def test_mixed_precision_hdg_face_precond(oracle_mod, nx, ny, k):
+    """FP32 face-block factors (warp-per-block LU) against the oracle's FP64 block Jacobi."""
+    o, s = setup_pair(oracle_mod, nx, ny, k, precision="mixed")
+    uo = o.initial()
+    ug = s.tensor(uo)
+    o.freeze(uo)
+    s.freeze(ug)
+    o.set_stage(uo, .003)
+    s.set_stage(ug, .003)
+    r = o.residual(uo)
+    o.hdg_refresh(uo, r)
+    s.hdg_refresh_projected(ug, s.tensor(r))
+    o.hdg_precond_refresh()
+    s.precond_refresh("hdg")
+    dl = direction(o.trace_size)
+    assert rel(np_(s.precond_apply("hdg", s.tensor(dl))), o.hdg_precond_apply(dl)) <= 1e-4
+
+
 @pytest.mark.parametrize("nx,ny,k", CASES)
 def test_hdg_condensation_schur_recovery(oracle_mod, nx, ny, k):
     o, s = setup_pair(oracle_mod, nx, ny, k)
