@@ -1,8 +1,8 @@
 // dgh1d: command-line front end of the B200 solver for the 1D problem, flag- and
 // CSV-compatible with the reference's dg_hdg_1d (dg_hdg_1d/src/main.cpp:7-107,
-// config.cpp:22-115).  The device path implements the block-Jacobi GMRES solve; --precond
-// block-ilu0 and --linear direct are refused with a message.  Additional flags: --precision
-// fp64|mixed (block-Jacobi factor precision) and --device N.
+// config.cpp:22-115).  The device path implements GMRES with block Jacobi or block ILU(0) in the
+// natural ordering; --ordering colamd with block-ilu0 and --linear direct are refused with a
+// message.  Additional flags: --precision fp64|mixed (block factor precision) and --device N.
 #include "dgh_gpu.h"
 
 #include <cmath>
@@ -32,7 +32,7 @@ Options parse(int argc, char **argv) {
     o.cfg.dim = 1;
     o.cfg.nx = 32;  // dg_hdg_1d/include/euler/config.hpp:8
     o.cfg.ny = 1;
-    bool time_seen = false, steps_seen = false, ilu = false, direct = false;
+    bool time_seen = false, steps_seen = false, ilu = false, direct = false, colamd = false;
     for (int i = 1; i < argc; ++i) {
         const std::string option = argv[i];
         auto value = [&]() {
@@ -86,6 +86,7 @@ Options parse(int argc, char **argv) {
         } else if (option == "--ordering") {
             auto order = value();
             require(order == "natural" || order == "colamd", "Invalid ordering");
+            colamd = order == "colamd";
         } else if (option == "--precond") {
             auto name = value();
             require(name == "block-jacobi" || name == "block-ilu0", "Invalid block preconditioner");
@@ -93,7 +94,7 @@ Options parse(int argc, char **argv) {
         } else if (option == "--help") {
             std::cout << "1D periodic Euler DG / condensed HDG on one B200\n"
                          "--cells N --k K --quad Q --cfl C (--T T | --steps N)\n"
-                         "--method dg|hdg|both --linear gmres --precond block-jacobi\n"
+                         "--method dg|hdg|both --linear gmres --precond block-jacobi|block-ilu0\n"
                          "--ordering natural --restart N --max-linear N --max-newton N\n"
                          "--ntol R --ltol R --safety S --prefix PATH\n"
                          "--integrator ssp-dirk3|be --newton-steps N --warmup-updates N\n"
@@ -107,7 +108,8 @@ Options parse(int argc, char **argv) {
     require(o.integrator == "be" || o.integrator == "ssp-dirk3", "Invalid integrator");
     require(o.method == "dg" || o.method == "hdg" || o.method == "both", "Method must be dg, hdg, or both");
     require(!direct, "The dense --linear direct reference is a CPU-only check; use gmres");
-    require(!ilu, "The device solver implements --precond block-jacobi only");
+    require(!(ilu && colamd), "The device solver implements the natural block ordering only");
+    o.cfg.preconditioner = ilu ? 1 : 0;
     o.cfg.integrator = o.integrator == "be" ? DGH_INTEGRATOR_BE : DGH_INTEGRATOR_DIRK3;
     return o;
 }
@@ -203,7 +205,8 @@ int main(int argc, char **argv) {
                 ck(dgh_l2_error(ctx, dev, st.final_time, err));
             }
             summary << name << ',' << cells << ',' << base.degree << ',' << quad << ',' << base.cfl << ','
-                    << o.integrator << ",gmres,block-jacobi,natural," << base.nonlinear_tolerance << ','
+                    << o.integrator << ",gmres," << (base.preconditioner ? "block-ilu0" : "block-jacobi") << ",natural,"
+                    << base.nonlinear_tolerance << ','
                     << base.linear_tolerance << ',' << base.safety << ',' << base.newton_steps << ','
                     << base.warmup_updates << ',' << st.steps << ',' << st.final_time << ',' << st.newton_iterations
                     << ',' << st.krylov_iterations << ',' << st.max_linear_residual << ',' << st.max_dg_linear_residual

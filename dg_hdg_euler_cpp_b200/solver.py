@@ -19,6 +19,7 @@ METHODS = {"dg": 0, "hdg": 1, "both": 2}
 INTEGRATORS = {"ssp-dirk3": 0, "be": 1}
 TESTCASES = {"diagonal": 0, "wave": 1, "axis": 2}
 PRECISIONS = {"fp64": 0, "mixed": 1}
+PRECONDITIONERS = {"block-jacobi": 0, "block-ilu0": 1}
 OPS = {"dg": 0, "hdg": 1, "dg_t": 2}
 
 
@@ -33,7 +34,7 @@ def make_config(**kw) -> _lib.dgh_config:
     cfg = _lib.dgh_config()
     lib.dgh_config_default(ctypes.byref(cfg))
     aliases = {"k": "degree", "ntol": "nonlinear_tolerance", "ltol": "linear_tolerance", "T": "final_time",
-               "cells": "nx", "quad": "quadrature"}
+               "cells": "nx", "quad": "quadrature", "precond": "preconditioner"}
     for key, val in kw.items():
         key = aliases.get(key, key)
         if key == "method":
@@ -44,6 +45,8 @@ def make_config(**kw) -> _lib.dgh_config:
             val = TESTCASES[val] if isinstance(val, str) else val
         elif key == "precision":
             val = PRECISIONS[val] if isinstance(val, str) else val
+        elif key == "preconditioner":
+            val = PRECONDITIONERS[val] if isinstance(val, str) else val
         if not hasattr(cfg, key):
             raise KeyError(key)
         setattr(cfg, key, val)

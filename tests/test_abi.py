@@ -85,14 +85,16 @@ def test_dimension_and_quadrature_validation(lib, fields, message):
 
 
 def test_1d_cli_validates_flags_before_device_work():
-    """The 1D front end parses dg_hdg_1d's flags and refuses the paths it does not build."""
+    """The 1D front end parses dg_hdg_1d's flags and refuses the paths it does not build
+    (the block COLAMD ordering, the dense direct solve)."""
     import subprocess
 
     from dg_hdg_euler_cpp_b200 import BIN1D_PATH
 
     if not BIN1D_PATH.exists():
         pytest.skip("dgh1d not built")
-    for args, msg in [(["--precond", "block-ilu0"], "block-jacobi only"), (["--linear", "direct"], "CPU-only"),
+    for args, msg in [(["--precond", "block-ilu0", "--ordering", "colamd"], "natural block ordering only"),
+                      (["--linear", "direct"], "CPU-only"),
                       (["--T", ".1", "--steps", "2"], "Choose either --T or --steps"),
                       (["--integrator", "rk4"], "Invalid integrator"), (["--bogus"], "Unknown option")]:
         res = subprocess.run([str(BIN1D_PATH), *args], capture_output=True, text=True, timeout=60)

@@ -266,3 +266,92 @@ def test_device_errors_use_the_reference_messages():
     bad[0] = -5.0  # density at the node nearest x = -1: the left trace of cell 0 turns negative
     with pytest.raises(DGHError, match="Invalid frozen face state"):
         s.freeze(bad)
+
+
+# ---- block ILU(0) (--precond block-ilu0, block_ilu.cpp:15-84, natural ordering) ---------------
+@pytest.mark.parametrize("cells,k,quad,precision,tol", [(8, 2, 0, "fp64", 1e-10), (6, 3, 6, "fp64", 1e-10),
+                                                        (5, 8, 0, "fp64", 1e-10), (3, 1, 0, "fp64", 1e-10),
+                                                        (7, 3, 0, "mixed", 1e-4)])
+def test_block_ilu0_precond(oracle_mod, cells, k, quad, precision, tol):
+    """The ILU(0) factors of the periodic DG and trace block patterns and their two sweeps
+    against the oracle's restatement (FP64: 1e-10; FP32 factors: 1e-4)."""
+    from dg_hdg_euler_cpp_b200.solver import Solver
+
+    o = oracle_mod.Oracle1D(f"--cells {cells} --k {k} --quad {quad} --integrator be --steps 1 --precond block-ilu0")
+    s = Solver(dim=1, cells=cells, k=k, quad=quad, cfl=2.0, integrator="be", steps=1, method="both",
+               precision=precision, precond="block-ilu0")
+    u = o.initial()
+    ug = s.tensor(u)
+    o.freeze(u)
+    s.freeze(ug)
+    o.set_stage(u, .05)
+    s.set_stage(ug, .05)
+    up = u + 1e-3 * direction(u.size)
+    o.dg_refresh(up)
+    s.dg_refresh(s.tensor(up))
+    o.dg_precond_refresh()
+    s.precond_refresh("dg")
+    d = direction(u.size, .31, .79)
+    assert rel(np_(s.precond_apply("dg", s.tensor(d))), o.dg_precond_apply(d)) <= tol
+    r = o.residual(up)
+    o.hdg_refresh(up, r)
+    s.hdg_refresh_projected(s.tensor(up), s.tensor(r))
+    o.hdg_precond_refresh()
+    s.precond_refresh("hdg")
+    dl = direction(o.trace_size, .31, .79)
+    assert rel(np_(s.precond_apply("hdg", s.tensor(dl))), o.hdg_precond_apply(dl)) <= tol
+    s.close()
+
+
+@pytest.mark.parametrize("k,integrator", [(2, "ssp-dirk3"), (4, "be")])
+def test_block_ilu0_advance_matches_oracle(oracle_mod, k, integrator):
+    """TimeIntegrator::advance with block ILU(0) on 12 cells, both methods, device vs oracle."""
+    from dg_hdg_euler_cpp_b200.solver import Solver
+
+    args = f"--cells 12 --k {k} --cfl 2 --integrator {integrator} --T 0.05 --restart 20 --precond block-ilu0"
+    o = oracle_mod.Oracle1D(args)
+    u0 = o.initial()
+    for method in ("dg", "hdg"):
+        so, st_o, _ = o.advance(method, u0)
+        s = Solver(dim=1, cells=12, k=k, cfl=2.0, integrator=integrator, final_time=0.05, restart=20, method=method,
+                   precond="block-ilu0")
+        sg, st_g, _ = s.advance(method, u0)
+        assert np.max(np.abs(sg - so)) <= 1e-10 * np.max(np.abs(so))
+        assert st_g["newton_iterations"] == st_o["newton_iterations"]
+        assert abs(st_g["krylov_iterations"] - st_o["krylov_iterations"]) <= st_o["newton_iterations"]
+        s.close()
+
+
+def test_block_ilu0_cli_matches_oracle_cli(oracle_mod):
+    """dgh1d --precond block-ilu0 against the oracle's CLI on the same run: histories, Krylov
+    counts and L2 errors."""
+    args = ["--cells", "32", "--k", "3", "--steps", "2", "--method", "both", "--cfl", "2", "--restart", "20",
+            "--precond", "block-ilu0"]
+    with tempfile.TemporaryDirectory() as tmp:
+        res = run_cli([*args, "--prefix", f"{tmp}/gpu"])
+        assert res.returncode == 0, res.stderr + res.stdout
+        oracle_mod.run_cli_1d([*args, "--prefix", f"{tmp}/cpu"])
+        its, ref = read_csv(f"{tmp}/gpu_iterations.csv"), read_csv(f"{tmp}/cpu_iterations.csv")
+        summ, sref = read_csv(f"{tmp}/gpu_summary.csv"), read_csv(f"{tmp}/cpu_summary.csv")
+    assert_history_close(its, ref, rtol=1e-10, krylov_slack=1)
+    for a, b in zip(summ, sref):
+        assert a["preconditioner"] == b["preconditioner"] == "block-ilu0"
+        for key in ("rho_L2", "momentum_L2", "energy_L2"):
+            assert abs(float(a[key]) - float(b[key])) <= 1e-10 * float(b[key]), key
+
+
+def test_block_ilu0_nonfinite_block_message():
+    """A non-finite block reaching the ILU(0) factorisation reports DenseLU's require() text
+    (dense_lu.hpp:11-12) and stops the refresh."""
+    from dg_hdg_euler_cpp_b200.solver import DGHError, Solver
+
+    s = Solver(dim=1, cells=4, k=2, method="dg", precond="block-ilu0")
+    u = s.initial()
+    s.freeze(u)
+    s.set_stage(u, .05)
+    bad = u.clone()
+    bad[3] = float("nan")
+    s.dg_refresh(bad)  # the linearisation caches carry the NaN into the blocks
+    with pytest.raises(DGHError, match="Nonfinite block LU input"):
+        s.precond_refresh("dg")
+    s.close()
