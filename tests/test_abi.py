@@ -162,3 +162,19 @@ def test_perturbation_keeps_states_positive():
     p = perturb(u, 3, 2, 2, 0.25)
     assert p.min() >= 0.75 - 1e-12 and p.max() <= 1.25 + 1e-12
     assert not np.allclose(p, 1)
+
+
+def test_reference_executable_names():
+    """The reference's drivers accept only bin/*.exe (scripts/experiment.py:74-79): the front
+    ends are also installed as dg_hdg_2d.exe and dg_hdg.exe (the reference's target names,
+    dg_hdg_2d/CMakeLists.txt:16, dg_hdg_1d/CMakeLists.txt:18 with CMAKE_EXECUTABLE_SUFFIX .exe)."""
+    import subprocess
+
+    from dg_hdg_euler_cpp_b200 import BIN_PATH
+
+    for name, dim in (("dg_hdg_2d.exe", "2D"), ("dg_hdg.exe", "1D")):
+        exe = BIN_PATH.parent / name
+        if not exe.exists():
+            pytest.skip("front ends not built")
+        res = subprocess.run([str(exe), "--help"], capture_output=True, text=True, timeout=60)
+        assert res.returncode == 0 and res.stdout.startswith(dim), (name, res.stdout[:80])
