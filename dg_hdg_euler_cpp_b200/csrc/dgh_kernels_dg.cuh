@@ -455,6 +455,18 @@ __device__ inline double cell_block_entry(int r, int c, const double *jx, const 
     return val;
 }
 
+// Copies the basis tables a kernel indexes per thread into shared memory: indexed reads of a
+// kernel parameter with lane-varying indices serialise in the parameter bank, shared-memory
+// reads do not.  The caller synchronises before the first use.
+template <int N> __device__ inline void stage_basis(const Basis1D &b, Basis1D &sb) {
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) sb.dw[k] = b.dw[k];
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        sb.w[k] = b.w[k];
+        sb.eL[k] = b.eL[k];
+        sb.eR[k] = b.eR[k];
+    }
+}
+
 // DG diagonal blocks written row-major into the factor pool (precision TF).
 template <int N, typename TF>
 __global__ void __launch_bounds__(256)
@@ -462,14 +474,16 @@ k_dg_assemble(TF *__restrict__ pool, const double *__restrict__ vol, const doubl
               const double *__restrict__ speeds, Basis1D b, Grid g, double inv_step, int first, int count) {
     constexpr int P = N * N, M = NVAR * P;
     __shared__ double jx[P * 16], jy[P * 16], fj[NFACES * N * 16];
+    __shared__ Basis1D sb;
+    stage_basis<N>(b, sb);
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         const int cell = first + blk;
         __syncthreads();
-        cell_tables<N, false>(cell, vol, fcache, speeds, b, g, jx, jy, fj);
+        cell_tables<N, false>(cell, vol, fcache, speeds, sb, g, jx, jy, fj);
         __syncthreads();
         TF *A = pool + (size_t)blk * M * M;
         for (int idx = threadIdx.x; idx < M * M; idx += blockDim.x)
-            A[idx] = (TF)cell_block_entry<N>(idx / M, idx % M, jx, jy, fj, b, g, inv_step);
+            A[idx] = (TF)cell_block_entry<N>(idx / M, idx % M, jx, jy, fj, sb, g, inv_step);
     }
 }
 

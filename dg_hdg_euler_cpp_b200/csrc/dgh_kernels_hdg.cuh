@@ -16,14 +16,16 @@ k_hdg_assemble(TF *__restrict__ aug, const double *__restrict__ vol, const doubl
                double inv_step, int first, int count) {
     constexpr int P = N * N, M = NVAR * P, FW = NVAR * N, T = NFACES * FW, LD = M + T + 1;
     __shared__ double jx[P * 16], jy[P * 16], fj[NFACES * N * 16], stab[NFACES * N];
+    __shared__ Basis1D sb;
+    stage_basis<N>(b, sb);
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         const int cell = first + blk;
         __syncthreads();
-        cell_tables<N, true>(cell, vol, fcache, speeds, b, g, jx, jy, fj);
+        cell_tables<N, true>(cell, vol, fcache, speeds, sb, g, jx, jy, fj);
         for (int k = threadIdx.x; k < NFACES * N; k += blockDim.x) {
             const int side = k / N, q = k % N, face = face_of(g, cell, side);
             const double tau = speeds[2 * (face * N + q) + (side % 2 ? 0 : 1)];
-            stab[k] = face_weight(g, b, face, q) * tau;
+            stab[k] = face_weight(g, sb, face, q) * tau;
         }
         __syncthreads();
         TF *A = aug + (size_t)blk * M * LD;
@@ -31,13 +33,13 @@ k_hdg_assemble(TF *__restrict__ aug, const double *__restrict__ vol, const doubl
             const int r = idx / LD, c = idx % LD;
             double val;
             if (c < M) {
-                val = cell_block_entry<N>(r, c, jx, jy, fj, b, g, inv_step);
+                val = cell_block_entry<N>(r, c, jx, jy, fj, sb, g, inv_step);
             } else if (c < M + T) {
                 const int k = c - M, side = k / FW, rem = k % FW, vv = rem / N, q = rem % N;
                 const int v = r / P, node = r % P, ix = node % N, iy = node / N;
                 val = 0;
                 if (v == vv) {
-                    const double *e = side % 2 ? b.eR : b.eL;
+                    const double *e = side % 2 ? sb.eR : sb.eL;
                     if (side < 2 && iy == q) val = -stab[side * N + q] * e[ix];
                     if (side >= 2 && ix == q) val = -stab[side * N + q] * e[iy];
                 }
