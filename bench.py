@@ -150,6 +150,16 @@ def algorithmic_bytes(kind: str, m: int, cells: int, fw: int, faces: int, t: int
     raise ValueError(kind)
 
 
+# DRAM bytes (read + write) of one k_lu_solve<float> launch per 324 x 324 block, from one ncu
+# capture at 64x64 k = 8 (4,096 blocks: 1.810513 GB read, 0.010409 GB written); the traffic of a
+# launch grows with the block count.
+SOLVE_FP32_TRAFFIC_PER_BLOCK_K8 = (1.810513e9 + 0.010409e9) / 4096
+
+
+def solve_traffic(args):
+    return SOLVE_FP32_TRAFFIC_PER_BLOCK_K8 * args.nx * args.nx if args.k == 8 else None
+
+
 def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: bool, rank: int, local: int):
     from dg_hdg_euler_cpp_b200 import _lib
     from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
@@ -434,7 +444,10 @@ def main():
                    "l2": "inputs larger than L2 (factor pool 27-55 GB, Schur pool 10.9 GB)",
                    "value_definition": "(K_dg+K_hdg)/(t_dg+t_hdg) over the mixed-precision DG and HDG solves"},
         "roofline": ({k: dom[k] for k in ("bound", "achieved", "peak", "unit", "frac")} | {
-            "traffic": None, "kernel": dom["kernel"], "peak_source": peak_src,
+            "traffic": solve_traffic(args) if dom["kernel"].startswith("k_lu_solve<float>") else None,
+            "traffic_source": "ncu dram bytes of one launch at 64x64 k=8 "
+            "(profiles/k_lu_solve_fp32_64x64_k8.md) times the block-count ratio",
+            "kernel": dom["kernel"], "peak_source": peak_src,
             "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_launch_ms"]}) if dom else None,
         "gpu_launches": int(sum(results[k]["launches"] for k in head)),
         "breakdown": results,
