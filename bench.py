@@ -56,6 +56,8 @@ def parse():
                    help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
     p.add_argument("--cpu-sample-nx", type=int, default=32)
+    p.add_argument("--cpu-single-nx", type=int, default=16,
+                   help="mesh of the single-thread CPU sample (0 skips it)")
     return p.parse_args()
 
 
@@ -371,13 +373,13 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
             "gmres_cycles": "cuda_graph" if graph else "stepped"}
 
 
-def cpu_baseline(args, threads: int, steps: int, warm: int):
+def cpu_baseline(args, threads: int, steps: int, warm: int, n: int | None = None):
     """The oracle (a restatement of the reference's CPU algorithm) on the host cores: the same
     protocol at a reduced mesh of the same degree, DG and HDG, scaled by the cell-count ratio."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle_py
 
-    n = args.cpu_sample_nx
+    n = n or args.cpu_sample_nx
     scale = (args.nx / n) ** 2
     res = {}
     for method in ("dg", "hdg"):
@@ -394,7 +396,7 @@ def cpu_baseline(args, threads: int, steps: int, warm: int):
     return {"value": 2.0 / total, "unit": "updates/s", "cores": threads, "kind": "port",
             "sample": f"oracle (C++ restatement of the reference, FP64, {threads} threads) on {n}x{n} k={args.k}, "
                       f"same BE CFL5 GMRES(20) protocol, {steps} timed updates per method after {warm + 1} warm-up; "
-                      f"per-update time scaled by the cell ratio {scale:g} to 256^2",
+                      f"per-update time scaled by the cell ratio {scale:g} to {args.nx}^2",
             "per_method": res}
 
 
@@ -468,6 +470,9 @@ def main():
         line["breakdown"]["gmres_graph_vs_stepped"] = graph_comparison(torch, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, os.cpu_count() or 1, 1, 0)
+        if args.cpu_single_nx:  # the reference is single-threaded by construction
+            single = cpu_baseline(args, 1, 1, 0, n=args.cpu_single_nx)
+            line["cpu_baseline"]["single_thread"] = {k: single[k] for k in ("value", "unit", "cores", "sample")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg is not None:
