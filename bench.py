@@ -111,7 +111,10 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------ distributed plumbing
-def dist_setup(gpus: int):
+def dist_setup(gpus: int, backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): the replicas share no
+    data, so the group only carries the barriers around the timed region and the max over
+    ranks of each timing.  backend "gloo" runs the same plumbing on CPU processes."""
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -122,21 +125,24 @@ def dist_setup(gpus: int):
         import torch.distributed as dist
 
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=None)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return rank, local, world, pg
 
 
 def barrier(pg, torch):
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
 
 
 def allmax(pg, torch, value: float) -> float:
+    """The largest value over the ranks (every rank gets it)."""
     if pg is None:
         return value
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 

@@ -1,0 +1,71 @@
+"""The multi-process plumbing of bench.py (one process per GPU, replicas only): two gloo ranks on
+CPU take the same barriers and reduce each timing to the maximum over ranks; the reference arm
+prints from rank 0 only."""
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+WORKER = r"""
+import os, sys, json
+sys.path.insert(0, sys.argv[1])
+import torch
+import bench
+rank, local, world, pg = bench.dist_setup(2, backend="gloo")
+bench.barrier(pg, torch)
+got = bench.allmax(pg, torch, 10.0 + 5.0 * rank)
+bench.barrier(pg, torch)
+print(json.dumps({"rank": rank, "world": world, "max": got}))
+pg.destroy_process_group()
+"""
+
+
+def run_ranks(code, extra_env=None, args=()):
+    port = free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="", **(extra_env or {}))
+        procs.append(subprocess.Popen([sys.executable, "-c", code, str(ROOT), *args], env=env, stdout=subprocess.PIPE,
+                                      stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        out, err = p.communicate(timeout=300)
+        assert p.returncode == 0, err[-2000:]
+        outs.append(out)
+    return outs
+
+
+def test_two_gloo_ranks_take_the_max_over_ranks():
+    import json
+
+    outs = run_ranks(WORKER)
+    rows = [json.loads(o.strip().splitlines()[-1]) for o in outs]
+    assert sorted(r["rank"] for r in rows) == [0, 1]
+    assert all(r["world"] == 2 and r["max"] == 15.0 for r in rows)
+
+
+def test_reference_arm_prints_on_rank_zero_only():
+    code = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+import bench
+sys.argv = ["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--nx", "256",
+            "--cpu-sample-nx", "16", "--k", "8"]
+bench.main()
+"""
+    outs = run_ranks(code)
+    lines = [[l for l in o.splitlines() if l.startswith("{")] for o in outs]
+    assert len(lines[0]) == 1 and lines[1] == []
+    assert '"impl": "reference"' in lines[0][0]
