@@ -117,6 +117,7 @@ struct dgh_ctx {
     int aug_cells = 0;
     void *face_pool = nullptr;
     int *face_perm = nullptr;
+    bool face_inverse = false;  // mixed 2D: face_pool holds FP32 explicit inverses
     // 1D block ILU(0): the periodic block pattern, its symbolic update schedule, the pattern
     // blocks (row-major, slot order) and the diagonal blocks' permutations, per operator
     struct IluPlan {
@@ -446,7 +447,13 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     } else {
         need(c->face_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->fw * c->fw;
-        if (c->mixed()) launch_solve<float>(c, (const float *)c->face_pool, c->face_perm, stride, c->fw, c->faces, x, z);
+        if (c->face_inverse) {
+            constexpr int wpc = INV_APPLY_THREADS / 32;
+            const int grid = std::min((c->faces + wpc - 1) / wpc, c->sms * 8);
+            k_inv_apply<<<grid, INV_APPLY_THREADS, 0, c->stream>>>((const float *)c->face_pool, c->fw, c->faces, x, z);
+            c->launched();
+        } else if (c->mixed())
+            launch_solve<float>(c, (const float *)c->face_pool, c->face_perm, stride, c->fw, c->faces, x, z);
         else launch_solve<double>(c, (const double *)c->face_pool, c->face_perm, stride, c->fw, c->faces, x, z);
     }
 }
@@ -1725,7 +1732,26 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             need(c->condensed, "Condense the HDG operator before refreshing its preconditioner");
             const long long tot = (long long)c->faces * c->fw * c->fw;
             const size_t stride = (size_t)c->fw * c->fw;
-            if (c->mixed()) {
+            c->face_inverse = false;
+            if (c->mixed() && c->fw <= 64 && (size_t)tot <= (size_t)c->aug_cells * c->m * (c->m + c->t + 1)) {
+                // FP64 blocks in the condensation workspace (free until the next condensation),
+                // inverted in FP64 and stored as FP32 inverses
+                DGH_DISPATCH_N(c->n, {
+                    k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, c->aug,
+                                                                                                  c->basis, c->g);
+                });
+                c->launched();
+                const size_t smem = inv_narrow_smem_bytes(c->fw);
+                allow_dynamic_smem((const void *)k_inv_narrow, smem);
+                int resident = 0;
+                ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_inv_narrow, INV_THREADS, smem), "occupancy");
+                constexpr int wpc = INV_THREADS / 32;
+                const int grid = std::min((c->faces + wpc - 1) / wpc, c->sms * std::max(1, resident));
+                k_inv_narrow<<<grid, INV_THREADS, smem, c->stream>>>(c->aug, c->fw, c->faces, (float *)c->face_pool,
+                                                                     c->status, ST_SINGULAR);
+                c->launched();
+                c->face_inverse = true;
+            } else if (c->mixed()) {
                 DGH_DISPATCH_N(c->n, {
                     k_face_blocks<N, float><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (float *)c->face_pool,
                                                                                                  c->basis, c->g);

@@ -453,6 +453,154 @@ k_lu_narrow(T *__restrict__ pool, int m, int count, int *__restrict__ perm_out, 
     }
 }
 
+// Explicit inverses of narrow FP64 blocks (m <= 64, the HDG face blocks in the mixed form), one
+// warp per block in shared memory: k_lu_narrow's pivoted LU (same pivot rule and singularity
+// test), then A^{-1} = U^{-1} L^{-1} P column by column (lane c owns columns c and c + 32), written
+// rounded to FP32 in groups of four columns (element (r, c) at (c / 4) 4m + 4r + c % 4, m a
+// multiple of 4) so that k_inv_apply's lane r reads its row as 16-byte vectors.  Applying an
+// FP32 inverse is a dense product with no dependent triangle steps, which for 36-wide blocks
+// is what bounds the triangular solves.  Shared memory per warp: 2 m (m + 1) doubles.
+constexpr int INV_THREADS = 128;
+inline size_t inv_narrow_smem_bytes(int m) { return (size_t)(INV_THREADS / 32) * 2 * m * (m + 1) * sizeof(double); }
+__global__ void __launch_bounds__(INV_THREADS)
+k_inv_narrow(const double *__restrict__ pool, int m, int count, float *__restrict__ inv_out, int *status,
+             int singular_bit) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, pitch = m + 1;
+    double *S = reinterpret_cast<double *>(smraw) + (size_t)wib * 2 * m * pitch, *X = S + (size_t)m * pitch;
+    const int warps = gridDim.x * (INV_THREADS / 32);
+    for (int blk = blockIdx.x * (INV_THREADS / 32) + wib; blk < count; blk += warps) {
+        const double *A = pool + (size_t)blk * m * m;
+        for (int e = lane; e < m * m; e += 32) S[(e / m) * pitch + e % m] = A[e];
+        int orig0 = lane, orig1 = lane + 32;
+        __syncwarp();
+        for (int j = 0; j < m; ++j) {
+            double best = -1.;
+            int bi = 0x7fffffff;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = lane + 32 * h;
+                if (r >= j && r < m) {
+                    const double a = fabs(S[r * pitch + j]);
+                    if (a > best) { best = a; bi = r; }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            const int p = (bi == 0x7fffffff || !(best == best)) ? j : bi;
+            if (p != j) {
+                for (int c = lane; c < m; c += 32) {
+                    const double t = S[j * pitch + c];
+                    S[j * pitch + c] = S[p * pitch + c];
+                    S[p * pitch + c] = t;
+                }
+                const int oj = __shfl_sync(0xffffffffu, j < 32 ? orig0 : orig1, j & 31);
+                const int op = __shfl_sync(0xffffffffu, p < 32 ? orig0 : orig1, p & 31);
+                if (lane == (j & 31)) { if (j < 32) orig0 = op; else orig1 = op; }
+                if (lane == (p & 31)) { if (p < 32) orig0 = oj; else orig1 = oj; }
+            }
+            __syncwarp();
+            const double pivot = S[j * pitch + j];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = lane + 32 * h;
+                if (r > j && r < m) {
+                    double l = S[r * pitch + j];
+                    if (pivot != 0.) l = l / pivot;
+                    S[r * pitch + j] = l;
+                    for (int c = j + 1; c < m; ++c) S[r * pitch + c] -= l * S[j * pitch + c];
+                }
+            }
+            __syncwarp();
+        }
+        bool bad = false;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = lane + 32 * h;
+            if (r < m) {
+                const double dd = S[r * pitch + r];
+                if (!isfinite(dd) || !(fabs(dd) > 2.2250738585072014e-308)) bad = true;
+            }
+        }
+        if (__any_sync(0xffffffffu, bad)) {
+            if (lane == 0) atomicOr(status, singular_bit);
+            continue;
+        }
+        // column c of A^{-1}: the right-hand side P e_c is the unit vector at the position i
+        // whose original row is c (orig(i) == c); unit-lower forward, then upper backward
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c = lane + 32 * h;
+            int at = -1;
+            for (int i = 0; i < m; ++i) {
+                const int oi = __shfl_sync(0xffffffffu, i < 32 ? orig0 : orig1, i & 31);
+                if (oi == c) at = i;
+            }
+            if (c < m) {
+                for (int i = 0; i < at; ++i) X[i * pitch + c] = 0.;  // above the unit entry
+                for (int i = at; i < m; ++i) {
+                    double v = i == at ? 1. : 0.;
+                    for (int k = at; k < i; ++k) v -= S[i * pitch + k] * X[k * pitch + c];
+                    X[i * pitch + c] = v;
+                }
+                for (int i = m - 1; i >= 0; --i) {
+                    double v = X[i * pitch + c];
+                    for (int k = i + 1; k < m; ++k) v -= S[i * pitch + k] * X[k * pitch + c];
+                    X[i * pitch + c] = v / S[i * pitch + i];
+                }
+            }
+        }
+        __syncwarp();
+        float *out = inv_out + (size_t)blk * m * m;
+        for (int e = lane; e < m * m; e += 32) {
+            const int g = e / (4 * m), r = (e / 4) % m, cc = 4 * g + e % 4;
+            out[e] = (float)X[r * pitch + cc];
+        }
+        __syncwarp();
+    }
+}
+
+// z = A^{-1} b per block with the FP32 inverses of k_inv_narrow: one warp per block, lane r
+// computes rows r and r + 32 (FP32 accumulation) from 16-byte loads of its row, b broadcast by
+// shuffles.  m is a multiple of 4 (m = 4n).
+constexpr int INV_APPLY_THREADS = 256;
+__global__ void __launch_bounds__(INV_APPLY_THREADS)
+k_inv_apply(const float *__restrict__ inv, int m, int count, const double *__restrict__ rhs, double *__restrict__ z) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (INV_APPLY_THREADS / 32);
+    for (int blk = blockIdx.x * (INV_APPLY_THREADS / 32) + (threadIdx.x >> 5); blk < count; blk += warps) {
+        const float4 *A4 = reinterpret_cast<const float4 *>(inv + (size_t)blk * m * m);
+        const double *b = rhs + (size_t)blk * m;
+        const float b0 = lane < m ? (float)b[lane] : 0.f, b1 = lane + 32 < m ? (float)b[lane + 32] : 0.f;
+        float acc0 = 0.f, acc1 = 0.f;
+        const bool r0 = lane < m, r1 = lane + 32 < m;
+        const int groups = m / 4;
+#pragma unroll 3
+        for (int g = 0; g < groups; ++g) {
+            float bj[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int j = 4 * g + e;
+                bj[e] = j < 32 ? __shfl_sync(0xffffffffu, b0, j) : __shfl_sync(0xffffffffu, b1, j - 32);
+            }
+            if (r0) {
+                const float4 a = A4[(size_t)g * m + lane];
+                acc0 += a.x * bj[0] + a.y * bj[1] + a.z * bj[2] + a.w * bj[3];
+            }
+            if (r1) {
+                const float4 a = A4[(size_t)g * m + lane + 32];
+                acc1 += a.x * bj[0] + a.y * bj[1] + a.z * bj[2] + a.w * bj[3];
+            }
+        }
+        if (r0) z[(size_t)blk * m + lane] = (double)acc0;
+        if (r1) z[(size_t)blk * m + lane + 32] = (double)acc1;
+    }
+}
+
 // Block solve z = A^{-1} b with the factors of k_lu (block_jacobi.hpp:24-39): permute, unit
 // lower solve, upper solve.  One warp owns one block and streams its factors exactly once with
 // no CTA-wide barriers; lane i owns row 32 s + i of slab s and reads 16-byte column groups of
