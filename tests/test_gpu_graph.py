@@ -99,3 +99,25 @@ def test_graph_newton_updates_equal_stepped_1d_and_2d():
             for a, b in zip(rows[(False, method)], rows[(True, method)]):
                 for key in ("residual_physical_rms", "krylov_iterations", "linear_relative_residual", "damping"):
                     assert a[key] == b[key], (kw, method, key)
+
+
+def test_graph_newton_updates_equal_stepped_1d_block_ilu0():
+    """With the 1D block ILU(0) preconditioner (single-CTA sweeps inside the replayed cycles)
+    the graph-replayed updates equal the stepped ones bitwise."""
+    from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
+
+    rows = {}
+    for graph in (False, True):
+        s = Solver(dim=1, cells=24, k=3, cfl=5.0, integrator="be", steps=1, newton_steps=3, method="both",
+                   restart=20, precond="block-ilu0")
+        s.gmres_graph(graph)
+        for method in ("dg", "hdg"):
+            it = Integrator(s, method)
+            it.stage_begin(s.initial())
+            rows[(graph, method)] = [it.update() for _ in range(3)]
+            it.close()
+        s.close()
+    for method in ("dg", "hdg"):
+        for a, b in zip(rows[(False, method)], rows[(True, method)]):
+            for key in ("residual_physical_rms", "krylov_iterations", "linear_relative_residual", "damping"):
+                assert a[key] == b[key], (method, key)
