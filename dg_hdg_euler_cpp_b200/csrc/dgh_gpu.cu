@@ -12,6 +12,7 @@
 #include "dgh_kernels_krylov.cuh"
 #include "dgh_kernels_lu.cuh"
 #include "dgh_kernels_lu2.cuh"
+#include "dgh_kernels_q.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -90,6 +91,8 @@ struct dgh_ctx {
     Grid g{};
     Basis1D basis{};
     Basis1D *basis_dev = nullptr;  // device copy, for tables indexed per thread
+    BasisQ *bq = nullptr;          // 2D over-integration: the volume rule (Q > n)
+    double *volq = nullptr;        // (u, v, H) at the volume points [cell][Q*Q][3]
     Case cs{};
     double step_size = 0, inv_step = 0;
     int sms = 148, red_grid = 592;
@@ -195,6 +198,7 @@ struct dgh_ctx {
     void sync() { ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
     bool mixed() const { return cfg.precision == DGH_PRECISION_MIXED; }
     bool d1() const { return dim == 1; }
+    bool overint() const { return dim == 2 && Q > n; }
     bool has_dg() const { return cfg.method == DGH_METHOD_DG || cfg.method == DGH_METHOD_BOTH; }
     bool has_hdg() const { return cfg.method == DGH_METHOD_HDG || cfg.method == DGH_METHOD_BOTH; }
     int team_blocks(int cpb) const { return (cells + cpb - 1) / cpb; }
@@ -295,6 +299,10 @@ void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
         using T = Team<N>;
         if (check) k_face_trace<N, true><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, tr, c->basis, c->g, c->ok);
         else k_face_trace<N, false><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, tr, c->basis, c->g, c->ok);
+        if (check && c->overint()) {  // the over-integrated rule also checks its volume points
+            k_points_check_q<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(u, c->bq, c->g, c->ok);
+            c->launched();
+        }
     });
     c->launched();
 }
@@ -472,12 +480,18 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
     DGH_DISPATCH_N(c->n, {
         using T = Team<N>;
         k_dg_apply<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(v, c->traces2, c->vol, c->fcache, c->speeds,
-                                                                            out, c->basis_dev, c->g, c->inv_step);
+                                                                            out, c->basis_dev, c->g, c->inv_step,
+                                                                            c->overint() ? 0 : 1);
+        if (c->overint()) {
+            k_vol_apply_q<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(v, c->volq, out, c->bq, c->g);
+            c->launched();
+        }
     });
     c->launched();
 }
 void dg_apply_t(dgh_ctx *c, const double *w, double *out) {
     need(!c->d1(), "The adjoint J^T w is built for the 2D operator only");
+    need(!c->overint(), "The adjoint J^T w is built for the collocated volume rule only");
     need(c->linearised, "Refresh the volume Jacobian before applying it");
     launch_trace(c, w, c->traces2, false);
     DGH_DISPATCH_N(c->n, {
@@ -998,7 +1012,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
              "Invalid mesh or degree");
         need(k.quadrature == 0 || k.quadrature >= k.degree + 1, "Quadrature must be >= degree+1");
         if (k.dim == 2)
-            need(k.quadrature == 0 || k.quadrature == k.degree + 1, "Over-integration (--quad > k+1) is not supported");
+            need(k.quadrature <= MAXQ2, "Quadrature above 16 points is not supported on the device (2D)");
         else
             need(k.quadrature <= MAXQ1, "Quadrature above 20 points is not supported on the device");
         need(k.restart > 0 && k.max_linear > 0 && k.max_newton > 0 && k.steps >= 0, "Invalid iteration limit");
@@ -1037,7 +1051,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->t = NFACES * c->fw;
         c->N = (long long)c->cells * c->m;
         c->NT = (long long)c->faces * c->fw;
-        c->Q = c->n;
+        c->Q = k.quadrature ? k.quadrature : c->n;
         c->nspeeds = 2 * (size_t)c->faces * c->n;
         // example.hpp:9-14
         const double pi = std::acos(-1.);
@@ -1097,6 +1111,40 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->ok = c->alloc<int>(1);
         ck(cudaMemset(c->status, 0, sizeof(int)), "memset");
         build_rule(c);
+        if (c->overint()) {
+            // nodal_basis.hpp:37-56: the volume rule's values and weighted derivatives
+            BasisQ h{};
+            h.Q = c->Q;
+            std::vector<double> qx, qw, bary(n, 1.), D(n * n, 0.);
+            gauss_rule(c->Q, qx, qw);
+            const auto &xn = c->xnodes;
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                    if (i != j) bary[i] /= xn[i] - xn[j];
+            for (int i = 0; i < n; ++i) {
+                double sum = 0;
+                for (int j = 0; j < n; ++j)
+                    if (i != j) {
+                        D[i * n + j] = bary[j] / (bary[i] * (xn[i] - xn[j]));
+                        sum += D[i * n + j];
+                    }
+                D[i * n + i] = -sum;
+            }
+            for (int q = 0; q < c->Q; ++q) {
+                const auto v = lagrange(xn, qx[q]);
+                for (int i = 0; i < n; ++i) h.V[q * n + i] = v[i];
+                h.qw[q] = qw[q];
+            }
+            for (int q = 0; q < c->Q; ++q)
+                for (int i = 0; i < n; ++i) {
+                    double sum = 0;
+                    for (int kk = 0; kk < n; ++kk) sum += h.V[q * n + kk] * D[kk * n + i];
+                    h.wd[q * n + i] = qw[q] * sum;
+                }
+            c->bq = c->alloc<BasisQ>(1);
+            ck(cudaMemcpy(c->bq, &h, sizeof(BasisQ), cudaMemcpyHostToDevice), "upload volume rule");
+            c->volq = c->alloc<double>((size_t)c->cells * c->Q * c->Q * 3);
+        }
         c->basis_dev = c->alloc<Basis1D>(1);
         ck(cudaMemcpy(c->basis_dev, &c->basis, sizeof(Basis1D), cudaMemcpyHostToDevice), "upload basis");
         const int tb = 256;
@@ -1311,12 +1359,15 @@ int dgh_freeze(dgh_ctx *c, const double *u, double *rate) {
             const int tot = 2 * c->cells * N;
             k_speeds<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, c->g, c->cfg.safety, c->status);
             using T = Team<N>;
-            k_rate<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->speeds, c->g, c->partial, c->status);
+            if (c->overint())
+                k_rate_q<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(u, c->speeds, c->bq, c->g, c->partial, c->status);
+            else
+                k_rate<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->speeds, c->g, c->partial, c->status);
         });
         c->launched(2);
         c->check_status();
         DGH_DISPATCH_N(c->n, {
-            const int nb = c->team_blocks(Team<N>::CPB);
+            const int nb = c->overint() ? std::min(c->cells, c->sms * 4) : c->team_blocks(Team<N>::CPB);
             std::vector<double> part(nb);
             ck(cudaMemcpyAsync(part.data(), c->partial, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
             c->sync();
@@ -1357,7 +1408,12 @@ int dgh_residual(dgh_ctx *c, const double *u, double *r) {
         DGH_DISPATCH_N(c->n, {
             using T = Team<N>;
             k_residual<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->old, c->traces, c->speeds, r,
-                                                                               c->basis, c->g, 1. / c->step_size);
+                                                                               c->basis, c->g, 1. / c->step_size,
+                                                                               c->overint() ? 0 : 1);
+            if (c->overint()) {
+                k_vol_residual_q<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(u, r, c->bq, c->g);
+                c->launched();
+            }
         });
         c->launched();
     });
@@ -1503,6 +1559,10 @@ void linearise(dgh_ctx *c, const double *u) {
     DGH_DISPATCH_N(c->n, {
         const long long tv = (long long)c->cells * N * N;
         k_volume_cache<N><<<(unsigned)((tv + 255) / 256), 256, 0, c->stream>>>(u, c->vol, c->g);
+        if (c->overint()) {
+            k_volume_cache_q<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(u, c->volq, c->bq, c->g);
+            c->launched();
+        }
         const int tf = 2 * c->cells * N;
         k_face_cache<N><<<(tf + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, c->fcache, c->basis, c->g);
     });
@@ -1534,7 +1594,11 @@ int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
         } else {
             DGH_DISPATCH_N(c->n, {
                 k_dg_assemble<N, double><<<1, 256, 0, c->stream>>>(tmp, c->vol, c->fcache, c->speeds, c->basis, c->g,
-                                                                    c->inv_step, row, 1);
+                                                                    c->inv_step, row, 1, c->overint() ? 0 : 1);
+                if (c->overint()) {
+                    k_vol_block_q<N, double><<<1, Q_THREADS, 0, c->stream>>>(tmp, c->m, c->volq, c->bq, c->g, row, 1);
+                    c->launched();
+                }
             });
         }
         c->launched();
@@ -1563,7 +1627,12 @@ void dg_factor(dgh_ctx *c, int variant, int first, int count) {
                 const int cnt = std::min(c->dg_ws_cells, first + count - f);
                 DGH_DISPATCH_N(c->n, {
                     k_dg_assemble<N, double><<<std::min(cnt, c->sms * 8), 256, 0, c->stream>>>(
-                        c->dg_ws, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step, f, cnt);
+                        c->dg_ws, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step, f, cnt, c->overint() ? 0 : 1);
+                    if (c->overint()) {
+                        k_vol_block_q<N, double><<<std::min(cnt, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                            c->dg_ws, c->m, c->volq, c->bq, c->g, f, cnt);
+                        c->launched();
+                    }
                 });
                 c->launched();
                 launch_lu_left<false>(c, c->dg_ws, stride, c->m, c->m, cnt, c->dg_perm + (size_t)f * c->m, ST_SINGULAR,
@@ -1573,7 +1642,12 @@ void dg_factor(dgh_ctx *c, int variant, int first, int count) {
             float *pool = (float *)c->dg_pool + (size_t)first * stride;
             DGH_DISPATCH_N(c->n, {
                 k_dg_assemble<N, float><<<grid, 256, 0, c->stream>>>(pool, c->vol, c->fcache, c->speeds, c->basis, c->g,
-                                                                     c->inv_step, first, count);
+                                                                     c->inv_step, first, count, c->overint() ? 0 : 1);
+                if (c->overint()) {
+                    k_vol_block_q<N, float><<<std::min(count, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                        pool, c->m, c->volq, c->bq, c->g, first, count);
+                    c->launched();
+                }
             });
             c->launched();
             launch_lu<float>(c, pool, stride, c->m, c->m, count, c->dg_perm + (size_t)first * c->m, ST_SINGULAR, true);
@@ -1582,7 +1656,12 @@ void dg_factor(dgh_ctx *c, int variant, int first, int count) {
         double *pool = (double *)c->dg_pool + (size_t)first * stride;
         DGH_DISPATCH_N(c->n, {
             k_dg_assemble<N, double><<<grid, 256, 0, c->stream>>>(pool, c->vol, c->fcache, c->speeds, c->basis, c->g,
-                                                                  c->inv_step, first, count);
+                                                                  c->inv_step, first, count, c->overint() ? 0 : 1);
+            if (c->overint()) {
+                k_vol_block_q<N, double><<<std::min(count, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                    pool, c->m, c->volq, c->bq, c->g, first, count);
+                c->launched();
+            }
         });
         c->launched();
         if (variant == 0)
@@ -1597,7 +1676,12 @@ void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int
     const int ld = c->m + c->t + 1, grid = std::min(count, c->sms * 8);
     DGH_DISPATCH_N(c->n, {
         k_hdg_assemble<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->vol, c->fcache, c->speeds, r, c->basis, c->g,
-                                                               c->inv_step, first, count);
+                                                               c->inv_step, first, count, c->overint() ? 0 : 1);
+        if (c->overint()) {
+            k_vol_block_q<N, double><<<std::min(count, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                c->aug, ld, c->volq, c->bq, c->g, first, count);
+            c->launched();
+        }
     });
     c->launched();
     if (variant == 0) {

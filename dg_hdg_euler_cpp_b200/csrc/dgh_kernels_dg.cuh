@@ -127,7 +127,8 @@ k_rate(const double *__restrict__ u, const double *__restrict__ speeds, Grid g, 
 template <int N>
 __global__ void __launch_bounds__(Team<N>::THREADS)
 k_residual(const double *__restrict__ u, const double *__restrict__ old, const double *__restrict__ traces,
-           const double *__restrict__ speeds, double *__restrict__ r, Basis1D b, Grid g, double inv_step) {
+           const double *__restrict__ speeds, double *__restrict__ r, Basis1D b, Grid g, double inv_step,
+           int volterm = 1) {
     using T = Team<N>;
     __shared__ double fx[T::CPB][NVAR * T::P], fy[T::CPB][NVAR * T::P];
     __shared__ double ff[T::CPB][NFACES * N * NVAR];
@@ -184,7 +185,7 @@ k_residual(const double *__restrict__ u, const double *__restrict__ old, const d
             wy += fy[sub][v * T::P + ix + N * q] * b.dw[q * N + iy];
         }
         double val = mass * (uu[v] - old[base + v * T::P + lt]) * inv_step;
-        if (N > 1) val -= sx * b.w[iy] * wx + sy * b.w[ix] * wy;
+        if (N > 1 && volterm) val -= sx * b.w[iy] * wx + sy * b.w[ix] * wy;
         val += b.eL[ix] * ff[sub][(0 * N + iy) * NVAR + v] + b.eR[ix] * ff[sub][(1 * N + iy) * NVAR + v] +
                b.eL[iy] * ff[sub][(2 * N + ix) * NVAR + v] + b.eR[iy] * ff[sub][(3 * N + ix) * NVAR + v];
         r[base + v * T::P + lt] = val;
@@ -234,7 +235,7 @@ template <int N>
 __global__ void __launch_bounds__(Team<N>::THREADS, 65536 / (Team<N>::THREADS * 72))
 k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const double *__restrict__ vol,
            const double *__restrict__ fcache, const double *__restrict__ speeds, double *__restrict__ out,
-           const Basis1D *__restrict__ bp, Grid g, double inv_step) {
+           const Basis1D *__restrict__ bp, Grid g, double inv_step, int volterm = 1) {
     // the basis tables are indexed per thread: read them through L1 from a device copy rather
     // than from the kernel's parameter bank, where lane-varying indices serialise
     const Basis1D &b = *bp;
@@ -296,7 +297,7 @@ k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const d
             wy += fy[sub][v * T::P + ix + N * q] * b.dw[q * N + iy];
         }
         double val = mass * dd[v] * inv_step;
-        if (N > 1) val -= sx * b.w[iy] * wx + sy * b.w[ix] * wy;
+        if (N > 1 && volterm) val -= sx * b.w[iy] * wx + sy * b.w[ix] * wy;
         val += b.eL[ix] * ff[sub][(0 * N + iy) * NVAR + v] + b.eR[ix] * ff[sub][(1 * N + iy) * NVAR + v] +
                b.eL[iy] * ff[sub][(2 * N + ix) * NVAR + v] + b.eR[iy] * ff[sub][(3 * N + ix) * NVAR + v];
         out[base + v * T::P + lt] = val;
@@ -437,18 +438,18 @@ __device__ inline void cell_tables(int cell, const double *__restrict__ vol, con
 // row == col, or hybrid.cpp:31-55 for the HDG local matrix) and M/tau on the diagonal.
 template <int N>
 __device__ inline double cell_block_entry(int r, int c, const double *jx, const double *jy, const double *fj,
-                                          const Basis1D &b, const Grid &g, double inv_step) {
+                                          const Basis1D &b, const Grid &g, double inv_step, bool volterm = true) {
     constexpr int P = N * N;
     const int v = r / P, rn = r % P, ix = rn % N, iy = rn / N;
     const int w = c / P, cn = c % P, jx_ = cn % N, jy_ = cn / N;
     double val = 0;
     const int vw = v * 4 + w;
     if (iy == jy_) {
-        if (N > 1) val -= .5 * g.hy * b.w[jy_] * jx[cn * 16 + vw] * b.dw[jx_ * N + ix];
+        if (N > 1 && volterm) val -= .5 * g.hy * b.w[jy_] * jx[cn * 16 + vw] * b.dw[jx_ * N + ix];
         val += b.eL[ix] * b.eL[jx_] * fj[(0 * N + iy) * 16 + vw] + b.eR[ix] * b.eR[jx_] * fj[(1 * N + iy) * 16 + vw];
     }
     if (ix == jx_) {
-        if (N > 1) val += -.5 * g.hx * b.w[jx_] * jy[cn * 16 + vw] * b.dw[jy_ * N + iy];
+        if (N > 1 && volterm) val += -.5 * g.hx * b.w[jx_] * jy[cn * 16 + vw] * b.dw[jy_ * N + iy];
         val += b.eL[iy] * b.eL[jy_] * fj[(2 * N + ix) * 16 + vw] + b.eR[iy] * b.eR[jy_] * fj[(3 * N + ix) * 16 + vw];
     }
     if (r == c) val += .25 * g.hx * g.hy * b.w[ix] * b.w[iy] * inv_step;
@@ -467,11 +468,13 @@ template <int N> __device__ inline void stage_basis(const Basis1D &b, Basis1D &s
     }
 }
 
-// DG diagonal blocks written row-major into the factor pool (precision TF).
+// DG diagonal blocks written row-major into the factor pool (precision TF).  volterm = 0 leaves the
+// volume term out (it is added at the over-integrated points by k_vol_block_q).
 template <int N, typename TF>
 __global__ void __launch_bounds__(256)
 k_dg_assemble(TF *__restrict__ pool, const double *__restrict__ vol, const double *__restrict__ fcache,
-              const double *__restrict__ speeds, Basis1D b, Grid g, double inv_step, int first, int count) {
+              const double *__restrict__ speeds, Basis1D b, Grid g, double inv_step, int first, int count,
+              int volterm = 1) {
     constexpr int P = N * N, M = NVAR * P;
     __shared__ double jx[P * 16], jy[P * 16], fj[NFACES * N * 16];
     __shared__ Basis1D sb;
@@ -483,7 +486,7 @@ k_dg_assemble(TF *__restrict__ pool, const double *__restrict__ vol, const doubl
         __syncthreads();
         TF *A = pool + (size_t)blk * M * M;
         for (int idx = threadIdx.x; idx < M * M; idx += blockDim.x)
-            A[idx] = (TF)cell_block_entry<N>(idx / M, idx % M, jx, jy, fj, sb, g, inv_step);
+            A[idx] = (TF)cell_block_entry<N>(idx / M, idx % M, jx, jy, fj, sb, g, inv_step, volterm != 0);
     }
 }
 

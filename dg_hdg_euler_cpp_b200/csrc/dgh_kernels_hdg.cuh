@@ -13,7 +13,7 @@ template <int N, typename TF>
 __global__ void __launch_bounds__(256)
 k_hdg_assemble(TF *__restrict__ aug, const double *__restrict__ vol, const double *__restrict__ fcache,
                const double *__restrict__ speeds, const double *__restrict__ rvol, Basis1D b, Grid g,
-               double inv_step, int first, int count) {
+               double inv_step, int first, int count, int volterm = 1) {
     constexpr int P = N * N, M = NVAR * P, FW = NVAR * N, T = NFACES * FW, LD = M + T + 1;
     __shared__ double jx[P * 16], jy[P * 16], fj[NFACES * N * 16], stab[NFACES * N];
     __shared__ Basis1D sb;
@@ -33,7 +33,7 @@ k_hdg_assemble(TF *__restrict__ aug, const double *__restrict__ vol, const doubl
             const int r = idx / LD, c = idx % LD;
             double val;
             if (c < M) {
-                val = cell_block_entry<N>(r, c, jx, jy, fj, sb, g, inv_step);
+                val = cell_block_entry<N>(r, c, jx, jy, fj, sb, g, inv_step, volterm != 0);
             } else if (c < M + T) {
                 const int k = c - M, side = k / FW, rem = k % FW, vv = rem / N, q = rem % N;
                 const int v = r / P, node = r % P, ix = node % N, iy = node / N;

@@ -33,9 +33,6 @@ void validate(const Config &c) {
     require(c.testcase == "diagonal" || c.testcase == "wave" || c.testcase == "axis",
             "Invalid testcase");
     require(c.quadrature == 0 || c.quadrature >= c.degree + 1, "Quadrature must be >= degree+1");
-    // The over-integrated volume rule is outside the restated path.
-    require(c.quadrature == 0 || c.quadrature == c.degree + 1,
-            "Over-integration (--quad > k+1) is not part of this restatement");
     require(c.restart > 0 && c.max_linear > 0 && c.max_newton > 0 && c.steps >= 0,
             "Invalid iteration limit");
     require(c.newton_steps >= 0 && c.warmup_updates >= 0, "Invalid timing update count");
@@ -163,7 +160,7 @@ Vec Basis::evaluate(double z) const {
     return v;
 }
 
-Basis::Basis(int degree) : nodes(degree + 1), points(degree + 1) {
+Basis::Basis(int degree, int quadrature) : nodes(degree + 1), points(quadrature ? quadrature : degree + 1) {
     const int n = nodes;
     gauss(n, x, w);
     Vec bary(n, 1.);
@@ -183,6 +180,22 @@ Basis::Basis(int degree) : nodes(degree + 1), points(degree + 1) {
     dw.assign(n * n, 0.);
     for (int q = 0; q < n; ++q)
         for (int i = 0; i < n; ++i) dw[q * n + i] = w[q] * D[q * n + i];
+    // nodal_basis.hpp:37-57: values at the volume points (the identity when collocated) and
+    // weighted_derivatives = diag(qw) * values * D
+    const int P = points;
+    gauss(P, qx, qw);
+    values.assign(P * n, 0.);
+    for (int q = 0; q < P; ++q) {
+        Vec v = evaluate(qx[q]);
+        for (int i = 0; i < n; ++i) values[q * n + i] = P == n ? (q == i ? 1. : 0.) : v[i];
+    }
+    wd.assign(P * n, 0.);
+    for (int q = 0; q < P; ++q)
+        for (int i = 0; i < n; ++i) {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += values[q * n + k] * D[k * n + i];
+            wd[q * n + i] = qw[q] * s;
+        }
     left = evaluate(-1);
     right = evaluate(1);
     gauss(std::max(20, 2 * n + 3), ex, ew);
@@ -304,7 +317,7 @@ State Example::exact(double x, double y, double t) const {
 
 // ---------------------------------------------------------------- discretization.cpp
 Problem::Problem(const Config &c)
-    : config(c), basis(c.degree), nx(c.nx), ny(c.ny), n(basis.nodes), cells(c.nx * c.ny),
+    : config(c), basis(c.degree, c.quadrature), nx(c.nx), ny(c.ny), n(basis.nodes), cells(c.nx * c.ny),
       plane(n * n), block(NVAR * n * n), example(c.testcase), hx(example.lx / c.nx),
       hy(example.ly / c.ny) {
     validate(c);
@@ -324,6 +337,57 @@ Problem::Problem(const Config &c)
     inverse_trace_mass.resize(trace_mass.size());
     for (size_t i = 0; i < trace_mass.size(); ++i) inverse_trace_mass[i] = 1 / trace_mass[i];
     speeds.assign(face_count() * n, Speed{0, 0});
+    Q = basis.points;
+}
+void Problem::interpolate(const double *nodal, double *pts) const {
+    const Vec &V = basis.values;
+    Vec t((size_t)Q * n);
+    for (int v = 0; v < NVAR; ++v) {
+        for (int iy = 0; iy < n; ++iy)  // t(qx, iy) = sum_ix V(qx, ix) U(ix, iy)
+            for (int a = 0; a < Q; ++a) {
+                double s = 0;
+                for (int ix = 0; ix < n; ++ix) s += V[a * n + ix] * nodal[v * plane + ix + n * iy];
+                t[a + Q * iy] = s;
+            }
+        for (int b = 0; b < Q; ++b)  // pts(qx, qy) = sum_iy t(qx, iy) V(qy, iy)
+            for (int a = 0; a < Q; ++a) {
+                double s = 0;
+                for (int iy = 0; iy < n; ++iy) s += t[a + Q * iy] * V[b * n + iy];
+                pts[v * Q * Q + a + Q * b] = s;
+            }
+    }
+}
+void Problem::subtract_weak_points(const double *fx, const double *fy, double *r) const {
+    const double sx = .5 * hy, sy = .5 * hx;
+    const Vec &V = basis.values, &wd = basis.wd, &qw = basis.qw;
+    Vec t((size_t)n * Q);
+    for (int v = 0; v < NVAR; ++v) {
+        const double *x = fx + (size_t)v * Q * Q, *y = fy + (size_t)v * Q * Q;
+        for (int b = 0; b < Q; ++b)  // t(i, qy) = sum_qx wd(qx, i) Fx(qx, qy)
+            for (int i = 0; i < n; ++i) {
+                double s = 0;
+                for (int a = 0; a < Q; ++a) s += wd[a * n + i] * x[a + Q * b];
+                t[i + n * b] = s;
+            }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double s = 0;
+                for (int b = 0; b < Q; ++b) s += t[i + n * b] * qw[b] * V[b * n + j];
+                r[v * plane + i + n * j] -= sx * s;
+            }
+        for (int b = 0; b < Q; ++b)  // t(i, qy) = sum_qx qw(qx) V(qx, i) Fy(qx, qy)
+            for (int i = 0; i < n; ++i) {
+                double s = 0;
+                for (int a = 0; a < Q; ++a) s += qw[a] * V[a * n + i] * y[a + Q * b];
+                t[i + n * b] = s;
+            }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double s = 0;
+                for (int b = 0; b < Q; ++b) s += t[i + n * b] * wd[b * n + j];
+                r[v * plane + i + n * j] -= sy * s;
+            }
+    }
 }
 int Problem::neighbor(int cell, int side) const {
     int x = cell % nx, y = cell / nx;
@@ -374,6 +438,27 @@ void Problem::volume_residual(const Vec &u, Vec &r) const {
     r.resize(size());
     for (int i = 0; i < size(); ++i) r[i] = mass[i] * (u[i] - old[i]) / step_size;
     if (n == 1) return;
+    if (Q != n) {
+#pragma omp parallel
+        {
+            const int QQ = Q * Q;
+            Vec pts((size_t)NVAR * QQ), fx((size_t)NVAR * QQ), fy((size_t)NVAR * QQ);
+#pragma omp for schedule(static)
+            for (int cell = 0; cell < cells; ++cell) {
+                interpolate(u.data() + cell * block, pts.data());
+                for (int q = 0; q < QQ; ++q) {
+                    State s{pts[q], pts[QQ + q], pts[2 * QQ + q], pts[3 * QQ + q]};
+                    State a = example.gas.flux(s, 0), b = example.gas.flux(s, 1);
+                    for (int v = 0; v < NVAR; ++v) {
+                        fx[v * QQ + q] = a[v];
+                        fy[v * QQ + q] = b[v];
+                    }
+                }
+                subtract_weak_points(fx.data(), fy.data(), r.data() + cell * block);
+            }
+        }
+        return;
+    }
 #pragma omp parallel
     {
         Vec fx(block), fy(block);
@@ -476,9 +561,18 @@ double Problem::freeze(const Vec &u) {
                 const Speed s = speeds[fs[side] * n + q];
                 alpha[side / 2] = std::max({alpha[side / 2], s.a, s.b});
             }
+        // discretization.cpp:184-192: the states at the volume points (the nodes when collocated)
+        Vec pts;
         const double *uc = u.data() + cell * block;
-        for (int node = 0; node < plane; ++node) {
-            State s{uc[node], uc[plane + node], uc[2 * plane + node], uc[3 * plane + node]};
+        int npts = plane, stride = plane;
+        if (Q != n) {
+            pts.resize((size_t)NVAR * Q * Q);
+            interpolate(uc, pts.data());
+            uc = pts.data();
+            npts = stride = Q * Q;
+        }
+        for (int node = 0; node < npts; ++node) {
+            State s{uc[node], uc[stride + node], uc[2 * stride + node], uc[3 * stride + node]};
             double ir, vx, vy, p, H;
             example.gas.primitive(s, ir, vx, vy, p, H);
             require(s[Density] > 0 && p > 0, "Invalid CFL volume state");
@@ -528,6 +622,13 @@ bool Problem::admissible(const Vec &u) const {
         for (int node = 0; node < plane; ++node)
             for (int v = 0; v < NVAR; ++v) pts[node * NVAR + v] = uc[v * plane + node];
         if (!physical(pts.data(), plane)) return false;
+        if (Q != n) {  // discretization.cpp:224-227: also at the volume points
+            Vec q((size_t)NVAR * Q * Q), qs((size_t)NVAR * Q * Q);
+            interpolate(uc, q.data());
+            for (int k = 0; k < Q * Q; ++k)
+                for (int v = 0; v < NVAR; ++v) qs[k * NVAR + v] = q[v * Q * Q + k];
+            if (!physical(qs.data(), Q * Q)) return false;
+        }
         for (int side = 0; side < NFACES; ++side) {
             face_values(uc, side, fv.data());
             if (!physical(fv.data(), n)) return false;
@@ -674,7 +775,7 @@ State Problem::error(const Vec &u, double time) const {
 // ---------------------------------------------------------------- volume/face jacobian, DG operator
 DGOperator::DGOperator(const Problem &p) : p_(p) {
     const int nf = p.face_count(), n = p.n;
-    prim_.assign((size_t)p.cells * p.plane * 3, 0.);
+    prim_.assign((size_t)p.cells * p.Q * p.Q * 3, 0.);
     fl_.assign((size_t)nf * n * 3, 0.);
     fr_.assign((size_t)nf * n * 3, 0.);
     tau_l_.assign(nf * n, 0.); tau_r_ = tau_l_; blend_l_ = tau_l_; blend_r_ = tau_l_; penalty_ = tau_l_;
@@ -689,7 +790,20 @@ void DGOperator::refresh(const Vec &u) {
     require(p.step_size > 0, "Set the time step before refreshing the Jacobian");
     inverse_step_ = 1 / p.step_size;
     const int n = p.n, plane = p.plane;
-    if (n > 1)
+    if (n > 1 && p.Q != n) {  // volume_jacobian.cpp:33-38: primitives at the volume points
+        const int QQ = p.Q * p.Q;
+        Vec pts((size_t)NVAR * QQ);
+        for (int cell = 0; cell < p.cells; ++cell) {
+            p.interpolate(u.data() + cell * p.block, pts.data());
+            for (int q = 0; q < QQ; ++q) {
+                State s{pts[q], pts[QQ + q], pts[2 * QQ + q], pts[3 * QQ + q]};
+                double ir, vx, vy, pr, H;
+                p.example.gas.primitive(s, ir, vx, vy, pr, H);
+                double *c = &prim_[((size_t)cell * QQ + q) * 3];
+                c[0] = vx; c[1] = vy; c[2] = H;
+            }
+        }
+    } else if (n > 1)
         for (int cell = 0; cell < p.cells; ++cell)
             for (int node = 0; node < plane; ++node) {
                 const double *uc = u.data() + cell * p.block;
@@ -758,7 +872,20 @@ void DGOperator::apply(const Vec &d, Vec &out) const {
 #pragma omp for schedule(static)
         for (int cell = 0; cell < p.cells; ++cell) {
             double *oc = out.data() + cell * blk;
-            if (n > 1) {
+            if (n > 1 && p.Q != n) {  // volume_jacobian.cpp:64-69: the direction at the points
+                const int QQ = p.Q * p.Q;
+                Vec pd((size_t)NVAR * QQ), px((size_t)NVAR * QQ), py((size_t)NVAR * QQ);
+                p.interpolate(d.data() + cell * blk, pd.data());
+                for (int q = 0; q < QQ; ++q) {
+                    double dd[4] = {pd[q], pd[QQ + q], pd[2 * QQ + q], pd[3 * QQ + q]};
+                    double ax[4], ay[4];
+                    const double *c = &prim_[((size_t)cell * QQ + q) * 3];
+                    normal_action(c, dd, ax, 0);
+                    normal_action(c, dd, ay, 1);
+                    for (int v = 0; v < NVAR; ++v) { px[v * QQ + q] = ax[v]; py[v * QQ + q] = ay[v]; }
+                }
+                p.subtract_weak_points(px.data(), py.data(), oc);
+            } else if (n > 1) {
                 const double *dc = d.data() + cell * blk;
                 for (int node = 0; node < plane; ++node) {
                     double dd[4] = {dc[node], dc[plane + node], dc[2 * plane + node], dc[3 * plane + node]};
@@ -833,7 +960,44 @@ void DGOperator::volume_block(int cell, double *out) const {
     require(ready_, "Refresh the volume Jacobian before assembling a block");
     const int n = p.n, plane = p.plane, m = p.block;
     std::fill(out, out + (size_t)m * m, 0.);
-    if (n > 1) {
+    if (n > 1 && p.Q != n) {
+        // volume_jacobian.cpp:90-116: d r(v, i, j) / d U(w, k, l) summed over the points (a, b):
+        // -(hy/2) wd(a,i) X(v,w) V(a,k) V(b,l) qw(b) V(b,j) - (hx/2) qw(a) V(a,i) Y(v,w) V(a,k) V(b,l) wd(b,j)
+        const int Q = p.Q;
+        const Vec &V = p.basis.values, &wd = p.basis.wd, &qw = p.basis.qw;
+        std::vector<Jac> X((size_t)Q * Q), Y((size_t)Q * Q);
+        for (int q = 0; q < Q * Q; ++q) {
+            const double *c = &prim_[((size_t)cell * Q * Q + q) * 3];
+            X[q] = p.example.gas.cached_jacobian(c[0], c[1], c[2], 0);
+            Y[q] = p.example.gas.cached_jacobian(c[0], c[1], c[2], 1);
+        }
+        Vec lx((size_t)n * n), ly((size_t)n * n);  // [k][i] for one (b, v, w)
+        for (int b = 0; b < Q; ++b)
+            for (int wv = 0; wv < NVAR; ++wv)
+                for (int v = 0; v < NVAR; ++v) {
+                    for (int k = 0; k < n; ++k)
+                        for (int i = 0; i < n; ++i) {
+                            double sxv = 0, syv = 0;
+                            for (int a = 0; a < Q; ++a) {
+                                const int q = a + Q * b;
+                                sxv += wd[a * n + i] * X[q][v * 4 + wv] * V[a * n + k];
+                                syv += qw[a] * V[a * n + i] * Y[q][v * 4 + wv] * V[a * n + k];
+                            }
+                            lx[k * n + i] = -sxv;
+                            ly[k * n + i] = -syv;
+                        }
+                    for (int l = 0; l < n; ++l)
+                        for (int k = 0; k < n; ++k) {
+                            double *column = out + (size_t)p.local(wv, k + n * l) * m;
+                            for (int j = 0; j < n; ++j) {
+                                const double cx = .5 * p.hy * qw[b] * V[b * n + j] * V[b * n + l];
+                                const double cy = .5 * p.hx * wd[b * n + j] * V[b * n + l];
+                                for (int i = 0; i < n; ++i)
+                                    column[v * plane + n * j + i] += cx * lx[k * n + i] + cy * ly[k * n + i];
+                            }
+                        }
+                }
+    } else if (n > 1) {
         const Vec &dw = p.basis.dw, &w = p.basis.w;
         for (int jy = 0; jy < n; ++jy)
             for (int jx = 0; jx < n; ++jx) {
@@ -883,6 +1047,7 @@ void DGOperator::block(int row, int col, double *out) const {
 }
 // J^T w assembled from the five coupling blocks of each block row (dense, small meshes only).
 void DGOperator::apply_transpose(const Vec &wv, Vec &out) const {
+    require(p_.Q == p_.n, "The adjoint is restated for the collocated volume rule only");
     const Problem &p = p_;
     const int m = p.block;
     out.assign(p.size(), 0.);

@@ -43,13 +43,15 @@ struct Config {
 Config parse(int argc, char **argv);  // config.cpp:31-122
 void validate(const Config &c);       // config.cpp:6-22
 
-// nodal_basis.hpp:9-66 (collocated Gauss nodes; the over-integrated rule is not restated).
+// nodal_basis.hpp:9-66: Gauss nodes, and the volume quadrature of `points` >= nodes points.
 struct Basis {
     int nodes = 0, points = 0;
     Vec x, w, left, right;
-    Vec dw;  // weighted derivative, dw[q*n+i] = w_q * l_i'(x_q)
+    Vec dw;  // weighted derivative at the nodes, dw[q*n+i] = w_q * l_i'(x_q)
+    Vec qx, qw;      // volume rule (points)
+    Vec values, wd;  // [q][i]: l_i(qx_q) (identity when points == nodes), qw_q * l_i'(qx_q)
     Vec ex, ew, evalues, projection;  // error rule, values [Q][n], projection [n][Q]
-    explicit Basis(int degree);
+    explicit Basis(int degree, int quadrature = 0);
     Vec evaluate(double z) const;
 };
 void gauss(int n, Vec &x, Vec &w);
@@ -84,6 +86,7 @@ class Problem {
     int nx, ny, n, cells, plane, block;  // block = NVAR*n*n
     Example example;
     double hx, hy, step_size = 0;
+    int Q = 0;  // volume quadrature points per direction (Q > n: over-integrated volume terms)
     Vec old, mass, inverse_mass, trace_mass, inverse_trace_mass;
     std::vector<Speed> speeds;
     explicit Problem(const Config &c);
@@ -112,6 +115,12 @@ class Problem {
     State integral(const Vec &u) const;
     State error(const Vec &u, double time) const;
 
+    // tensor_product.cpp:11-21: nodal cell data (var-major) -> values at the Q x Q points,
+    // pts[v*Q*Q + qx + Q*qy]
+    void interpolate(const double *nodal, double *pts) const;
+    // tensor_product.cpp:57-72 (points != nodes): r -= (hy/2) Wd^T Fx (qw V) + (hx/2) (qw V)^T Fy Wd
+    void subtract_weak_points(const double *fx, const double *fy, double *r) const;
+
   private:
     bool physical(const double *states_qv, int count) const;
     void subtract_weak(const double *fx, const double *fy, double *r) const;
@@ -138,7 +147,7 @@ class DGOperator {
     const Problem &p_;
     double inverse_step_ = 0;
     bool ready_ = false;
-    Vec prim_;                   // [cell][node][3] = u, v, H
+    Vec prim_;                   // [cell][point][3] = u, v, H at the volume points
     Vec fl_, fr_;                // [face][q][3]
     Vec tau_l_, tau_r_, blend_l_, blend_r_, penalty_, weights_;  // [face][q]
     Vec diagonal_;               // trace diagonal D

@@ -68,7 +68,7 @@ def test_invalid_configuration_is_rejected_before_any_device_work(lib):
     ({"dim": 1, "nx": 2}, "Invalid mesh or degree"),
     ({"dim": 1, "degree": 3, "quadrature": 3}, "Quadrature must be >= degree+1"),
     ({"dim": 1, "degree": 3, "quadrature": 21}, "Quadrature above 20 points"),
-    ({"dim": 2, "degree": 3, "quadrature": 6}, "Over-integration (--quad > k+1) is not supported"),
+    ({"dim": 2, "degree": 3, "quadrature": 17}, "Quadrature above 16 points is not supported on the device (2D)"),
 ])
 def test_dimension_and_quadrature_validation(lib, fields, message):
     """dg_hdg_1d/src/config.cpp:6-21 and the device limits, checked before any device work."""

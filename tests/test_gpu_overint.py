@@ -1,0 +1,129 @@
+"""The 2D over-integrated volume rule (--quad Q > k+1) on the device against the oracle's
+restatement (tests/test_oracle_overint.py pins the oracle): residual, CFL rate, admissibility at
+the volume points, J*v, cell blocks, the block-Jacobi solve, the HDG condensation, and whole
+runs.  Tolerances as in tests/test_gpu_parity.py."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(4, 3, 2, 4), (3, 3, 3, 6), (3, 4, 1, 3)]
+
+
+def direction(n, a=.7, b=1.9):
+    i = np.arange(n)
+    return np.sin(a * i) + .2 * np.cos(b * i)
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+def setup(oracle_mod, nx, ny, k, quad, precision="fp64"):
+    from dg_hdg_euler_cpp_b200.solver import Solver
+
+    o = oracle_mod.Oracle(f"--nx {nx} --ny {ny} --k {k} --quad {quad} --cfl 2 --integrator be --steps 1")
+    s = Solver(nx=nx, ny=ny, k=k, quad=quad, cfl=2.0, integrator="be", steps=1, method="both", precision=precision)
+    return o, s
+
+
+@pytest.mark.parametrize("nx,ny,k,quad", CASES)
+def test_residual_rate_jv_blocks_precond(oracle_mod, nx, ny, k, quad):
+    o, s = setup(oracle_mod, nx, ny, k, quad)
+    u = o.initial()
+    ug = s.tensor(u)
+    ro, rg = o.freeze(u), s.freeze(ug)
+    assert abs(ro - rg) <= 1e-14 * ro
+    o.set_stage(u, .01)
+    s.set_stage(ug, .01)
+    up = u + 1e-3 * direction(u.size)
+    assert rel(np_(s.residual(s.tensor(up))), o.residual(up)) <= 1e-12
+    o.dg_refresh(up)
+    s.dg_refresh(s.tensor(up))
+    d = direction(u.size, .31, .79)
+    assert rel(np_(s.dg_apply(s.tensor(d))), o.dg_apply(d)) <= 1e-12
+    for cell in sorted({0, nx * ny // 2, nx * ny - 1}):
+        assert rel(s.dg_block(cell, cell), o.dg_block(cell, cell)) <= 1e-12
+    o.dg_precond_refresh()
+    s.precond_refresh("dg")
+    assert rel(np_(s.precond_apply("dg", s.tensor(d))), o.dg_precond_apply(d)) <= 1e-10
+
+
+@pytest.mark.parametrize("nx,ny,k,quad", CASES[:2])
+def test_hdg_condensation(oracle_mod, nx, ny, k, quad):
+    o, s = setup(oracle_mod, nx, ny, k, quad)
+    u = o.initial()
+    o.freeze(u)
+    s.freeze(s.tensor(u))
+    o.set_stage(u, .01)
+    s.set_stage(s.tensor(u), .01)
+    up = u + 1e-3 * direction(u.size)
+    r = o.residual(up)
+    o.hdg_refresh(up, r)
+    s.hdg_refresh_projected(s.tensor(up), s.tensor(r))
+    assert rel(np_(s.hdg_rhs()), o.hdg_rhs()) <= 1e-11
+    dl = direction(o.trace_size)
+    assert rel(np_(s.hdg_apply(s.tensor(dl))), o.hdg_apply(dl)) <= 1e-11
+    assert rel(np_(s.hdg_recover(s.tensor(dl))), o.hdg_recover(dl)) <= 1e-11
+
+
+def test_admissibility_at_the_volume_points(oracle_mod):
+    """Positive at the nodes and faces, negative between them: only the over-integrated rule
+    rejects it, on the device as in the oracle."""
+    from dg_hdg_euler_cpp_b200.solver import Solver
+
+    o = oracle_mod.Oracle("--nx 3 --ny 3 --k 3 --quad 8")
+    s = Solver(nx=3, ny=3, k=3, quad=8, method="dg")
+    sc = Solver(nx=3, ny=3, k=3, method="dg")
+    u = o.initial()
+    bad = u.copy()
+    plane = 16
+    bad[0:plane] = np.tile([1., 1e-3, 1e-3, 1.], 4)
+    bad[plane:3 * plane] = 0.
+    bad[3 * plane:4 * plane] = 1.
+    assert sc.admissible(sc.tensor(bad))
+    assert not s.admissible(s.tensor(bad)) and not o.admissible(bad)
+    assert s.admissible(s.tensor(u))
+
+
+@pytest.mark.parametrize("method", ["dg", "hdg"])
+def test_advance_matches_oracle(oracle_mod, method):
+    """TimeIntegrator::advance with Q = k + 3 on a 4x4 k = 2 mesh, BE then DIRK3."""
+    from dg_hdg_euler_cpp_b200.solver import Solver
+
+    for integrator in ("be", "ssp-dirk3"):
+        args = f"--nx 4 --ny 4 --k 2 --quad 5 --cfl 2 --integrator {integrator} --T 0.02 --restart 20"
+        o = oracle_mod.Oracle(args)
+        u0 = o.initial()
+        so, st_o, _ = o.advance(method, u0)
+        s = Solver(nx=4, ny=4, k=2, quad=5, cfl=2.0, integrator=integrator, final_time=0.02, restart=20,
+                   method=method)
+        sg, st_g, _ = s.advance(method, u0)
+        assert np.max(np.abs(sg - so)) <= 1e-10 * np.max(np.abs(so)), integrator
+        assert st_g["newton_iterations"] == st_o["newton_iterations"]
+        assert abs(st_g["krylov_iterations"] - st_o["krylov_iterations"]) <= 2 * st_o["newton_iterations"]
+        s.close()
+
+
+def test_mixed_precision_and_adjoint_refusal(oracle_mod):
+    from dg_hdg_euler_cpp_b200.solver import DGHError, Solver
+
+    out = {}
+    for precision in ("fp64", "mixed"):
+        s = Solver(nx=4, ny=4, k=2, quad=5, cfl=2.0, integrator="be", final_time=0.02, restart=20,
+                   method="dg", precision=precision)
+        out[precision] = s.advance("dg", np_(s.initial()))[0]
+        if precision == "fp64":
+            u = s.initial()
+            s.freeze(u)
+            s.set_stage(u, .01)
+            s.dg_refresh(u)
+            with pytest.raises(DGHError, match="collocated volume rule only"):
+                s.dg_apply_T(u)
+        s.close()
+    assert np.max(np.abs(out["mixed"] - out["fp64"])) <= 1e-10 * np.max(np.abs(out["fp64"]))
