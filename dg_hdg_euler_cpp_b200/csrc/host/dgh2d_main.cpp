@@ -212,7 +212,8 @@ int main(int argc, char **argv) {
                 ck(dgh_upload(ctx, dev, solution.data(), N));
                 ck(dgh_l2_error(ctx, dev, st.final_time, err));
             }
-            summary << name << ',' << base.nx << ',' << base.ny << ',' << base.degree << ',' << n << ',' << base.cfl
+            summary << name << ',' << base.nx << ',' << base.ny << ',' << base.degree << ','
+                    << (base.quadrature ? base.quadrature : n) << ',' << base.cfl
                     << ',' << o.integrator << ",gmres,block-jacobi,natural," << base.nonlinear_tolerance << ','
                     << base.linear_tolerance << ',' << base.safety << ',' << base.newton_steps << ','
                     << base.warmup_updates << ',' << st.steps << ',' << st.final_time << ',' << st.newton_iterations

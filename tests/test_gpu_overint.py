@@ -127,3 +127,34 @@ def test_mixed_precision_and_adjoint_refusal(oracle_mod):
                 s.dg_apply_T(u)
         s.close()
     assert np.max(np.abs(out["mixed"] - out["fp64"])) <= 1e-10 * np.max(np.abs(out["fp64"]))
+
+
+def test_cli_quad_summary_and_history(oracle_mod):
+    """dg_hdg_2d --quad 5 on 4x4 k = 2 through the CLI: the summary reports the volume rule's
+    point count, and the run's Newton history and L2 errors follow the oracle's advance."""
+    import subprocess
+    import tempfile
+
+    from conftest import read_csv
+    from dg_hdg_euler_cpp_b200 import BIN_PATH
+
+    args = "--nx 4 --ny 4 --k 2 --quad 5 --cfl 2 --integrator be --T 0.02 --restart 20"
+    with tempfile.TemporaryDirectory() as tmp:
+        res = subprocess.run([str(BIN_PATH), *args.split(), "--method", "both", "--no-save-solution",
+                              "--prefix", f"{tmp}/run"], capture_output=True, text=True, timeout=600)
+        assert res.returncode == 0, res.stderr + res.stdout
+        summ = read_csv(f"{tmp}/run_summary.csv")
+        rows = read_csv(f"{tmp}/run_iterations.csv")
+    o = oracle_mod.Oracle(args)
+    for row in summ:
+        assert row["quad"] == "5"
+        _, st, ups = o.advance(row["method"], o.initial())
+        assert int(row["newton_iterations"]) == st["newton_iterations"]
+        ours = [r for r in rows if r["method"] == row["method"]]
+        assert len(ours) == len(ups)
+        r0 = ups[0][8]  # oracle update rows: column 8 is residual_physical_rms
+        for a, b in zip(ours, ups):
+            ra, rb = float(a["residual_physical_rms"]), b[8]
+            assert abs(ra - rb) <= 1e-10 * max(rb, 1e-10 * r0)
+        assert [int(a["krylov_iterations"]) for a in ours] == [int(b[3]) for b in ups] or \
+            abs(sum(int(a["krylov_iterations"]) for a in ours) - st["krylov_iterations"]) <= 2 * len(ups)
