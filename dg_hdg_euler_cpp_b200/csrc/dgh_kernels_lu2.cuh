@@ -155,6 +155,53 @@ __device__ __forceinline__ void ll_prefetch(const double *__restrict__ A, int ld
     }
 }
 
+// Pitch (doubles) of the 32-row staging area of the final layout passes: >= m and = 2 mod 16,
+// so that lanes reading 16 bytes of consecutive rows hit distinct banks.  32 * pitch doubles fit
+// the panel area of mp * LL_AP for every m = 4 n^2 the kernel accepts (n <= 11).
+__device__ __forceinline__ int ll_stage_pitch(int m) { return m + (18 - m % 16) % 16; }
+
+// dst[0..m) = src[0..m) by one warp: 16-byte loads, up to four in flight per lane (m even and
+// both rows 16-byte aligned: every row starts at a multiple of 8 m bytes, m = 4 n^2).
+__device__ __forceinline__ void ll_stage_row(double *dst, const double *src, int m) {
+    const int lane = threadIdx.x & 31, h = m / 2;
+    const double2 *s2 = reinterpret_cast<const double2 *>(src);
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+    for (int c0 = lane; c0 < h; c0 += 4 * 32) {
+        double2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 32 * u;
+            if (c < h) v[u] = s2[c];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 32 * u;
+            if (c < h) d2[c] = v[u];
+        }
+    }
+}
+
+// Warp-wide pivot choice over the lanes' candidates (v, position, slot): the largest v wins,
+// then the smallest position (v = |a|, -1 for a NaN entry, -2 for no candidate).  v maps to an
+// order-preserving 64-bit key (non-negative doubles order as their bit patterns; -0 is folded
+// to +0, which compares equal to it), reduced as two 32-bit halves with redux.sync; the winner's
+// own (v, position, slot) are then broadcast, so every lane ends with the value the pairwise
+// comparison would have kept.
+__device__ __forceinline__ void ll_warp_argmax(double &bv, int &bp, int &bs) {
+    const unsigned long long key = bv == -2. ? 0ull
+                                   : bv == -1. ? 1ull
+                                               : (unsigned long long)__double_as_longlong(fabs(bv)) + 2ull;
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    const bool top = hi == mh && lo == ml;
+    const unsigned mpos = __reduce_min_sync(0xffffffffu, top ? (unsigned)bp : 0xffffffffu);
+    const int src = __ffs(__ballot_sync(0xffffffffu, top && (unsigned)bp == mpos)) - 1;
+    bv = __shfl_sync(0xffffffffu, bv, src);
+    bp = __shfl_sync(0xffffffffu, bp, src);
+    bs = __shfl_sync(0xffffffffu, bs, src);
+}
+
 // Batched LU.  AUG = false: pool holds m x m blocks (ld = m); on exit row i of each block is
 // position i of the factors (unit L below, U on and above the diagonal), perm_out[i] = its
 // original row, and with slab_out the block is rewritten in the slab layout of k_lu_solve.
@@ -248,12 +295,7 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                     };
                     consider(s0, pos0);
                     consider(s1, pos1);
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                        const int op = __shfl_xor_sync(0xffffffffu, bp, o), os = __shfl_xor_sync(0xffffffffu, bs, o);
-                        if (ov > bv || (ov == bv && op < bp)) { bv = ov; bp = op; bs = os; }
-                    }
+                    ll_warp_argmax(bv, bp, bs);
                     if (lane == 0) {
                         cand_v[jj & 1][warp] = bv;
                         cand_p[jj & 1][warp] = bp;
@@ -286,25 +328,39 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                     const double pv = prow[jj], rpv = pv != 0. ? 1. / pv : 1.;
                     const int cme = b0 + g4;  // this lane's column inside the sub-panel
                     const double pcm = prow[cme];
-                    // elimination inside the sub-panel, 8 rows at a time: lane = (row r8, column b0+g4)
+                    // elimination inside the sub-panel, 8 rows at a time: lane = (row r8, column b0+g4).
+                    // Group grp of batch t holds the slots of lanes 8 grp .. 8 grp + 7 (s0 for t = 0,
+                    // s1 for t = 1), so the rows still below the pivot are bits of two ballots.  All
+                    // multipliers are read first, then the sub-panel columns updated, then the
+                    // multipliers stored over column jj once every lane has read it.
+                    const unsigned own0 = __ballot_sync(0xffffffffu, s0 < m && pos0 > tp);
+                    const unsigned own1 = __ballot_sync(0xffffffffu, s1 < m && pos1 > tp);
+                    double lv[2][4];
 #pragma unroll
-                    for (int t = 0; t < 2; ++t) {
-                        const int sb = k0 + 8 * warp + t * LL_THREADS;  // this batch's first slot
-                        if (sb >= m) break;
-                        const bool own = (t ? s1 : s0) < m && (t ? pos1 : pos0) > tp;
+                    for (int t = 0; t < 2; ++t)
 #pragma unroll
                         for (int grp = 0; grp < 4; ++grp) {
-                            const bool act = __shfl_sync(0xffffffffu, own, 8 * grp + r8);
-                            double *row = acc + min(sb + 64 * grp + r8, mp - 1) * LL_AP;  // used only if act
-                            double l = 0.;
-                            if (act) {
-                                l = row[jj] * rpv;
-                                if (cme > jj) row[cme] -= l * pcm;
-                            }
-                            __syncwarp();
-                            if (act && g4 == 0) row[jj] = l;
+                            const bool act = ((t ? own1 : own0) >> (8 * grp + r8)) & 1u;
+                            const double *row = acc + min(k0 + 8 * warp + t * LL_THREADS + 64 * grp + r8, mp - 1) * LL_AP;
+                            lv[t][grp] = act ? row[jj] * rpv : 0.;
                         }
-                    }
+#pragma unroll
+                    for (int t = 0; t < 2; ++t)
+#pragma unroll
+                        for (int grp = 0; grp < 4; ++grp) {
+                            const bool act = ((t ? own1 : own0) >> (8 * grp + r8)) & 1u;
+                            double *row = acc + min(k0 + 8 * warp + t * LL_THREADS + 64 * grp + r8, mp - 1) * LL_AP;
+                            if (act && cme > jj) row[cme] -= lv[t][grp] * pcm;
+                        }
+                    __syncwarp();
+#pragma unroll
+                    for (int t = 0; t < 2; ++t)
+#pragma unroll
+                        for (int grp = 0; grp < 4; ++grp) {
+                            const bool act = ((t ? own1 : own0) >> (8 * grp + r8)) & 1u;
+                            double *row = acc + min(k0 + 8 * warp + t * LL_THREADS + 64 * grp + r8, mp - 1) * LL_AP;
+                            if (act && g4 == 0) row[jj] = lv[t][grp];
+                        }
                     __syncwarp();
                 }
                 // rank-4 update of columns b0+4..nb-1 for this warp's unpivoted rows
@@ -321,15 +377,16 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                             bfr[nt] = g4 == 0 ? uu[0] : g4 == 1 ? uu[1] : g4 == 2 ? uu[2] : uu[3];
                         }
                     }
+                    const unsigned own0 = __ballot_sync(0xffffffffu, s0 < m && pos0 > tp);
+                    const unsigned own1 = __ballot_sync(0xffffffffu, s1 < m && pos1 > tp);
 #pragma unroll
                     for (int t = 0; t < 2; ++t) {
                         const int sb = k0 + 8 * warp + t * LL_THREADS;
-                        if (sb >= m) break;
-                        const bool own = (t ? s1 : s0) < m && (t ? pos1 : pos0) > tp;
 #pragma unroll
                         for (int grp = 0; grp < 4; ++grp) {
-                            const bool act = __shfl_sync(0xffffffffu, own, 8 * grp + r8);
-                            if (!__any_sync(0xffffffffu, act)) continue;
+                            const unsigned gbits = ((t ? own1 : own0) >> (8 * grp)) & 0xffu;
+                            if (!gbits) continue;  // warp-uniform: no row of the group below the pivots
+                            const bool act = (gbits >> r8) & 1u;
                             double *row = acc + min(sb + 64 * grp + r8, mp - 1) * LL_AP;  // used only if act
                             const double a = act ? -row[b0 + g4] : 0.;
 #pragma unroll
@@ -455,16 +512,23 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
             }
         } else if (out32) {
             // ---- FP32 slabs straight from the original-row storage: stage 32 position rows
+            // (16-byte loads, several in flight per thread), then each lane converts one row's
+            // 4 columns of a slab group into one float4
             constexpr int W = SlabVec<float>::W;
-            double *stage = acc;  // 32 rows x m doubles fit: 32 * m <= mp * LL_AP
+            const int sp = ll_stage_pitch(m);
+            double *stage = acc;
+            float4 *out = reinterpret_cast<float4 *>(out32 + (size_t)blk * m * m);
             for (int r0 = 0; r0 < m; r0 += 32) {
                 const int nt = min(32, m - r0);
-                for (int idx = tid; idx < nt * m; idx += LL_THREADS)
-                    stage[idx] = A[(size_t)piv[r0 + idx / m] * ld + idx % m];
+                for (int rr = warp; rr < nt; rr += NW) ll_stage_row(stage + (size_t)rr * sp, A + (size_t)piv[r0 + rr] * ld, m);
                 __syncthreads();
-                float *reg = out32 + (size_t)blk * m * m + (size_t)r0 * m;
+                float4 *reg = out + (size_t)r0 * m / W;
                 for (int g = warp; g < m / W; g += NW)
-                    for (int e = lane; e < nt * W; e += 32) reg[(size_t)g * nt * W + e] = (float)stage[(e / W) * m + g * W + e % W];
+                    for (int rr = lane; rr < nt; rr += 32) {
+                        const double2 a = *reinterpret_cast<const double2 *>(stage + (size_t)rr * sp + g * W);
+                        const double2 b = *reinterpret_cast<const double2 *>(stage + (size_t)rr * sp + g * W + 2);
+                        reg[(size_t)g * nt + rr] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+                    }
                 __syncthreads();
             }
             for (int i = tid; i < m; i += LL_THREADS) perm_out[(size_t)blk * m + i] = piv[i];
@@ -472,10 +536,7 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
             // ---- gather the rows into position order, 32 columns at a time
             for (int c0 = 0; c0 < m; c0 += LL_NB) {
                 const int w = min(LL_NB, m - c0);
-                for (int idx = tid; idx < m * LL_NB; idx += LL_THREADS) {
-                    const int i = idx / LL_NB, cc = idx % LL_NB;
-                    if (cc < w) acc[i * LL_AP + cc] = A[(size_t)piv[i] * ld + c0 + cc];
-                }
+                ll_load_cols(acc, A, ld, piv, m, mp, c0, w);
                 __syncthreads();
                 for (int idx = tid; idx < m * LL_NB; idx += LL_THREADS) {
                     const int i = idx / LL_NB, cc = idx % LL_NB;
@@ -486,14 +547,17 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
             for (int i = tid; i < m; i += LL_THREADS) perm_out[(size_t)blk * m + i] = piv[i];
             if (slab_out) {  // in-place conversion to the slab layout read by k_lu_solve
                 constexpr int W = SlabVec<double>::W;
-                double *stage = acc;  // 32 rows x m doubles fit: 32 * m <= mp * LL_AP
+                const int sp = ll_stage_pitch(m);
+                double *stage = acc;
                 for (int r0 = 0; r0 < m; r0 += 32) {
                     const int nt = min(32, m - r0);
                     double *reg = A + (size_t)r0 * m;
-                    for (int idx = tid; idx < nt * m; idx += LL_THREADS) stage[idx] = reg[idx];
+                    for (int rr = warp; rr < nt; rr += NW) ll_stage_row(stage + (size_t)rr * sp, reg + (size_t)rr * m, m);
                     __syncthreads();
+                    double2 *reg2 = reinterpret_cast<double2 *>(reg);
                     for (int g = warp; g < m / W; g += NW)
-                        for (int e = lane; e < nt * W; e += 32) reg[(size_t)g * nt * W + e] = stage[(e / W) * m + g * W + e % W];
+                        for (int rr = lane; rr < nt; rr += 32)
+                            reg2[(size_t)g * nt + rr] = *reinterpret_cast<const double2 *>(stage + (size_t)rr * sp + g * W);
                     __syncthreads();
                 }
             }

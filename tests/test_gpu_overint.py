@@ -131,11 +131,11 @@ def test_mixed_precision_and_adjoint_refusal(oracle_mod):
 
 def test_cli_quad_summary_and_history(oracle_mod):
     """dg_hdg_2d --quad 5 on 4x4 k = 2 through the CLI: the summary reports the volume rule's
-    point count, and the run's Newton history and L2 errors follow the oracle's advance."""
+    point count, and the Newton history of each method follows the oracle's advance."""
     import subprocess
     import tempfile
 
-    from conftest import read_csv
+    from conftest import assert_history_close, read_csv
     from dg_hdg_euler_cpp_b200 import BIN_PATH
 
     args = "--nx 4 --ny 4 --k 2 --quad 5 --cfl 2 --integrator be --T 0.02 --restart 20"
@@ -151,10 +151,8 @@ def test_cli_quad_summary_and_history(oracle_mod):
         _, st, ups = o.advance(row["method"], o.initial())
         assert int(row["newton_iterations"]) == st["newton_iterations"]
         ours = [r for r in rows if r["method"] == row["method"]]
-        assert len(ours) == len(ups)
-        r0 = ups[0][8]  # oracle update rows: column 8 is residual_physical_rms
-        for a, b in zip(ours, ups):
-            ra, rb = float(a["residual_physical_rms"]), b[8]
-            assert abs(ra - rb) <= 1e-10 * max(rb, 1e-10 * r0)
-        assert [int(a["krylov_iterations"]) for a in ours] == [int(b[3]) for b in ups] or \
-            abs(sum(int(a["krylov_iterations"]) for a in ours) - st["krylov_iterations"]) <= 2 * len(ups)
+        # oracle update rows: step, stage, iteration, krylov, time, stage_time, dt, cfl, rms, ...
+        ref = [dict(method=row["method"], step=str(int(u[0])), stage=str(int(u[1])), iteration=str(int(u[2])),
+                    krylov_iterations=int(u[3]), time=u[4], stage_time=u[5], dt=u[6], cfl=u[7],
+                    residual_physical_rms=u[8]) for u in ups]
+        assert_history_close(ours, ref, krylov_slack=2)
