@@ -147,13 +147,19 @@ def build(verbose: bool = False) -> None:
         raise RuntimeError("building libdgh_gpu.so failed")
 
 
-def load() -> ctypes.CDLL:
-    """Load the CUDA library; raises when it has not been built (no fallback path exists)."""
+def load(path: Path | None = None) -> ctypes.CDLL:
+    """Load the CUDA library; raises when it has not been built (no fallback path exists).
+
+    `path` selects another build of the same C ABI (the cycle-counter build lib/libdgh_gpu_probe.so
+    of lu_probe.py) for the process; it must come before the first load."""
     global _lib
+    if path is not None and _lib is not None and _lib._name != str(path):
+        raise RuntimeError(f"{_lib._name} is already loaded in this process")
     if _lib is None:
-        if not LIB_PATH.exists():
-            raise RuntimeError(f"{LIB_PATH} is missing: build it with dg_hdg_euler_cpp_b200.build()")
-        lib = ctypes.CDLL(str(LIB_PATH))
+        path = Path(path) if path is not None else LIB_PATH
+        if not path.exists():
+            raise RuntimeError(f"{path} is missing: build it with dg_hdg_euler_cpp_b200.build()")
+        lib = ctypes.CDLL(str(path))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.restype = res

@@ -24,9 +24,14 @@
 #pragma once
 #include "dgh_kernels_lu.cuh"
 
-// Optional per-phase cycle counters for offline tuning harnesses; empty in the library build.
+// Optional per-phase cycle counters (lu_probe.h, `make probe`); empty in the library build.
+// Phases: 0 panel load, 1 chunk triangle, 2 chunk GEMM, 3 pivot search (to the chosen pivot,
+// barrier included), 7 elimination, 6 rank-4 update, 4 write-back and triangle inverses,
+// 5 right-hand sides or final layout.
 #ifndef LL_PROBE
 #define LL_PROBE(phase)
+#define LL_PROBE_DECL
+#define LL_PROBE_FLUSH
 #endif
 
 namespace dgh {
@@ -227,6 +232,7 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = LL_THREADS / 32;
     double *tri = tri_all + (size_t)blockIdx.x * P * LL_TRI;
+    LL_PROBE_DECL
 
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         double *A = pool + (size_t)blk * stride;
@@ -283,6 +289,7 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 int psl[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
+                    LL_PROBE(3);
                     const int jj = b0 + u, tp = k0 + jj;
                     double bv = -2.;
                     int bp = 0x7fffffff, bs = -1;
@@ -312,6 +319,7 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                         if (ov > bv || (ov == bv && op < bp)) { bv = ov; bp = op; bs = cand_s[jj & 1][w]; }
                     }
                     psl[u] = bs;
+                    LL_PROBE(7);
                     // swap positions tp and bp (the slot at tp moves to bp)
                     if (s0 < m) { if (s0 == bs) pos0 = tp; else if (pos0 == tp) pos0 = bp; }
                     if (s1 < m) { if (s1 == bs) pos1 = tp; else if (pos1 == tp) pos1 = bp; }
@@ -363,6 +371,7 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                         }
                     __syncwarp();
                 }
+                LL_PROBE(6);
                 // rank-4 update of columns b0+4..nb-1 for this warp's unpivoted rows
                 if (b0 + 4 < nb) {
                     const int tp = k0 + b0 + 3;
@@ -562,10 +571,12 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 }
             }
         }
-        LL_PROBE(6);
+        LL_PROBE(5);
         if (tid == 0 && bad) atomicOr(status, singular_bit);
         __syncthreads();
     }
+    LL_PROBE(5);
+    LL_PROBE_FLUSH;
 }
 
 }  // namespace dgh

@@ -178,3 +178,19 @@ def test_reference_executable_names():
             pytest.skip("front ends not built")
         res = subprocess.run([str(exe), "--help"], capture_output=True, text=True, timeout=60)
         assert res.returncode == 0 and res.stdout.startswith(dim), (name, res.stdout[:80])
+
+
+def test_probe_build_is_opt_in_and_exclusive(lib):
+    """The cycle-counter build (make probe) exports the same C ABI plus its counter table, and a
+    process keeps the library it loaded first."""
+    from dg_hdg_euler_cpp_b200 import _lib
+    from dg_hdg_euler_cpp_b200.lu_probe import PHASES, PROBE_LIB
+
+    assert sorted(PHASES) == list(range(8))
+    with pytest.raises(RuntimeError, match="already loaded"):
+        _lib.load(PROBE_LIB)
+    assert _lib.load(_lib.LIB_PATH) is lib
+    if PROBE_LIB.exists():
+        probe = ctypes.CDLL(str(PROBE_LIB))
+        for name in list(_lib.SIGNATURES) + ["ll_probe_reset", "ll_probe_read"]:
+            assert hasattr(probe, name), name
