@@ -491,14 +491,18 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
 }
 void dg_apply_t(dgh_ctx *c, const double *w, double *out) {
     need(!c->d1(), "The adjoint J^T w is built for the 2D operator only");
-    need(!c->overint(), "The adjoint J^T w is built for the collocated volume rule only");
     need(c->linearised, "Refresh the volume Jacobian before applying it");
     launch_trace(c, w, c->traces2, false);
     DGH_DISPATCH_N(c->n, {
         using T = Team<N>;
         k_dg_apply_t<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(w, c->traces2, c->vol, c->fcache,
                                                                               c->speeds, out, c->basis, c->g,
-                                                                              c->inv_step);
+                                                                              c->inv_step, c->overint() ? 0 : 1);
+        if (c->overint()) {
+            k_vol_apply_q_t<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(w, c->volq, out, c->bq,
+                                                                                            c->g);
+            c->launched();
+        }
     });
     c->launched();
 }

@@ -309,12 +309,13 @@ k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const d
 // (J^T w)(a, b) = M w / tau - (hy/2) w_b Ax^T gx - (hx/2) w_a Ay^T gy.  Faces: with the jump
 // z = E_right-side w_L - E_left-side w_R of the two cells sharing a face, the left cell receives
 // lift((blend_l A_L + pen I)^T z) and the right cell lift((blend_r A_R - pen I)^T z).
-// Needs the face traces of w (k_face_trace on w).
+// Needs the face traces of w (k_face_trace on w).  volterm = 0 leaves out the collocated volume
+// term (the over-integrated rule adds its own, k_vol_apply_q_t).
 template <int N>
 __global__ void __launch_bounds__(Team<N>::THREADS)
 k_dg_apply_t(const double *__restrict__ w, const double *__restrict__ wtr, const double *__restrict__ vol,
              const double *__restrict__ fcache, const double *__restrict__ speeds, double *__restrict__ out,
-             Basis1D b, Grid g, double inv_step) {
+             Basis1D b, Grid g, double inv_step, int volterm = 1) {
     using T = Team<N>;
     __shared__ double ws[T::CPB][NVAR * T::P];
     __shared__ double ff[T::CPB][NFACES * N * NVAR];
@@ -379,7 +380,7 @@ k_dg_apply_t(const double *__restrict__ w, const double *__restrict__ wtr, const
             ty += ay[v * 4 + ww] * gy[v];
         }
         double val = mass * ws[sub][ww * T::P + lt] * inv_step;
-        if (N > 1) val -= sx * b.w[iy] * tx + sy * b.w[ix] * ty;
+        if (N > 1 && volterm) val -= sx * b.w[iy] * tx + sy * b.w[ix] * ty;
         val += b.eL[ix] * ff[sub][(0 * N + iy) * NVAR + ww] + b.eR[ix] * ff[sub][(1 * N + iy) * NVAR + ww] +
                b.eL[iy] * ff[sub][(2 * N + ix) * NVAR + ww] + b.eR[iy] * ff[sub][(3 * N + ix) * NVAR + ww];
         out[base + ww * T::P + lt] = val;

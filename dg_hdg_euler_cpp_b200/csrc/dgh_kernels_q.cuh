@@ -170,6 +170,85 @@ k_vol_apply_q(const double *__restrict__ d, const double *__restrict__ volq, dou
     }
 }
 
+// out -= the transpose of the over-integrated volume term of k_vol_apply_q, for the adjoint
+// J^T w.  With Kx(a,b; i,j) = (hy/2) wd[a][i] qw[b] V[b][j] and Ky(a,b; i,j) = (hx/2) qw[a] V[a][i]
+// wd[b][j] the forward term is sum_ab Kx Ax(a,b) I(d)(a,b) + Ky Ay(a,b) I(d)(a,b), I the
+// interpolation to the points; its transpose takes the point values gx = Kx^T w, gy = Ky^T w,
+// applies Ax^T gx + Ay^T gy at every point (cached_jacobian from (u, v, H) at the point) and
+// returns them to the nodes with I^T.
+template <int N>
+__global__ void __launch_bounds__(Q_THREADS)
+k_vol_apply_q_t(const double *__restrict__ w, const double *__restrict__ volq, double *__restrict__ out,
+                const BasisQ *__restrict__ bqp, Grid g) {
+    __shared__ QScratch<N> sc;
+    __shared__ BasisQ bq;
+    for (int k = threadIdx.x; k < (int)(sizeof(BasisQ) / sizeof(double)); k += blockDim.x)
+        reinterpret_cast<double *>(&bq)[k] = reinterpret_cast<const double *>(bqp)[k];
+    const int Q = bq.Q, QQ = Q * Q;
+    const double sx = .5 * g.hy, sy = .5 * g.hx;
+    for (int cell = blockIdx.x; cell < g.cells; cell += gridDim.x) {
+        __syncthreads();
+        q_load<N>(w + (size_t)cell * NVAR * N * N, sc.nodal);
+        // hx1[v][a][j] = sum_i wd[a][i] w(i, j) (in half), hy1[v][a][j] = sum_i V[a][i] w(i, j) (in pts)
+        for (int e = threadIdx.x; e < NVAR * Q * N; e += blockDim.x) {
+            const int v = e / (Q * N), rem = e % (Q * N), a = rem % Q, j = rem / Q;
+            double s1 = 0, s2 = 0;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const double wv = sc.nodal[v * N * N + i + N * j];
+                s1 += bq.wd[a * N + i] * wv;
+                s2 += bq.V[a * N + i] * wv;
+            }
+            sc.half[v * Q * N + a + Q * j] = s1;
+            sc.pts[v * Q * N + a + Q * j] = s2;
+        }
+        __syncthreads();
+        // gx[v][a + Q b] = sx qw[b] sum_j V[b][j] hx1, gy[v][a + Q b] = sy qw[a] sum_j wd[b][j] hy1
+        for (int e = threadIdx.x; e < NVAR * QQ; e += blockDim.x) {
+            const int v = e / QQ, q = e % QQ, a = q % Q, b = q / Q;
+            double s1 = 0, s2 = 0;
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                s1 += bq.V[b * N + j] * sc.half[v * Q * N + a + Q * j];
+                s2 += bq.wd[b * N + j] * sc.pts[v * Q * N + a + Q * j];
+            }
+            sc.fx[v * QQ + q] = sx * bq.qw[b] * s1;
+            sc.fy[v * QQ + q] = sy * bq.qw[a] * s2;
+        }
+        __syncthreads();
+        // t(a, b) = Ax^T gx + Ay^T gy at every point (in pts)
+        for (int q = threadIdx.x; q < QQ; q += blockDim.x) {
+            const double *c = volq + ((size_t)cell * QQ + q) * 3;
+            double ax[16], ay[16];
+            cached_jacobian(g.gamma, c[0], c[1], c[2], 0, ax);
+            cached_jacobian(g.gamma, c[0], c[1], c[2], 1, ay);
+#pragma unroll
+            for (int ww = 0; ww < NVAR; ++ww) {
+                double t = 0;
+#pragma unroll
+                for (int v = 0; v < NVAR; ++v) t += ax[v * 4 + ww] * sc.fx[v * QQ + q] + ay[v * 4 + ww] * sc.fy[v * QQ + q];
+                sc.pts[ww * QQ + q] = t;
+            }
+        }
+        __syncthreads();
+        // I^T: s1[w][k][b] = sum_a V[a][k] t(a, b) (in half), out(k, l) -= sum_b V[b][l] s1
+        for (int e = threadIdx.x; e < NVAR * N * Q; e += blockDim.x) {
+            const int v = e / (N * Q), rem = e % (N * Q), k = rem % N, b = rem / N;
+            double s = 0;
+            for (int a = 0; a < Q; ++a) s += bq.V[a * N + k] * sc.pts[v * QQ + a + Q * b];
+            sc.half[v * N * Q + k + N * b] = s;
+        }
+        __syncthreads();
+        double *o = out + (size_t)cell * NVAR * N * N;
+        for (int e = threadIdx.x; e < NVAR * N * N; e += blockDim.x) {
+            const int v = e / (N * N), rem = e % (N * N), k = rem % N, l = rem / N;
+            double s = 0;
+            for (int b = 0; b < Q; ++b) s += bq.V[b * N + l] * sc.half[v * N * Q + k + N * b];
+            o[e] -= s;
+        }
+    }
+}
+
 // A[row * ld + col] += the over-integrated volume block (volume_jacobian.cpp:90-116) for cells
 // first..first+count-1 (A chunk-relative): for each flux/state pair (v, w),
 //   LX_b(k, i) = -sum_a wd[a][i] X_ab(v,w) V[a][k],  LY_b(k, i) = -sum_a qw[a] V[a][i] Y_ab(v,w) V[a][k],

@@ -1047,7 +1047,6 @@ void DGOperator::block(int row, int col, double *out) const {
 }
 // J^T w assembled from the five coupling blocks of each block row (dense, small meshes only).
 void DGOperator::apply_transpose(const Vec &wv, Vec &out) const {
-    require(p_.Q == p_.n, "The adjoint is restated for the collocated volume rule only");
     const Problem &p = p_;
     const int m = p.block;
     out.assign(p.size(), 0.);

@@ -110,23 +110,80 @@ def test_advance_matches_oracle(oracle_mod, method):
         s.close()
 
 
-def test_mixed_precision_and_adjoint_refusal(oracle_mod):
-    from dg_hdg_euler_cpp_b200.solver import DGHError, Solver
+def test_mixed_precision_matches_fp64():
+    from dg_hdg_euler_cpp_b200.solver import Solver
 
     out = {}
     for precision in ("fp64", "mixed"):
         s = Solver(nx=4, ny=4, k=2, quad=5, cfl=2.0, integrator="be", final_time=0.02, restart=20,
                    method="dg", precision=precision)
         out[precision] = s.advance("dg", np_(s.initial()))[0]
-        if precision == "fp64":
-            u = s.initial()
-            s.freeze(u)
-            s.set_stage(u, .01)
-            s.dg_refresh(u)
-            with pytest.raises(DGHError, match="collocated volume rule only"):
-                s.dg_apply_T(u)
         s.close()
     assert np.max(np.abs(out["mixed"] - out["fp64"])) <= 1e-10 * np.max(np.abs(out["fp64"]))
+
+
+@pytest.mark.parametrize("nx,ny,k,quad", CASES)
+def test_adjoint_apply_and_transposed_solve(oracle_mod, nx, ny, k, quad):
+    """J^T w with the over-integrated volume term: the transpose identity, the transpose of the
+    oracle's coupling blocks, and the transposed block-Jacobi solve with those blocks."""
+    o, s = setup(oracle_mod, nx, ny, k, quad)
+    u = o.initial()
+    o.freeze(u)
+    s.freeze(s.tensor(u))
+    o.set_stage(u, .004)
+    s.set_stage(s.tensor(u), .004)
+    up = u + 1e-3 * direction(u.size)
+    o.dg_refresh(up)
+    s.dg_refresh(s.tensor(up))
+    v, w = direction(u.size, .31, .79), direction(u.size, .17, .53)
+    jv = np_(s.dg_apply(s.tensor(v)))
+    jtw = np_(s.dg_apply_T(s.tensor(w)))
+    lhs, rhs = float(jtw @ v), float(w @ jv)
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), np.linalg.norm(jtw) * np.linalg.norm(v))
+    ref = o.dg_apply_transpose(w)
+    assert rel(jtw, ref) <= 1e-12
+    s.precond_refresh("dg")
+    z = np_(s.precond_apply("dg_t", s.tensor(v)))
+    m = o.block
+    for cell in sorted({0, nx * ny // 2, nx * ny - 1}):
+        x = np.linalg.solve(o.dg_block(cell, cell).T, v[cell * m:(cell + 1) * m])
+        assert rel(z[cell * m:(cell + 1) * m], x) <= 1e-10
+
+
+def test_discrete_adjoint_gradient_with_quadrature():
+    """DIRK3 discrete adjoint on an over-integrated run against central differences (h = 1e-6)
+    of the replayed trajectory, as for the collocated rule."""
+    import ctypes
+
+    from dg_hdg_euler_cpp_b200 import _lib
+    from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
+
+    nx, ny, k, steps, every = 6, 6, 3, 3, 2
+    s = Solver(nx=nx, ny=ny, k=k, quad=6, cfl=0.3, integrator="ssp-dirk3", steps=steps, method="dg", restart=20)
+    it = Integrator(s, "dg")
+    u0 = np_(s.initial())
+    n = s.size
+    rho = ((np.arange(n) // (k + 1) ** 2) % 4) == 0
+    grad = np.zeros(n)
+    st = _lib.dgh_adjoint_stats()
+    rc = s.lib.dgh_dirk3_adjoint(it.h, steps, every, u0.ctypes.data_as(ctypes.c_void_p),
+                                 grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st))
+    assert rc == 0, s.lib.dgh_integrator_error(it.h).decode()
+
+    def objective(u):
+        val = ctypes.c_double()
+        rc = s.lib.dgh_dirk3_replay(it.h, np.ascontiguousarray(u).ctypes.data_as(ctypes.c_void_p), ctypes.byref(val))
+        assert rc == 0, s.lib.dgh_integrator_error(it.h).decode()
+        return val.value
+
+    h = 1e-6
+    for seed in range(2):
+        phi = np.where(rho, np.random.default_rng(seed).standard_normal(n), 0.0) * 0.05 * np.abs(u0)
+        fd = (objective(u0 + h * phi) - objective(u0 - h * phi)) / (2 * h)
+        ad = float(grad @ phi)
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (seed, fd, ad)
+    it.close()
+    s.close()
 
 
 def test_cli_quad_summary_and_history(oracle_mod):

@@ -56,6 +56,16 @@ def test_blocks_reproduce_jv(nx, ny, k, quad):
             assert np.max(np.abs(got - jv[row * m:(row + 1) * m])) <= 1e-12 * np.max(np.abs(jv))
 
 
+@pytest.mark.parametrize("nx,ny,k,quad", [(3, 3, 2, 5), (3, 4, 1, 4)])
+def test_transpose_identity(nx, ny, k, quad):
+    """The adjoint restated from the coupling blocks is the transpose of the matrix-free J*v."""
+    o, u = setup(nx, ny, k, quad)
+    o.dg_refresh(u + 1e-3 * direction(u.size, .2, .9))
+    v, w = direction(u.size), direction(u.size, .17, .53)
+    lhs, rhs = float(o.dg_apply_transpose(w) @ v), float(w @ o.dg_apply(v))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(rhs), 1.0)
+
+
 def test_rule_of_n_points_is_the_collocated_one():
     a, u = setup(4, 3, 3, 0)
     b, _ = setup(4, 3, 3, 4)
