@@ -1,7 +1,8 @@
 """The 2D over-integrated volume rule (--quad Q > k+1) on the device against the oracle's
 restatement (tests/test_oracle_overint.py pins the oracle): residual, CFL rate, admissibility at
-the volume points, J*v, cell blocks, the block-Jacobi solve, the HDG condensation, and whole
-runs.  Tolerances as in tests/test_gpu_parity.py."""
+the volume points, J*v, cell blocks, the block-Jacobi solve, the HDG condensation, whole runs
+and the CLI, and the adjoint (J^T w, the transposed solve, the DIRK3 discrete-adjoint gradient).
+Tolerances as in tests/test_gpu_parity.py and tests/test_gpu_adjoint.py."""
 import numpy as np
 import pytest
 
