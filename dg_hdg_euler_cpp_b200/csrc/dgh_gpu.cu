@@ -344,13 +344,13 @@ void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, in
 // The left-looking FP64 LU (dgh_kernels_lu2.cuh): grid = resident CTAs, each with its scratch.
 template <bool AUG>
 void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out,
-                    float *out32 = nullptr) {
+                    float *out32 = nullptr, double *x_out = nullptr, double *y_out = nullptr) {
     need(m <= 2 * LL_THREADS && m % 4 == 0, "LU block width unsupported by the left-looking kernel");
     const size_t smem = lu_left_smem_bytes(m);
     allow_dynamic_smem((const void *)k_lu_left<AUG>, smem);
     const int grid = std::min(count, c->lu_grid);
     k_lu_left<AUG><<<grid, LL_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, c->lu_tri, perm, c->status, bit,
-                                                          slab_out ? 1 : 0, out32);
+                                                          slab_out ? 1 : 0, out32, x_out, y_out);
     c->launched();
 }
 // Narrow blocks (m <= 64): one warp per block in shared memory.
@@ -1688,8 +1688,9 @@ void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int
         }
     });
     c->launched();
-    if (variant == 0) {
-        launch_lu_left<true>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
+    if (variant == 0) {  // X and y straight to their persistent arrays
+        launch_lu_left<true>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false, nullptr,
+                             c->X + (size_t)first * c->m * c->t, c->Y + (size_t)first * c->m);
     } else {
         launch_lu<double>(c, c->aug, (size_t)c->m * ld, c->m, ld, count, c->aug_perm, ST_SINGULAR_HDG, false);
         constexpr size_t bs_smem = backsolve_smem_bytes();
@@ -1701,8 +1702,12 @@ void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int
         c->launched();
     }
     DGH_DISPATCH_N(c->n, {
-        k_hdg_schur<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y, c->cy, c->basis,
-                                                            c->g, first, count);
+        if (variant == 0)
+            k_hdg_schur<N, double, true><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y,
+                                                                      c->cy, c->basis, c->g, first, count);
+        else
+            k_hdg_schur<N, double, false><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S, c->X, c->Y,
+                                                                       c->cy, c->basis, c->g, first, count);
     });
     c->launched();
 }

@@ -51,9 +51,13 @@ k_hdg_assemble(TF *__restrict__ aug, const double *__restrict__ vol, const doubl
     }
 }
 
-// From the solved augmented columns: S_K = -(C X) (t x t, row-major), cy = C y, and the
-// persistent copies of X (m x t row-major) and y.
-template <int N, typename TF>
+// From the solved columns [X | y] of every cell: S_K = -(C X) (t x t, row-major) and cy = C y.
+// IN_X: the condensation LU wrote X (m x t row-major) and y straight to their persistent arrays;
+// otherwise they are read from the augmented workspace (ld = m + t + 1) and copied out.  Each
+// thread restricts one solved column to one line of face nodes for both faces of an axis (the
+// two faces read the same line with the eL and eR weights), so every solved value is read twice
+// instead of four times.
+template <int N, typename TF, bool IN_X>
 __global__ void __launch_bounds__(256)
 k_hdg_schur(const TF *__restrict__ aug, const double *__restrict__ fcache, const double *__restrict__ speeds,
             double *__restrict__ S, double *__restrict__ X, double *__restrict__ y, double *__restrict__ cy,
@@ -80,35 +84,47 @@ k_hdg_schur(const TF *__restrict__ aug, const double *__restrict__ fcache, const
         }
         __syncthreads();
         const TF *A = aug + (size_t)blk * M * LD;
-        // C applied to every solved column: restrict to (side, q), then the 4x4 derivative
-        for (int idx = threadIdx.x; idx < NFACES * N * (T + 1); idx += blockDim.x) {
-            const int col = idx % (T + 1), sq = idx / (T + 1), side = sq / N, q = sq % N;
-            const double *e = side % 2 ? b.eR : b.eL;
-            double rv[4];
+        const double *Xc = X + (size_t)cell * M * T, *yc = y + (size_t)cell * M;
+        // C applied to every solved column: restrict to the (axis, q) line, then the 4x4 derivative
+        for (int idx = threadIdx.x; idx < 2 * N * (T + 1); idx += blockDim.x) {
+            const int col = idx % (T + 1), aq = idx / (T + 1), axis = aq / N, q = aq % N;
+            double rl[4], rr[4];
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
-                double s = 0;
+                double sl = 0, sr = 0;
 #pragma unroll
-                for (int i = 0; i < N; ++i)
-                    s += e[i] * (double)A[(size_t)(w * P + face_node(N, side, q, i)) * LD + M + col];
-                rv[w] = s;
+                for (int i = 0; i < N; ++i) {
+                    const int r = w * P + face_node(N, 2 * axis, q, i);
+                    const double val = IN_X ? (col < T ? Xc[(size_t)r * T + col] : yc[r])
+                                            : (double)A[(size_t)r * LD + M + col];
+                    sl += b.eL[i] * val;
+                    sr += b.eR[i] * val;
+                }
+                rl[w] = sl;
+                rr[w] = sr;
             }
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                double s = 0;
+            for (int h = 0; h < 2; ++h) {
+                const int side = 2 * axis + h, sq = side * N + q;
+                const double *rv = h ? rr : rl;
 #pragma unroll
-                for (int w = 0; w < 4; ++w) s += rv[w] * G[sq * 16 + v * 4 + w];
-                const int row = side * FW + v * N + q;
-                if (col < T) S[(size_t)cell * T * T + (size_t)row * T + col] = -s;
-                else cy[(size_t)cell * T + row] = s;
+                for (int v = 0; v < 4; ++v) {
+                    double s = 0;
+#pragma unroll
+                    for (int w = 0; w < 4; ++w) s += rv[w] * G[sq * 16 + v * 4 + w];
+                    const int row = side * FW + v * N + q;
+                    if (col < T) S[(size_t)cell * T * T + (size_t)row * T + col] = -s;
+                    else cy[(size_t)cell * T + row] = s;
+                }
             }
         }
-        for (int idx = threadIdx.x; idx < M * (T + 1); idx += blockDim.x) {
-            const int r = idx / (T + 1), c = idx % (T + 1);
-            const double val = (double)A[(size_t)r * LD + M + c];
-            if (c < T) X[(size_t)cell * M * T + (size_t)r * T + c] = val;
-            else y[(size_t)cell * M + r] = val;
-        }
+        if (!IN_X)
+            for (int idx = threadIdx.x; idx < M * (T + 1); idx += blockDim.x) {
+                const int r = idx / (T + 1), c = idx % (T + 1);
+                const double val = (double)A[(size_t)r * LD + M + c];
+                if (c < T) X[(size_t)cell * M * T + (size_t)r * T + c] = val;
+                else y[(size_t)cell * M + r] = val;
+            }
     }
 }
 

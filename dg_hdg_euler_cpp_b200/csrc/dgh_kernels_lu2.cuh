@@ -213,13 +213,15 @@ __device__ __forceinline__ void ll_warp_argmax(double &bv, int &bp, int &bs) {
 // With out32 != nullptr the factors are instead written, rounded to FP32, in the FP32 slab
 // layout to out32 (m x m per block) and pool is left in original-row order: the mixed
 // precision preconditioner factors in FP64 and stores FP32.
-// AUG = true: pool holds [A | B | r] with ld > m; on exit columns m..ld-1 hold A^{-1}[B r]
-// (row i = unknown i); the A part holds the factors in original-row order (not used later).
+// AUG = true: pool holds [A | B | r] with ld > m; on exit X | y = A^{-1}[B r] (row i = unknown i)
+// is in columns m..ld-1, or, with x_out, in x_out (m x (ld - m - 1) row-major per matrix) and
+// y_out (m per matrix); the A part holds the factors in original-row order (not used later).
 // tri: per-CTA scratch of ceil(m/32) * LL_TRI doubles.
 template <bool AUG>
 __global__ void __launch_bounds__(LL_THREADS, 2)
 k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, double *__restrict__ tri_all,
-          int *__restrict__ perm_out, int *status, int singular_bit, int slab_out, float *__restrict__ out32) {
+          int *__restrict__ perm_out, int *status, int singular_bit, int slab_out, float *__restrict__ out32,
+          double *__restrict__ x_out, double *__restrict__ y_out) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int mp = (m + LL_NB - 1) / LL_NB * LL_NB, P = mp / LL_NB;
     double *acc = reinterpret_cast<double *>(smraw);  // mp rows x LL_AP
@@ -513,9 +515,14 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                         __syncthreads();
                     }
                 }
+                const int T = ld - m - 1;
                 for (int idx = tid; idx < m * LL_NB; idx += LL_THREADS) {
-                    const int i = idx / LL_NB, cc = idx % LL_NB;
-                    if (cc < ncols) A[(size_t)i * ld + j0 + cc] = acc[i * LL_AP + cc];
+                    const int i = idx / LL_NB, cc = idx % LL_NB, col = j0 + cc - m;
+                    if (cc >= ncols) continue;
+                    const double v = acc[i * LL_AP + cc];
+                    if (!x_out) A[(size_t)i * ld + j0 + cc] = v;
+                    else if (col < T) x_out[(size_t)blk * m * T + (size_t)i * T + col] = v;
+                    else y_out[(size_t)blk * m + i] = v;
                 }
                 __syncthreads();
             }
