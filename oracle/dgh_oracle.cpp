@@ -1139,6 +1139,14 @@ std::vector<std::vector<int>> periodic_adjacency(int cells) {
     for (int c = 0; c < cells; ++c) adj[c] = {(c + cells - 1) % cells, c, (c + 1) % cells};
     return adj;
 }
+std::vector<std::vector<int>> cartesian_adjacency(int nx, int ny) {
+    std::vector<std::vector<int>> adj((size_t)nx * ny);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            adj[x + nx * y] = {x + nx * y, (x + nx - 1) % nx + nx * y, (x + 1) % nx + nx * y, x + nx * ((y + ny - 1) % ny),
+                               x + nx * ((y + 1) % ny)};
+    return adj;
+}
 BlockILU0::BlockILU0(const std::vector<std::vector<int>> &adjacency, int w)
     : rows((int)adjacency.size()), width(w), row_ptr(rows + 1, 0), diag(rows), lus(rows) {
     for (int r = 0; r < rows; ++r) {

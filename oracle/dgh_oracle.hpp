@@ -183,6 +183,9 @@ class BlockILU0 {
 };
 // BlockGraph::periodic(cells) adjacency (block_graph.cpp:30-35)
 std::vector<std::vector<int>> periodic_adjacency(int cells);
+// BlockGraph::cartesian(nx, ny) adjacency (block_graph.cpp:20-29): each cell, its left, right,
+// lower and upper periodic neighbours, cells numbered x + nx y.
+std::vector<std::vector<int>> cartesian_adjacency(int nx, int ny);
 class BlockJacobi {
   public:
     BlockJacobi(int blocks, int width);

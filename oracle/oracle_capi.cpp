@@ -18,6 +18,7 @@ struct Handle {
     std::unique_ptr<DGOperator> dg;
     std::unique_ptr<HybridOperator> hdg;
     std::unique_ptr<BlockJacobi> pc_dg, pc_hdg;
+    std::unique_ptr<BlockILU0> ilu_dg;  // 2D block ILU(0) on the cartesian block graph (no reference counterpart)
     Vec residual;
 };
 template <class F> int guard(F &&f) {
@@ -208,18 +209,34 @@ int oracle_hdg_precond_apply(void *hv, const double *x, double *z) {
     auto *h = static_cast<Handle *>(hv);
     return guard([&] { Vec o; h->pc_hdg->apply(vec(x, h->p->trace_size()), o); out(o, z); });
 }
-// op 0: DG Jv with block-Jacobi; op 1: Schur apply with face block-Jacobi
+// Block ILU(0) of the DG Jacobian in the natural ordering on BlockGraph::cartesian, the pattern
+// the reference's direct solver assembles in 2D (time_integrator.cpp:35); the reference's 2D
+// front end accepts block-jacobi only (config.cpp:102), so this exists to measure what ILU(0)
+// would save in 2D.
+int oracle_dg_precond_refresh_ilu(void *hv) {
+    auto *h = static_cast<Handle *>(hv);
+    return guard([&] {
+        h->ilu_dg = std::make_unique<BlockILU0>(cartesian_adjacency(h->p->nx, h->p->ny), h->p->block);
+        h->ilu_dg->refresh([&](int r, int c, double *o) { h->dg->block(r, c, o); });
+    });
+}
+// op 0: DG Jv with block-Jacobi; op 1: Schur apply with face block-Jacobi; op 2: DG Jv with the
+// 2D block ILU(0) of oracle_dg_precond_refresh_ilu
 int oracle_gmres(void *hv, int op, int restart, const double *rhs, double *x, int limit, double tol,
                  int *iters, double *rel, double *residual) {
     auto *h = static_cast<Handle *>(hv);
     return guard([&] {
-        const int n = op == 0 ? h->p->size() : h->p->trace_size();
-        GMRES g(n, restart, op == 0 ? h->p->inverse_mass : h->p->inverse_trace_mass);
+        const int n = op != 1 ? h->p->size() : h->p->trace_size();
+        GMRES g(n, restart, op != 1 ? h->p->inverse_mass : h->p->inverse_trace_mass);
         Vec xv;
         LinearResult res;
         if (op == 0)
             res = g.solve(Action{h->dg.get(), [](const void *c, const Vec &a, Vec &b) { static_cast<const DGOperator *>(c)->apply(a, b); }},
                           Action{h->pc_dg.get(), [](const void *c, const Vec &a, Vec &b) { static_cast<const BlockJacobi *>(c)->apply(a, b); }},
+                          vec(rhs, n), xv, limit, tol);
+        else if (op == 2)
+            res = g.solve(Action{h->dg.get(), [](const void *c, const Vec &a, Vec &b) { static_cast<const DGOperator *>(c)->apply(a, b); }},
+                          Action{h->ilu_dg.get(), [](const void *c, const Vec &a, Vec &b) { static_cast<const BlockILU0 *>(c)->apply(a, b); }},
                           vec(rhs, n), xv, limit, tol);
         else
             res = g.solve(Action{h->hdg.get(), [](const void *c, const Vec &a, Vec &b) { static_cast<const HybridOperator *>(c)->apply(a, b); }},

@@ -173,6 +173,10 @@ class Oracle:
     def dg_precond_refresh(self) -> None:
         self._call("oracle_dg_precond_refresh")
 
+    def dg_precond_refresh_ilu(self) -> None:
+        """2D block ILU(0) of the DG Jacobian on the cartesian block graph (GMRES op 2)."""
+        self._call("oracle_dg_precond_refresh_ilu")
+
     def dg_precond_apply(self, x) -> np.ndarray:
         o = np.zeros(self.size)
         self._call("oracle_dg_precond_apply", _p(np.ascontiguousarray(x)), _p(o))
@@ -223,7 +227,8 @@ class Oracle:
         return o
 
     def gmres(self, op: int, rhs, restart: int, limit: int, tol: float):
-        n = self.size if op == 0 else self.trace_size
+        """op 0: DG with block-Jacobi, 1: Schur with face block-Jacobi, 2: DG with 2D block ILU(0)."""
+        n = self.trace_size if op == 1 else self.size
         x, res = np.zeros(n), np.zeros(n)
         it, rel = ctypes.c_int(), ctypes.c_double()
         self._call("oracle_gmres", ctypes.c_int(op), ctypes.c_int(restart), _p(np.ascontiguousarray(rhs)),
