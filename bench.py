@@ -379,6 +379,26 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
             "gmres_cycles": "cuda_graph" if graph else "stepped"}
 
 
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks(path: Path) -> tuple[dict, str]:
+    """The roofline denominators: the measured copy bandwidth `hbm_gbs` (GB/s) of the pool's
+    peaks file when it holds a positive number, else the fallback figures; the second value
+    says which ("measured" or "fallback")."""
+    try:
+        peaks = json.loads(path.read_text())
+        hbm = float(peaks["hbm_gbs"])
+        if hbm > 0:
+            merged = dict(FALLBACK_PEAKS)
+            merged.update(peaks)
+            merged["hbm_gbs"] = hbm
+            return merged, "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
+    return dict(FALLBACK_PEAKS), "fallback"
+
+
 def cpu_baseline(args, threads: int, steps: int, warm: int, n: int | None = None):
     """The oracle (a restatement of the reference's CPU algorithm) on the host cores: the same
     protocol at a reduced mesh of the same degree, DG and HDG, scaled by the cell-count ratio."""
@@ -414,13 +434,7 @@ def main():
 
     rank, local, world, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    peaks_path = ROOT / "MEASURED_PEAKS.json"
-    if peaks_path.exists():
-        peaks = json.loads(peaks_path.read_text())
-        peak_src = "measured"
-    else:
-        peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
-        peak_src = "fallback"
+    peaks, peak_src = load_peaks(ROOT / "MEASURED_PEAKS.json")
     configs = [c.split(":") for c in args.configs.split(",")]
     results = {}
     finals = {}

@@ -69,3 +69,23 @@ bench.main()
     lines = [[l for l in o.splitlines() if l.startswith("{")] for o in outs]
     assert len(lines[0]) == 1 and lines[1] == []
     assert '"impl": "reference"' in lines[0][0]
+
+
+def test_roofline_peaks_file(tmp_path):
+    """bench.py takes the measured copy bandwidth from the pool's peaks file when it holds one
+    and says so; a missing, unreadable or incomplete file gives the fallback figures."""
+    import json
+
+    from conftest import ROOT
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    f = tmp_path / "MEASURED_PEAKS.json"
+    assert bench.load_peaks(f) == (bench.FALLBACK_PEAKS, "fallback")
+    f.write_text(json.dumps({"hbm_gbs": 6547.5, "bf16_tflops": 1500.0, "clocks": {"sm": 1965}}))
+    peaks, src = bench.load_peaks(f)
+    assert src == "measured" and peaks["hbm_gbs"] == 6547.5 and peaks["bf16_tflops"] == 1500.0
+    for bad in ("{", json.dumps({"bf16_tflops": 1500.0}), json.dumps({"hbm_gbs": None}), json.dumps({"hbm_gbs": 0})):
+        f.write_text(bad)
+        assert bench.load_peaks(f) == (bench.FALLBACK_PEAKS, "fallback"), bad
