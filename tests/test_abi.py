@@ -101,6 +101,25 @@ def test_1d_cli_validates_flags_before_device_work():
         assert res.returncode == 1 and msg in res.stderr, (args, res.stderr)
 
 
+def test_2d_cli_validates_flags_before_device_work():
+    """The 2D front end parses dg_hdg_2d's flags with the reference's texts (config.cpp:23-122):
+    block-jacobi is its only 2D preconditioner, and the dense direct solve stays a CPU check."""
+    import subprocess
+
+    from dg_hdg_euler_cpp_b200 import BIN_PATH
+
+    if not BIN_PATH.exists():
+        pytest.skip("dgh2d not built")
+    for args, msg in [(["--precond", "block-ilu0"], "2D currently supports block-jacobi only"),
+                      (["--linear", "direct"], "CPU-only"), (["--ordering", "rcm"], "Invalid ordering"),
+                      (["--T", ".1", "--steps", "2"], "Choose either --T or --steps"),
+                      (["--integrator", "rk4"], "Invalid integrator"), (["--testcase", "vortex"], "Invalid testcase"),
+                      (["--method", "fem"], "Method must be dg, hdg, or both"),
+                      (["--precision", "fp16"], "Invalid precision"), (["--bogus"], "Unknown option")]:
+        res = subprocess.run([str(BIN_PATH), *args], capture_output=True, text=True, timeout=60)
+        assert res.returncode == 1 and msg in res.stderr, (args, res.stderr)
+
+
 def test_no_cpu_fallback_without_gpu(lib):
     import torch
 
