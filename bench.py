@@ -383,7 +383,7 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
 def load_peaks(path: Path) -> tuple[dict, str]:
-    """The roofline denominators: the measured copy bandwidth `hbm_gbs` (GB/s) of the pool's
+    """The roofline denominators: the measured copy bandwidth `hbm_gbs` (GB/s) of the measured
     peaks file when it holds a positive number, else the fallback figures; the second value
     says which ("measured" or "fallback")."""
     try:

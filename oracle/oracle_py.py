@@ -1,8 +1,9 @@
 """Test infrastructure only: ctypes wrapper over the CPU oracle (oracle/_bin/liboracle.so).
 
 The oracle is a plain C++ restatement of the reference solver YueWu2002/DG_HDG_Euler_Cpp
-(dg_hdg_2d/src, dg_hdg_1d/src, common/).  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
-leg use this module, always as the checker and never as the thing measured or shipped.
+(dg_hdg_2d/src, dg_hdg_1d/src, common/).  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline use this module: to check the device results, and (the CPU baseline) as the timed CPU
+restatement of the reference.  The product never loads it.
 """
 from __future__ import annotations
 

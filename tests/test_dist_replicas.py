@@ -72,7 +72,7 @@ bench.main()
 
 
 def test_roofline_peaks_file(tmp_path):
-    """bench.py takes the measured copy bandwidth from the pool's peaks file when it holds one
+    """bench.py takes the measured copy bandwidth from the measured peaks file when it holds one
     and says so; a missing, unreadable or incomplete file gives the fallback figures."""
     import json
 

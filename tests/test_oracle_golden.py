@@ -1,6 +1,6 @@
 """Pin the CPU oracle against the reference's own archived outputs (tests/golden/).
 
-These tests validate the checker itself: they run the oracle (a C++ restatement of
+These tests validate the oracle itself: they run it (a C++ restatement of
 YueWu2002/DG_HDG_Euler_Cpp) on the exact command lines the reference archived and compare
 residual histories, Krylov counts, L2 errors and nodal solutions.
 """
