@@ -4,18 +4,24 @@
 Workload (the reference's speed protocol, speed_test/2d/benchmark.py:21-44): rotated simple wave
 (alpha = 45 deg, gamma = 3) on a periodic 256 x 256 mesh, Q8 (k = 8, 324 unknowns per cell),
 backward Euler at CFL 5, one stage, GMRES(20) with exact block-Jacobi, ntol = ltol = 1e-12,
-HLL safety 1.1.  A "step" is one Newton update.  Per configuration (method x precision):
-  warm-up : W updates from the projected initial state (untimed),
-  protocol: reset to the initial state, update 1 untimed (the reference's warm-up update),
-  timed   : the next K updates (protocol updates 2..K+1), bracketed by barrier + synchronize and
-            CUDA events on the library's stream; K=3 is exactly the reference's measured set.
+HLL safety 1.1.  A "step" is one Newton update.  The protocol unit is the reference's: reset to
+the projected initial state and start the stage, Newton update 1 untimed (the reference's
+warm-up update), updates 2-4 timed.  Per configuration (method x precision):
+  warm-up : W updates in protocol units (untimed),
+  timed   : K updates, in ceil(K/3) protocol units; each unit's timed updates are bracketed by
+            barrier + synchronize and CUDA events on the library's stream, and the K timed
+            updates are always protocol updates 2-4 (never post-convergence updates 5+).
 value = (K_dg + K_hdg) / (t_dg + t_hdg) for the mixed-precision (FP32 block-Jacobi factors,
 FP64 everything else) DG and HDG solves; the FP64 forms and the per-method numbers are in
-"breakdown".  e2e repeats the timed updates through the C ABI with host buffers
+"breakdown", and the mixed-vs-FP64 speed-up, state error and Krylov change per method at the
+top level.  e2e repeats the timed updates through the C ABI with host buffers
 (dgh_newton_update_host: state H2D, update, state D2H every step).
 
---impl reference times the reference algorithm's CPU implementation (the oracle restatement;
-the reference itself needs Eigen, which this image lacks) on the host cores.
+cpu_baseline and --impl reference time the reference algorithm's CPU implementation (the oracle
+restatement; the reference itself needs Eigen, which this image lacks) on the host cores:
+single-threaded (the reference is single-threaded by construction) and as P concurrent
+single-thread processes pinned to their own cores (the all-core throughput), on a 16^2 k=8 proxy
+of the same workload scaled by the cell ratio (256).
 """
 from __future__ import annotations
 
@@ -55,9 +61,6 @@ def parse():
     p.add_argument("--stepped", action="store_true",
                    help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
-    p.add_argument("--cpu-sample-nx", type=int, default=32)
-    p.add_argument("--cpu-single-nx", type=int, default=16,
-                   help="mesh of the single-thread CPU sample (0 skips it)")
     return p.parse_args()
 
 
@@ -168,43 +171,59 @@ def solve_traffic(args):
     return SOLVE_FP32_TRAFFIC_PER_BLOCK_K8 * args.nx * args.nx if args.k == 8 else None
 
 
-def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: bool, rank: int, local: int):
+PROTOCOL_TIMED = 3  # updates 2-4 of every protocol unit are timed (speed_test/2d/benchmark.py:26-36)
+
+
+def protocol_units(k: int) -> list[int]:
+    """Timed updates per protocol unit: K timed updates in ceil(K/3) units of at most 3."""
+    return [min(PROTOCOL_TIMED, k - i) for i in range(0, k, PROTOCOL_TIMED)]
+
+
+def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: bool, rank: int, local: int,
+               e2e: bool):
     from dg_hdg_euler_cpp_b200 import _lib
     from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
 
     K, W = args.steps, args.warmup
-    s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=W + K + 2,
+    s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=4,
                method=method, precision=precision, restart=20, max_linear=1500, ntol=args.ltol, ltol=args.ltol,
                safety=1.1, device=local, autotune=1 if args.autotune else 0)
     s.gmres_graph(not args.stepped)
     it = Integrator(s, method)
+    lib = s.lib
     stream = torch.cuda.ExternalStream(s.stream(), device=s.device)
     u0 = s.initial()
-    # warm-up
-    it.stage_begin(u0)
-    for _ in range(W):
-        it.update()
-    # protocol: reset, untimed update 1
-    it.stage_begin(u0)
-    first = it.update()
-    barrier(pg, torch)
-    lib = s.lib
-    lib.dgh_timing_enable(s.h, 1)
-    launches0 = s.launch_count()
+    # warm-up: W updates in protocol units (stage start + up to 4 updates), untimed
+    done = 0
+    while done < W:
+        it.stage_begin(u0)
+        for _ in range(min(4, W - done)):
+            it.update()
+            done += 1
     sampler = ClockSampler(local) if sampler_on else None
     if sampler:
         sampler.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    rows = [it.update() for _ in range(K)]
-    e1.record(stream)
-    e1.synchronize()
-    barrier(pg, torch)
+    lib.dgh_timing_enable(s.h, 1)
+    launches = 0
+    ms = 0.0
+    rows, firsts = [], []
+    for n_timed in protocol_units(K):
+        it.stage_begin(u0)      # reset to the projected state
+        firsts.append(it.update())  # protocol update 1, untimed
+        barrier(pg, torch)
+        launches0 = s.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rows += [it.update() for _ in range(n_timed)]
+        e1.record(stream)
+        e1.synchronize()
+        barrier(pg, torch)
+        launches += s.launch_count() - launches0
+        ms += e0.elapsed_time(e1)
     if sampler:
         sampler.stop()
-    ms = allmax(pg, torch, e0.elapsed_time(e1))
-    launches = s.launch_count() - launches0
+    ms = allmax(pg, torch, ms)
 
     def read_timers():
         out = {}
@@ -215,7 +234,7 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
             out[name] = {"ms": tot.value, "launches": cnt.value}
         return out
 
-    timers = read_timers()
+    timers = read_timers()  # all updates of the timed units, update 1 included
     lib.dgh_timing_enable(s.h, 0)
     final = np.empty(s.size)
     lib.dgh_download(s.h, final.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(it.state_ptr()), s.size)
@@ -233,10 +252,10 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
         s.gmres_graph(True)
     out = {
         "method": method, "precision": precision, "updates": K, "ms": ms, "updates_per_s": 1000.0 * K / ms,
-        "ms_per_update": ms / K, "krylov": [r["krylov_iterations"] for r in rows],
-        "krylov_update1": first["krylov_iterations"],
+        "ms_per_update": ms / K, "protocol_units": len(firsts), "krylov": [r["krylov_iterations"] for r in rows],
+        "krylov_update1": [r["krylov_iterations"] for r in firsts],
         "rms": [r["residual_physical_rms"] for r in rows], "damping": [r["damping"] for r in rows],
-        "launches": launches, "timers": timers, "device_gb": s.device_bytes() / 1e9,
+        "launches": launches, "timers_all_unit_updates": timers, "device_gb": s.device_bytes() / 1e9,
         "clocks": sampler.summary() if sampler else None, "gmres_cycles": "stepped" if args.stepped else "cuda_graph",
         "autotune": s.autotune_report(),
     }
@@ -257,28 +276,31 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
                            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "bytes_per_launch": kb,
                            "avg_launch_ms": avg_ms, "launches": tk["launches"]}
         if not args.stepped:
-            out["roofline"]["measured_on"] = "update 1 from the stage start, cycles launched step by step"
+            out["roofline"]["measured_on"] = "protocol update 1, cycles launched step by step"
     else:
         out["roofline"] = None
     if not args.stepped:
         out["kernel_timers_stepped_update"] = kernel_timers
-    # e2e through the C ABI with host buffers
-    if not args.no_e2e:
-        it.stage_begin(u0)
-        it.update()
+    # e2e through the C ABI with host buffers: the same protocol units, the timed updates through
+    # dgh_newton_update_host (state H2D, update, state D2H inside the timed region)
+    if e2e:
         host = torch.empty(s.size, dtype=torch.float64, pin_memory=True)
-        lib.dgh_download(s.h, ctypes.c_void_p(host.data_ptr()), ctypes.c_void_p(it.state_ptr()), s.size)
         st = _lib.dgh_update_stats()
-        barrier(pg, torch)
-        t0 = time.perf_counter()
-        for _ in range(K):
-            rc = lib.dgh_newton_update_host(it.h, ctypes.c_void_p(host.data_ptr()), ctypes.byref(st))
-            if rc != 0:
-                raise RuntimeError(lib.dgh_integrator_error(it.h).decode())
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        barrier(pg, torch)
-        e2e_s = allmax(pg, torch, t1 - t0)
+        e2e_s = 0.0
+        for n_timed in protocol_units(K):
+            it.stage_begin(u0)
+            it.update()
+            lib.dgh_download(s.h, ctypes.c_void_p(host.data_ptr()), ctypes.c_void_p(it.state_ptr()), s.size)
+            barrier(pg, torch)
+            t0 = time.perf_counter()
+            for _ in range(n_timed):
+                rc = lib.dgh_newton_update_host(it.h, ctypes.c_void_p(host.data_ptr()), ctypes.byref(st))
+                if rc != 0:
+                    raise RuntimeError(lib.dgh_integrator_error(it.h).decode())
+            torch.cuda.synchronize()
+            e2e_s += time.perf_counter() - t0
+            barrier(pg, torch)
+        e2e_s = allmax(pg, torch, e2e_s)
         out["e2e"] = {"seconds": e2e_s, "updates_per_s": K / e2e_s, "h2d_bytes_per_step": s.size * 8,
                       "d2h_bytes_per_step": s.size * 8}
     it.close()
@@ -399,31 +421,121 @@ def load_peaks(path: Path) -> tuple[dict, str]:
     return dict(FALLBACK_PEAKS), "fallback"
 
 
-def cpu_baseline(args, threads: int, steps: int, warm: int, n: int | None = None):
-    """The oracle (a restatement of the reference's CPU algorithm) on the host cores: the same
-    protocol at a reduced mesh of the same degree, DG and HDG, scaled by the cell-count ratio."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle_py
+# ------------------------------------------------------------------------------ CPU legs
+CPU_PROXY_NX = 16  # update 1 at 16^2 k=8 takes DG 205 / HDG 162 Krylov iterations, the reference's 256^2 207 / 167
 
-    n = n or args.cpu_sample_nx
-    scale = (args.nx / n) ** 2
-    res = {}
-    for method in ("dg", "hdg"):
-        o = oracle_py.Oracle(f"--nx {n} --ny {n} --k {args.k} --integrator be --steps 1 --newton-steps "
-                             f"{warm + 1 + steps} --warmup-updates {warm + 1} --cfl 5 --restart 20 --ntol {args.ltol} "
-                             f"--ltol {args.ltol} --safety 1.1", threads=threads)
+
+def host_info() -> dict:
+    """nproc, the CPU model (lscpu) and the available host memory."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=20).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except (OSError, subprocess.SubprocessError):
+        pass
+    avail = None
+    try:
+        for line in Path("/proc/meminfo").read_text().splitlines():
+            if line.startswith("MemAvailable:"):
+                avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    cores = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count() or 1))
+    return {"nproc": len(cores), "cores": cores, "cpu_model": model, "mem_available_gb": avail / 1e9 if avail else None}
+
+
+def _cpu_worker(core, nx, k, ltol, warm, timed, start, queue):
+    """One single-thread oracle process pinned to `core`: `warm` untimed and then, after the
+    common start barrier, the timed samples; each sample is protocol update 1 of a fresh stage
+    from the projected state (the update's own time, as the reference's iteration_s)."""
+    try:
+        if core is not None and hasattr(os, "sched_setaffinity"):
+            os.sched_setaffinity(0, {core})
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle_py
+
+        cfg = (f"--nx {nx} --ny {nx} --k {k} --integrator be --steps 1 --newton-steps 1 --warmup-updates 0 --cfl 5 "
+               f"--restart 20 --max-linear 1500 --ntol {ltol} --ltol {ltol} --safety 1.1")
+        o = oracle_py.Oracle(cfg, threads=1)
         u0 = o.initial()
-        _, st, ups = o.advance(method, u0)
-        timed = ups[warm + 1: warm + 1 + steps]
-        sec = float(np.sum(timed[:, 12]))
-        res[method] = {"sample_seconds_per_update": sec / len(timed), "krylov": timed[:, 3].astype(int).tolist(),
-                       "projected_256_seconds_per_update": sec / len(timed) * scale}
-    total = res["dg"]["projected_256_seconds_per_update"] + res["hdg"]["projected_256_seconds_per_update"]
-    return {"value": 2.0 / total, "unit": "updates/s", "cores": threads, "kind": "port",
-            "sample": f"oracle (C++ restatement of the reference, FP64, {threads} threads) on {n}x{n} k={args.k}, "
-                      f"same BE CFL5 GMRES(20) protocol, {steps} timed updates per method after {warm + 1} warm-up; "
-                      f"per-update time scaled by the cell ratio {scale:g} to {args.nx}^2",
-            "per_method": res}
+        for method in warm:
+            o.advance(method, u0)
+        start.wait(timeout=3600)
+        out = {"dg": [], "hdg": []}
+        for method in timed:
+            _, _, ups = o.advance(method, u0)
+            out[method].append((float(ups[0, 12]), int(ups[0, 3])))
+        queue.put({"core": core, "samples": out})
+    except Exception as exc:  # reported by the parent
+        queue.put({"core": core, "error": repr(exc)})
+
+
+def cpu_run(args, processes: int, warm_each: int, timed_each: int) -> dict:
+    """`processes` concurrent single-thread oracle processes (spawned: the parent may hold a CUDA
+    context), each pinned to its own core, each running `warm_each` untimed and `timed_each` timed
+    samples of DG and of HDG.  Throughput per method = the sum over processes of 1 / (mean sample
+    time); value = one DG plus one HDG update per 2 / (1/thr_dg + 1/thr_hdg), scaled from the
+    proxy mesh to the workload's mesh by the cell ratio."""
+    import multiprocessing as mp
+
+    info = host_info()
+    ctx = mp.get_context("spawn")
+    queue = ctx.Queue()
+    start = ctx.Barrier(processes)
+    plan = [m for _ in range(timed_each) for m in ("dg", "hdg")]
+    warm = [m for _ in range(warm_each) for m in ("dg", "hdg")]
+    procs = [ctx.Process(target=_cpu_worker, args=(info["cores"][i % len(info["cores"])], CPU_PROXY_NX, args.k,
+                                                   args.ltol, warm, plan, start, queue)) for i in range(processes)]
+    t0 = time.perf_counter()
+    for pr in procs:
+        pr.start()
+    results = [queue.get(timeout=7200) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+    wall = time.perf_counter() - t0
+    errors = [r["error"] for r in results if "error" in r]
+    if errors:
+        raise RuntimeError("CPU baseline worker failed: " + errors[0])
+    scale = (args.nx / CPU_PROXY_NX) ** 2
+    thr, per = {}, {}
+    for method in ("dg", "hdg"):
+        times = [[t for t, _ in r["samples"][method]] for r in results]
+        thr[method] = sum(len(t) / sum(t) for t in times)  # proxy updates/s over all processes
+        per[method] = {"proxy_seconds_per_update": [float(np.mean(t)) for t in times],
+                       "krylov": sorted({kr for r in results for _, kr in r["samples"][method]}),
+                       "updates_per_s_at_workload": thr[method] / scale}
+    value = 2.0 / (1.0 / thr["dg"] + 1.0 / thr["hdg"]) / scale
+    return {"value": value, "processes": processes, "per_method": per, "cell_ratio": scale, "wall_s": wall,
+            "timed_samples_per_process": timed_each, "host": {k: info[k] for k in ("nproc", "cpu_model",
+                                                                                  "mem_available_gb")}}
+
+
+def cpu_processes(info: dict) -> int:
+    """P = min(cores, host RAM / per-process peak RSS); a 16^2 k=8 oracle process peaks near 1 GB."""
+    p = info["nproc"]
+    if info.get("mem_available_gb"):
+        p = min(p, max(1, int(info["mem_available_gb"] / 1.5)))
+    return max(1, p)
+
+
+def cpu_baseline(args) -> dict:
+    """cpu_baseline of our arm: the oracle single-threaded (one process alone) and the all-core
+    throughput (P concurrent single-thread processes), one timed DG and HDG sample each."""
+    info = host_info()
+    single = cpu_run(args, 1, 0, 1)
+    allc = cpu_run(args, cpu_processes(info), 0, 1)
+    sample = (f"oracle (the reference's CPU algorithm restated in C++, FP64, single-threaded per process) on a "
+              f"{CPU_PROXY_NX}x{CPU_PROXY_NX} k={args.k} proxy: protocol update 1 of BE CFL5 GMRES(20) from the "
+              f"projected state (its Krylov counts match the reference's 256^2 update 1), per-update time scaled "
+              f"by the cell ratio {single['cell_ratio']:g}; all-core = {allc['processes']} concurrent "
+              f"single-thread processes pinned to their own cores ({info['nproc']} cores, {info['cpu_model']})")
+    return {"value": allc["value"], "unit": "updates/s", "cores": allc["processes"], "kind": "port",
+            "sample": sample, "single_thread": {"value": single["value"], "unit": "updates/s", "cores": 1,
+                                                "per_method": single["per_method"]},
+            "all_core": allc}
 
 
 def main():
@@ -436,10 +548,12 @@ def main():
     torch.cuda.set_device(local)
     peaks, peak_src = load_peaks(ROOT / "MEASURED_PEAKS.json")
     configs = [c.split(":") for c in args.configs.split(",")]
+    has_mixed = any(p == "mixed" for _, p in configs)
     results = {}
     finals = {}
     for method, precision in configs:
-        out, final = run_config(args, method, precision, torch, pg, peaks, rank == 0, rank, local)
+        e2e = not args.no_e2e and (precision == "mixed" or not has_mixed)  # e2e of the headline solves
+        out, final = run_config(args, method, precision, torch, pg, peaks, rank == 0, rank, local, e2e)
         results[f"{method}_{precision}"] = out
         finals[(method, precision)] = final
     # error of the mixed-precision state against the all-FP64 state after the same updates
@@ -451,6 +565,9 @@ def main():
                                                             results[f"{method}_fp64"]["updates_per_s"])
             results[f"{method}_mixed"]["krylov_change_vs_fp64"] = (
                 sum(results[f"{method}_mixed"]["krylov"]) - sum(results[f"{method}_fp64"]["krylov"]))
+    mixed_vs_fp64 = {m: {k: results[f"{m}_mixed"][k] for k in ("speedup_vs_fp64", "rel_error_vs_fp64",
+                                                               "krylov_change_vs_fp64")}
+                     for m in ("dg", "hdg") if "speedup_vs_fp64" in results.get(f"{m}_mixed", {})}
     head = [k for k in ("dg_mixed", "hdg_mixed") if k in results] or list(results)
     tot_upd = sum(results[k]["updates"] for k in head)
     tot_ms = sum(results[k]["ms"] for k in head)
@@ -461,7 +578,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": tot_ms / tot_upd, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 (FP32 block-Jacobi factors in the mixed forms)", "data": "synthetic",
         "config": {"workload": f"{args.nx}x{args.nx} k={args.k} rotated simple wave, BE CFL5, GMRES(20), exact "
-                               f"block-Jacobi, ntol=ltol={args.ltol:g}, one Newton update per step; value combines "
+                               f"block-Jacobi, ntol=ltol={args.ltol:g}, one Newton update per step, timed updates "
+                               f"are protocol updates 2-4 of ceil(K/3) reset-and-warm units; value combines "
                                f"the {' and '.join(head)} solves", "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (factor pool 27-55 GB, Schur pool 10.9 GB)",
                    "value_definition": "(K_dg+K_hdg)/(t_dg+t_hdg) over the mixed-precision DG and HDG solves"},
@@ -472,6 +590,10 @@ def main():
             "kernel": dom["kernel"], "peak_source": peak_src,
             "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_launch_ms"]}) if dom else None,
         "gpu_launches": int(sum(results[k]["launches"] for k in head)),
+        "speedup_vs_fp64": {m: v["speedup_vs_fp64"] for m, v in mixed_vs_fp64.items()},
+        "rel_error_vs_fp64": {m: v["rel_error_vs_fp64"] for m, v in mixed_vs_fp64.items()},
+        "krylov_change_vs_fp64": {m: v["krylov_change_vs_fp64"] for m, v in mixed_vs_fp64.items()},
+        "per_method_updates_per_s": {k: results[k]["updates_per_s"] for k in results},
         "breakdown": results,
     }
     clocks = [results[k]["clocks"] for k in head if results[k].get("clocks")]
@@ -489,10 +611,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_graph_check:
         line["breakdown"]["gmres_graph_vs_stepped"] = graph_comparison(torch, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, os.cpu_count() or 1, 1, 0)
-        if args.cpu_single_nx:  # the reference is single-threaded by construction
-            single = cpu_baseline(args, 1, 1, 0, n=args.cpu_single_nx)
-            line["cpu_baseline"]["single_thread"] = {k: single[k] for k in ("value", "unit", "cores", "sample")}
+        line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg is not None:
@@ -500,37 +619,37 @@ def main():
 
 
 def main_reference(args):
+    """The reference arm: the reference's CPU algorithm (the oracle restatement; the reference
+    itself needs Eigen, absent here) as P concurrent single-thread processes pinned to their own
+    cores, the all-core throughput of a single-threaded code.  Each step is one DG and one HDG
+    sample (protocol update 1 from the projected state) on the 16^2 k=8 proxy, scaled to the
+    workload's mesh by the cell ratio; the W warm-up and K timed steps are spread over the P
+    processes.  Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle_py
-
-    n = args.cpu_sample_nx
-    scale = (args.nx / n) ** 2
-    K, W = args.steps, args.warmup
-    per = {}
-    for method in ("dg", "hdg"):
-        o = oracle_py.Oracle(f"--nx {n} --ny {n} --k {args.k} --integrator be --steps 1 --newton-steps {W + 1 + K} "
-                             f"--warmup-updates {W + 1} --cfl 5 --restart 20 --ntol {args.ltol} --ltol {args.ltol} "
-                             f"--safety 1.1", threads=threads)
-        _, st, ups = o.advance(method, o.initial())
-        timed = ups[W + 1: W + 1 + K]
-        per[method] = {"sample_seconds": float(np.sum(timed[:, 12])), "krylov": timed[:, 3].astype(int).tolist()}
-    total_sample = per["dg"]["sample_seconds"] + per["hdg"]["sample_seconds"]
-    value = 2.0 * K / (total_sample * scale)
-    sample = (f"oracle (C++ restatement of the reference's CPU algorithm, FP64, {threads} threads) on {n}x{n} "
-              f"k={args.k} with the same BE CFL5 GMRES(20) protocol; per-update time scaled by the cell ratio "
-              f"{scale:g} to {args.nx}^2")
-    line = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": K, "warmup": W,
-            "ms_per_step": 1000.0 * total_sample * scale / (2 * K), "higher_is_better": True, "scaling": "weak",
+    info = host_info()
+    procs = min(cpu_processes(info), max(1, args.steps))
+    timed_each = -(-args.steps // procs)
+    warm_each = -(-args.warmup // procs) if args.warmup > 0 else 0
+    res = cpu_run(args, procs, min(warm_each, 1), timed_each)
+    value = res["value"]
+    sample = (f"oracle (the reference's CPU algorithm restated in C++, FP64) as {procs} concurrent single-thread "
+              f"processes pinned to their own cores ({info['nproc']} cores, {info['cpu_model']}); each step = one DG "
+              f"and one HDG protocol update 1 on a {CPU_PROXY_NX}x{CPU_PROXY_NX} k={args.k} proxy (Krylov counts "
+              f"matching the reference's 256^2 update 1), {timed_each} per process, scaled by the cell ratio "
+              f"{res['cell_ratio']:g}")
+    line = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": f"{args.nx}x{args.nx} k={args.k} rotated simple wave, BE CFL5, GMRES(20), exact "
                                    f"block-Jacobi, ntol=ltol={args.ltol:g}; DG and HDG FP64 (the reference has no "
-                                   f"mixed precision)"},
-            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample,
-                             "per_method": per},
+                                   f"mixed precision); measured on the {CPU_PROXY_NX}x{CPU_PROXY_NX} k={args.k} proxy "
+                                   f"and scaled by the cell ratio {res['cell_ratio']:g}, so ms_per_step is the "
+                                   f"projected {args.nx}^2 time, not the proxy's",
+                       "proxy_mesh": f"{CPU_PROXY_NX}x{CPU_PROXY_NX}", "cell_ratio": res["cell_ratio"]},
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": procs, "kind": "port", "sample": sample,
+                             "per_method": res["per_method"], "wall_s": res["wall_s"], "host": res["host"]},
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

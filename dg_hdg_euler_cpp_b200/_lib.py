@@ -150,8 +150,8 @@ def build(verbose: bool = False) -> None:
 def load(path: Path | None = None) -> ctypes.CDLL:
     """Load the CUDA library; raises when it has not been built (no fallback path exists).
 
-    `path` selects another build of the same C ABI (the cycle-counter build lib/libdgh_gpu_probe.so
-    of lu_probe.py) for the process; it must come before the first load."""
+    `path` selects another build of the same C ABI for the process; it must come before the
+    first load."""
     global _lib
     if path is not None and _lib is not None and _lib._name != str(path):
         raise RuntimeError(f"{_lib._name} is already loaded in this process")

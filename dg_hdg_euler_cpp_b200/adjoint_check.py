@@ -45,6 +45,57 @@ def fourier_modes(s, nx: int, ny: int, k: int) -> np.ndarray:
     return np.array(phis)
 
 
+def gradient_check(nx: int = 128, k: int = 4, steps: int = 20, every: int = 5, cfl: float = 2.0, h: float = 1e-6,
+                   amplitude: float = 0.02) -> dict:
+    """Adjoint gradient of J with respect to the 8 Fourier coefficients against central finite
+    differences of the replayed trajectory; returns the record main() prints."""
+    from . import _lib
+    from .solver import Integrator, Solver
+
+    s = Solver(nx=nx, ny=nx, k=k, cfl=cfl, integrator="ssp-dirk3", steps=steps, method="dg", restart=20)
+    s.gmres_graph(True)
+    it = Integrator(s, "dg")
+    try:
+        u0 = s.initial().cpu().numpy()
+        phis = amplitude * fourier_modes(s, nx, nx, k)
+        grad = np.zeros(s.size)
+        st = _lib.dgh_adjoint_stats()
+        t0 = time.perf_counter()
+        rc = s.lib.dgh_dirk3_adjoint(it.h, steps, every, u0.ctypes.data_as(ctypes.c_void_p),
+                                     grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st))
+        t_adj = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(s.lib.dgh_integrator_error(it.h).decode())
+        g_ad = phis @ grad
+
+        def objective(u):
+            val = ctypes.c_double()
+            rc2 = s.lib.dgh_dirk3_replay(it.h, np.ascontiguousarray(u).ctypes.data_as(ctypes.c_void_p),
+                                         ctypes.byref(val))
+            if rc2 != 0:
+                raise RuntimeError(s.lib.dgh_integrator_error(it.h).decode())
+            return val.value
+
+        replay = objective(u0)
+        t0 = time.perf_counter()
+        g_fd = np.array([(objective(u0 + h * phi) - objective(u0 - h * phi)) / (2 * h) for phi in phis])
+        t_fd = time.perf_counter() - t0
+        rel = np.abs(g_ad - g_fd) / np.max(np.abs(g_ad))
+        return {
+            "config": f"{nx}x{nx} k={k} DIRK3 CFL {cfl} steps {steps} checkpoints every {every}",
+            "objective": st.objective, "objective_replayed": replay, "final_time": st.final_time,
+            "forward_newton_updates": st.forward_newton, "adjoint_krylov": st.adjoint_krylov,
+            "checkpoints": st.checkpoints, "recomputed_steps": st.recomputed_steps,
+            "gradient_adjoint": g_ad.tolist(), "gradient_fd": g_fd.tolist(),
+            "max_error_rel_to_max_gradient": float(rel.max()),
+            "per_mode_rel_error": (np.abs(g_ad - g_fd) / np.abs(g_ad)).tolist(), "fd_step": h,
+            "adjoint_seconds": t_adj, "fd_seconds_16_forward_runs": t_fd, "within_1e-6": bool(rel.max() <= 1e-6),
+        }
+    finally:
+        it.close()
+        s.close()
+
+
 def main() -> None:
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--nx", type=int, default=128)
@@ -55,48 +106,7 @@ def main() -> None:
     p.add_argument("--h", type=float, default=1e-6)
     p.add_argument("--amplitude", type=float, default=0.02, help="scale of each mode (density units)")
     args = p.parse_args()
-
-    from . import _lib
-    from .solver import Integrator, Solver
-
-    s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=args.cfl, integrator="ssp-dirk3", steps=args.steps,
-               method="dg", restart=20)
-    it = Integrator(s, "dg")
-    u0 = s.initial().cpu().numpy()
-    phis = args.amplitude * fourier_modes(s, args.nx, args.nx, args.k)
-    grad = np.zeros(s.size)
-    st = _lib.dgh_adjoint_stats()
-    t0 = time.perf_counter()
-    rc = s.lib.dgh_dirk3_adjoint(it.h, args.steps, args.every, u0.ctypes.data_as(ctypes.c_void_p),
-                                 grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st))
-    t_adj = time.perf_counter() - t0
-    if rc != 0:
-        raise RuntimeError(s.lib.dgh_integrator_error(it.h).decode())
-    g_ad = phis @ grad
-
-    def objective(u):
-        val = ctypes.c_double()
-        rc2 = s.lib.dgh_dirk3_replay(it.h, np.ascontiguousarray(u).ctypes.data_as(ctypes.c_void_p), ctypes.byref(val))
-        if rc2 != 0:
-            raise RuntimeError(s.lib.dgh_integrator_error(it.h).decode())
-        return val.value
-
-    t0 = time.perf_counter()
-    g_fd = np.array([(objective(u0 + args.h * phi) - objective(u0 - args.h * phi)) / (2 * args.h) for phi in phis])
-    t_fd = time.perf_counter() - t0
-    rel = np.abs(g_ad - g_fd) / np.max(np.abs(g_ad))
-    out = {
-        "config": f"{args.nx}x{args.nx} k={args.k} DIRK3 CFL {args.cfl} steps {args.steps} checkpoints every "
-                  f"{args.every}", "objective": st.objective, "final_time": st.final_time,
-        "forward_newton_updates": st.forward_newton, "adjoint_krylov": st.adjoint_krylov,
-        "recomputed_steps": st.recomputed_steps, "gradient_adjoint": g_ad.tolist(), "gradient_fd": g_fd.tolist(),
-        "max_error_rel_to_max_gradient": float(rel.max()),
-        "per_mode_rel_error": (np.abs(g_ad - g_fd) / np.abs(g_ad)).tolist(), "fd_step": args.h, "adjoint_seconds": t_adj,
-        "fd_seconds_16_forward_runs": t_fd, "within_1e-6": bool(rel.max() <= 1e-6),
-    }
-    print(json.dumps(out))
-    it.close()
-    s.close()
+    print(json.dumps(gradient_check(args.nx, args.k, args.steps, args.every, args.cfl, args.h, args.amplitude)))
 
 
 if __name__ == "__main__":

@@ -24,16 +24,6 @@
 #pragma once
 #include "dgh_kernels_lu.cuh"
 
-// Optional per-phase cycle counters (lu_probe.h, `make probe`); empty in the library build.
-// Phases: 0 panel load, 1 chunk triangle, 2 chunk GEMM, 3 pivot search (to the chosen pivot,
-// barrier included), 7 elimination, 6 rank-4 update, 4 write-back and triangle inverses,
-// 5 right-hand sides or final layout.
-#ifndef LL_PROBE
-#define LL_PROBE(phase)
-#define LL_PROBE_DECL
-#define LL_PROBE_FLUSH
-#endif
-
 namespace dgh {
 
 constexpr int LL_NB = 32;              // panel width and chunk size
@@ -234,7 +224,6 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = LL_THREADS / 32;
     double *tri = tri_all + (size_t)blockIdx.x * P * LL_TRI;
-    LL_PROBE_DECL
 
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         double *A = pool + (size_t)blk * stride;
@@ -244,22 +233,18 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
 
         for (int p = 0; p < P; ++p) {
             const int k0 = p * LL_NB, nb = min(LL_NB, m - k0);
-            LL_PROBE(0);
             // ---- load panel columns k0..k0+nb-1 of every position (zero padding)
             ll_load_cols(acc, A, ld, piv, m, mp, k0, nb);
             __syncthreads();
             // ---- left-looking update with the finished chunks
             for (int q = 0; q < p; ++q) {
                 const int q0 = q * LL_NB;
-                LL_PROBE(1);
                 if (q + 1 < p) ll_prefetch(A, ld, piv, q0 + LL_NB, q0 + 2 * LL_NB, m);
                 ll_chunk_tri(acc, tri + (size_t)q * LL_TRI, q0);
                 __syncthreads();
-                LL_PROBE(2);
                 ll_chunk_gemm(acc, A, ld, piv, q0, LL_NB, q0 + LL_NB, m);
                 __syncthreads();
             }
-            LL_PROBE(3);
             // ---- factor the panel: rows at positions k0..m-1, one barrier per column.  Slot s
             // is acc row s.  The rows come in groups of 8 dealt round-robin to the warps (group G
             // to warp G % 8), so every warp holds about (m - k0) / 8 rows; lane l owns the slots
@@ -291,7 +276,6 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 int psl[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    LL_PROBE(3);
                     const int jj = b0 + u, tp = k0 + jj;
                     double bv = -2.;
                     int bp = 0x7fffffff, bs = -1;
@@ -321,7 +305,6 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                         if (ov > bv || (ov == bv && op < bp)) { bv = ov; bp = op; bs = cand_s[jj & 1][w]; }
                     }
                     psl[u] = bs;
-                    LL_PROBE(7);
                     // swap positions tp and bp (the slot at tp moves to bp)
                     if (s0 < m) { if (s0 == bs) pos0 = tp; else if (pos0 == tp) pos0 = bp; }
                     if (s1 < m) { if (s1 == bs) pos1 = tp; else if (pos1 == tp) pos1 = bp; }
@@ -373,7 +356,6 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                         }
                     __syncwarp();
                 }
-                LL_PROBE(6);
                 // rank-4 update of columns b0+4..nb-1 for this warp's unpivoted rows
                 if (b0 + 4 < nb) {
                     const int tp = k0 + b0 + 3;
@@ -424,7 +406,6 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 for (int k = 0; k < 4; ++k) ppsl[k] = psl[k];
                 pb0 = b0;
             }
-            LL_PROBE(4);
             // ---- new positions, write back, permutation update
             if (s0 < m) posmap[s0] = pos0;
             if (s1 < m) posmap[s1] = pos1;
@@ -488,7 +469,6 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
             __syncthreads();
         }
 
-        LL_PROBE(5);
         if (AUG) {
             // ---- right-hand sides: forward with L, backward with U, 32 columns at a time
             for (int j0 = m; j0 < ld; j0 += LL_NB) {
@@ -578,12 +558,9 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 }
             }
         }
-        LL_PROBE(5);
         if (tid == 0 && bad) atomicOr(status, singular_bit);
         __syncthreads();
     }
-    LL_PROBE(5);
-    LL_PROBE_FLUSH;
 }
 
 }  // namespace dgh

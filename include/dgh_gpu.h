@@ -59,7 +59,8 @@ enum { DGH_OP_DG = 0, DGH_OP_HDG = 1, DGH_OP_DG_T = 2 };
 /* config.hpp:7-18 plus the precision and the operators to allocate.  dim = 1 selects the 1D
  * solver of dg_hdg_1d/ (config.hpp:7-19 there): nx is the number of cells, ny is ignored,
  * NVAR = 3, two faces per cell, and quadrature may exceed degree+1 (over-integration, up to
- * 20 points).  In 2D the quadrature is collocated (0 or degree+1). */
+ * 20 points).  In 2D the quadrature is 0 or degree+1 (collocated) or any value from degree+2
+ * to 16 (the over-integrated volume rule). */
 typedef struct dgh_config {
     int nx, ny, degree, quadrature;
     int restart, max_linear, max_newton, steps, newton_steps, warmup_updates;
@@ -266,7 +267,8 @@ int dgh_dirk3_adjoint(dgh_integrator *it, int steps, int checkpoint_every, const
 int dgh_dirk3_replay(dgh_integrator *it, const double *host_u0, double *objective);
 
 /* ---- Allocation-free residual ---------------------------------------------------------------
- * No counterpart in the reference.  R(u) exactly as dgh_residual computes it, for callers that
+ * No counterpart in the reference.  R(u) as dgh_residual computes it on a context with the
+ * collocated volume rule (quadrature 0 or degree+1; there is no quadrature argument), for callers that
  * cannot allocate device memory: an allocation-free time loop, work issued while a stream is
  * being captured into a CUDA graph (cudaMalloc is not permitted there), or a host that plans
  * every byte of device memory itself.  It needs no context and allocates nothing (no cudaMalloc,
@@ -279,7 +281,10 @@ int dgh_dirk3_replay(dgh_integrator *it, const double *host_u0, double *objectiv
  *    them) and the output r are device pointers the caller owns; geometry follows testcase
  *    (DGH_TEST_*) and gamma = 3.  Work is queued on stream (a cudaStream_t; NULL = default).
  *  - The first call on a device looks up the scratch array's device address with that device
- *    current; make that first call before any stream capture.
+ *    current and keeps it; make that first call before any stream capture.  The kept address
+ *    belongs to the device's primary context: after cudaDeviceReset (or anything else that
+ *    destroys that context) it is stale, and the entry point must not be called again in
+ *    that process.
  *  - Every call shares the one scratch array and the kernels overwrite all of it that they read,
  *    so nothing needs clearing between calls; but calls whose work overlaps on the GPU (other
  *    streams, other host threads) race on it and must be ordered by the caller.

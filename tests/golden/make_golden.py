@@ -32,8 +32,8 @@ ACC = "accuracy_test/results/2d_submission_20261019T234902_AtKkgL/job_7640912/da
 for n in (32, 64, 128, 256):
     FILES.append((f"{ACC}/n{n}_summary.csv", f"acc_n{n}_summary.csv"))
     FILES.append((f"{ACC}/n{n}.command.json", f"acc_n{n}.command.json"))
-FILES.append((f"{ACC}/n32_iterations.csv", "acc_n32_iterations.csv"))
-FILES.append((f"{ACC}/n64_iterations.csv", "acc_n64_iterations.csv"))
+for n in (32, 64, 128, 256):
+    FILES.append((f"{ACC}/n{n}_iterations.csv", f"acc_n{n}_iterations.csv"))
 FILES.append((f"{ACC}/convergence.csv", "acc_convergence.csv"))
 # 2D speed family, 256^2 BE CFL5 four updates (config 256^2 k=8 and k=0..7)
 SPD = "speed_test/results/2d_submission_20261019T205542_KhFC6z/job_7635952/data"
@@ -42,6 +42,12 @@ for k in range(9):
         FILES.append((f"{SPD}/k{k}_{m}_iterations.csv", f"speed256_k{k}_{m}_iterations.csv"))
         FILES.append((f"{SPD}/k{k}_{m}_summary.csv", f"speed256_k{k}_{m}_summary.csv"))
 FILES.append((f"{SPD}/k8_dg.command.json", "speed256_k8_dg.command.json"))
+# 512^2 k=8, BE CFL5 four updates, GMRES(30) (DG and HDG ran as separate jobs)
+N512 = "speed_test/results/2d_n512_restart30_20261020T220633_rt2c3wx6"
+for m, job in (("dg", "job_7718103"), ("hdg", "job_7687732")):
+    for part in ("iterations", "summary"):
+        FILES.append((f"{N512}/{job}/data/k8_{m}_{part}.csv", f"speed512_k8_{m}_{part}.csv"))
+    FILES.append((f"{N512}/{job}/data/k8_{m}.command.json", f"speed512_k8_{m}.command.json"))
 # 1D production-path checks (code_test/1d/test_solver.py): 32 cells k=3 one BE step and
 # 16 cells k=2 DIRK3 to T=0.02, DG and HDG, block-Jacobi GMRES, with their commands
 ONE = "code_test/1d/results/intel_final_20261019"

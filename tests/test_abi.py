@@ -199,17 +199,11 @@ def test_reference_executable_names():
         assert res.returncode == 0 and res.stdout.startswith(dim), (name, res.stdout[:80])
 
 
-def test_probe_build_is_opt_in_and_exclusive(lib):
-    """The cycle-counter build (make probe) exports the same C ABI plus its counter table, and a
-    process keeps the library it loaded first."""
+def test_library_path_is_exclusive_per_process(lib):
+    """A process keeps the library it loaded first: asking for another build of the C ABI after
+    the first load is refused."""
     from dg_hdg_euler_cpp_b200 import _lib
-    from dg_hdg_euler_cpp_b200.lu_probe import PHASES, PROBE_LIB
 
-    assert sorted(PHASES) == list(range(8))
     with pytest.raises(RuntimeError, match="already loaded"):
-        _lib.load(PROBE_LIB)
+        _lib.load(_lib.LIB_PATH.with_name("libdgh_gpu_other.so"))
     assert _lib.load(_lib.LIB_PATH) is lib
-    if PROBE_LIB.exists():
-        probe = ctypes.CDLL(str(PROBE_LIB))
-        for name in list(_lib.SIGNATURES) + ["ll_probe_reset", "ll_probe_read"]:
-            assert hasattr(probe, name), name

@@ -61,14 +61,30 @@ def test_reference_arm_prints_on_rank_zero_only():
 import sys
 sys.path.insert(0, sys.argv[1])
 import bench
-sys.argv = ["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--nx", "256",
-            "--cpu-sample-nx", "16", "--k", "8"]
+sys.argv = ["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "2", "--warmup", "1", "--nx", "256",
+            "--k", "2"]
 bench.main()
 """
     outs = run_ranks(code)
     lines = [[l for l in o.splitlines() if l.startswith("{")] for o in outs]
     assert len(lines[0]) == 1 and lines[1] == []
     assert '"impl": "reference"' in lines[0][0]
+    import json
+
+    rec = json.loads(lines[0][0])
+    assert rec["value"] > 0 and rec["config"]["proxy_mesh"] == "16x16" and rec["config"]["cell_ratio"] == 256
+    assert rec["cpu_baseline"]["cores"] >= 1 and rec["cpu_baseline"]["host"]["nproc"] >= 1
+    assert rec["cpu_baseline"]["per_method"]["dg"]["krylov"]
+
+
+def test_protocol_units_time_updates_two_to_four_only():
+    """K timed updates come in ceil(K/3) protocol units of at most 3 (updates 2-4 of each unit)."""
+    import bench
+
+    assert bench.protocol_units(20) == [3, 3, 3, 3, 3, 3, 2]
+    assert bench.protocol_units(3) == [3]
+    assert bench.protocol_units(1) == [1]
+    assert sum(bench.protocol_units(17)) == 17 and max(bench.protocol_units(17)) == 3
 
 
 def test_roofline_peaks_file(tmp_path):

@@ -87,36 +87,44 @@ def test_256_initial_residual_and_dt(k):
 
 
 @pytest.mark.parametrize("method,precision", [("dg", "fp64"), ("hdg", "fp64"), ("dg", "mixed"), ("hdg", "mixed")])
-def test_256_k8_speed_protocol_first_updates(method, precision):
-    """Full-size 256^2 k=8 BE CFL 5 (the speed configuration): after Newton updates 1 and 2 the
-    residual rms matches the reference's archived history; FP64 Krylov counts within +-1."""
+def test_256_k8_speed_protocol_all_updates(method, precision):
+    """Full-size 256^2 k=8 BE CFL 5 (the speed configuration), all four Newton updates of the
+    reference's speed protocol against its archived history: the residual rms at the start of
+    every update (1e-10 relative above 1e-6 r0, an absolute 1e-10 r0 floor below, where the last
+    two sit at 1e-9 and 7e-13), the residual after update 4, and in FP64 the Krylov counts
+    207/237/262/349 (DG) and 167/191/218/250 (HDG) within +-1 for updates 1-3.  Update 4 solves a
+    system whose right-hand side is the residual at the 7e-13 rounding floor, so its direction is
+    rounding noise and its Krylov count is held to 5 %."""
     from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
 
     ref = read_csv(GOLDEN / f"speed256_k8_{method}_iterations.csv")
+    assert len(ref) == 4
     s = Solver(nx=256, ny=256, k=8, cfl=5.0, integrator="be", steps=1, newton_steps=4, method=method, restart=20,
                precision=precision)
+    s.gmres_graph(True)
     it = Integrator(s, method)
     u = s.initial()
     dt = it.stage_begin(u)
     assert abs(dt - float(ref[0]["dt"])) <= 1e-15 * dt
-    rows = [it.update(), it.update()]
+    rows = [it.update() for _ in range(4)]
+    r0 = float(ref[0]["residual_physical_rms"])
     for k, row in enumerate(rows):
-        assert abs(row["residual_physical_rms"] - float(ref[k]["residual_physical_rms"])) <= 1e-10 * float(
-            ref[k]["residual_physical_rms"])
+        x, y = row["residual_physical_rms"], float(ref[k]["residual_physical_rms"])
+        if y > 1e-6 * r0:
+            assert abs(x - y) <= 1e-10 * y, (k, x, y)
+        else:
+            assert abs(x - y) <= 1e-10 * r0, (k, x, y)
         if precision == "fp64":
-            assert abs(row["krylov_iterations"] - int(ref[k]["krylov_iterations"])) <= 1
-    # the residual after update 2 (third row of the archived history)
-    r = s.vec()
-    state = s.torch.empty_like(r)
+            kr, kref = row["krylov_iterations"], int(ref[k]["krylov_iterations"])
+            assert abs(kr - kref) <= (1 if k < 3 else max(1, round(0.05 * kref))), (k, kr, kref)
+    # the residual after update 4 sits at the same rounding floor
     import ctypes
 
+    state = s.vec()
     s.lib.dgh_axpby(s.h, 1.0, ctypes.c_void_p(it.state_ptr()), 0.0, ctypes.c_void_p(it.state_ptr()),
                     ctypes.c_void_p(state.data_ptr()), state.numel())
     s.lib.dgh_sync(s.h)
-    rms2 = s.residual_rms(s.residual(state))
-    ref2 = float(ref[2]["residual_physical_rms"])
-    # 1e-9 is far below the rms (1e-3 of r0); compare on the absolute floor used for histories
-    assert abs(rms2 - ref2) <= 1e-10 * float(ref[0]["residual_physical_rms"])
+    assert s.residual_rms(s.residual(state)) <= 1e-10 * r0
     it.close()
     s.close()
 
