@@ -29,7 +29,7 @@ class dgh_config(ctypes.Structure):
         ("method", ctypes.c_int), ("integrator", ctypes.c_int), ("testcase", ctypes.c_int),
         ("precision", ctypes.c_int), ("check_update", ctypes.c_int), ("device", ctypes.c_int),
         ("dim", ctypes.c_int), ("autotune", ctypes.c_int),
-        ("preconditioner", ctypes.c_int),
+        ("preconditioner", ctypes.c_int), ("condense32", ctypes.c_int),
     ]
 
 
@@ -110,6 +110,7 @@ SIGNATURES = {
     "dgh_hdg_block": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "dgh_hdg_recover": (ctypes.c_int, [_VP, _VP, _VP]),
     "dgh_hdg_recovered_residual": (ctypes.c_int, [_VP, _VP, _VP]),
+    "dgh_hdg_retarget": (ctypes.c_int, [_VP, _VP]),
     "dgh_gmres": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, ctypes.c_int, ctypes.c_double, _I, _D]),
     "dgh_autotune_report": (ctypes.c_int, [_VP, _D]),
     "dgh_gmres_graph_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
@@ -122,6 +123,14 @@ SIGNATURES = {
     "dgh_newton_update": (ctypes.c_int, [_VP, ctypes.POINTER(dgh_update_stats)]),
     "dgh_newton_update_host": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(dgh_update_stats)]),
     "dgh_integrator_state": (_VP, [_VP]),
+    "dgh_integrator_set_limits": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "dgh_block_jacobi_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.POINTER(_VP)]),
+    "dgh_block_jacobi_destroy": (ctypes.c_int, [_VP]),
+    "dgh_block_jacobi_error": (ctypes.c_char_p, [_VP]),
+    "dgh_block_jacobi_factor": (ctypes.c_int, [_VP, _VP]),
+    "dgh_block_jacobi_apply": (ctypes.c_int, [_VP, _VP, _VP]),
+    "dgh_block_jacobi_perm": (ctypes.c_int, [_VP, _I]),
     "dgh_dirk3_adjoint": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.POINTER(dgh_adjoint_stats)]),
     "dgh_dirk3_replay": (ctypes.c_int, [_VP, _VP, _D]),
     "dgh_batch_create": (ctypes.c_int, [ctypes.POINTER(dgh_config), ctypes.c_int, ctypes.POINTER(_VP)]),

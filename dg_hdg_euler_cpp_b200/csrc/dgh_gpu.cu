@@ -118,9 +118,17 @@ struct dgh_ctx {
     double *aug = nullptr;
     int *aug_perm = nullptr;
     int aug_cells = 0;
+    size_t aug_bytes = 0;
     void *face_pool = nullptr;
     int *face_perm = nullptr;
     bool face_inverse = false;  // mixed 2D: face_pool holds FP32 explicit inverses
+    // FP32 condensation (dgh_config.condense32, 2D): the cells' LU factors of A in FP32 slabs
+    // with their permutations, the Schur blocks in FP32, the FP32 view of the condensation
+    // workspace, and a volume scratch vector for the recovery
+    float *S32 = nullptr, *lu32 = nullptr, *aug32 = nullptr;
+    int *lu32_perm = nullptr;
+    double *hq = nullptr;
+    bool c32() const { return cfg.condense32 != 0 && dim == 2; }
     // 1D block ILU(0): the periodic block pattern, its symbolic update schedule, the pattern
     // blocks (row-major, slot order) and the diagonal blocks' permutations, per operator
     struct IluPlan {
@@ -330,7 +338,8 @@ template <typename TF> void setup_lu_attrs(size_t smem) {
     allow_dynamic_smem((const void *)k_lu<TF, LU_NB, lu_tc<TF>()>, smem);
 }
 template <typename TF>
-void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out) {
+void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, int bit, bool slab_out,
+               bool lfix = false) {
     constexpr int TC = lu_tc<TF>();
     const size_t smem = lu_smem_bytes<TF, LU_NB, TC>(m);
     setup_lu_attrs<TF>(smem);
@@ -338,7 +347,7 @@ void launch_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, in
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu<TF, LU_NB, TC>, LU_THREADS, smem), "occupancy");
     const int grid = std::min(count, c->sms * std::max(1, per_sm));
     k_lu<TF, LU_NB, TC><<<grid, LU_THREADS, smem, c->stream>>>(pool, stride, m, ld, count, perm, c->status, bit,
-                                                               slab_out ? 1 : 0);
+                                                               slab_out ? 3 : lfix ? 2 : 0);
     c->launched();
 }
 // The left-looking FP64 LU (dgh_kernels_lu2.cuh): grid = resident CTAs, each with its scratch.
@@ -513,7 +522,23 @@ void hdg_apply(dgh_ctx *c, const double *lam, double *out) {
         c->launched();
         return;
     }
-    DGH_DISPATCH_N(c->n, { k_hdg_apply<N><<<c->faces, 256, 0, c->stream>>>(c->S, c->speeds, lam, out, c->basis, c->g); });
+    DGH_DISPATCH_N(c->n, {
+        if (c->c32()) k_hdg_apply32<N><<<c->faces, 256, 0, c->stream>>>(c->S32, c->speeds, lam, out, c->basis, c->g);
+        else k_hdg_apply<N><<<c->faces, 256, 0, c->stream>>>(c->S, c->speeds, lam, out, c->basis, c->g);
+    });
+    c->launched();
+}
+// Face-block Jacobi blocks of the current Schur operator (FP64 or FP32 Schur blocks) into pool.
+template <typename TF> void face_blocks(dgh_ctx *c, TF *pool) {
+    const long long tot = (long long)c->faces * c->fw * c->fw;
+    DGH_DISPATCH_N(c->n, {
+        if (c->c32())
+            k_face_blocks<N, TF, float><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S32, c->speeds, pool,
+                                                                                              c->basis, c->g);
+        else
+            k_face_blocks<N, TF, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, pool,
+                                                                                               c->basis, c->g);
+    });
     c->launched();
 }
 void op_apply(dgh_ctx *c, int op, const double *x, double *y) {
@@ -1011,6 +1036,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         need(k.dim == 1 || k.dim == 2, "Invalid dimension (1 or 2)");
         need(k.preconditioner == 0 || k.preconditioner == 1, "Invalid block preconditioner");
         need(k.preconditioner == 0 || k.dim == 1, "2D currently supports block-jacobi only");
+        need(k.condense32 == 0 || (k.condense32 == 1 && k.dim == 2), "FP32 condensation is a 2D HDG option (0 or 1)");
         // config.cpp:6-22 (dg_hdg_1d/src/config.cpp:6-21 in 1D)
         need(k.nx >= 3 && (k.dim == 1 || k.ny >= 3) && k.degree >= 0 && k.degree <= 8 && k.quadrature >= 0,
              "Invalid mesh or degree");
@@ -1161,15 +1187,24 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
             c->dg_perm = c->alloc<int>((size_t)c->cells * c->m);
         }
         if (c->has_hdg()) {
-            c->S = c->alloc<double>((size_t)c->cells * c->t * c->t);
-            c->X = c->alloc<double>((size_t)c->cells * c->m * c->t);
+            if (c->c32()) {  // FP32 Schur blocks and kept FP32 cell factors instead of FP64 S and X
+                c->S32 = c->alloc<float>((size_t)c->cells * c->t * c->t);
+                c->lu32 = c->alloc<float>((size_t)c->cells * c->m * c->m);
+                c->lu32_perm = c->alloc<int>((size_t)c->cells * c->m);
+                c->hq = c->alloc<double>(c->N);
+            } else {
+                c->S = c->alloc<double>((size_t)c->cells * c->t * c->t);
+                c->X = c->alloc<double>((size_t)c->cells * c->m * c->t);
+            }
             c->Y = c->alloc<double>((size_t)c->cells * c->m);
             c->cy = c->alloc<double>((size_t)c->cells * c->t);
             c->hrhs = c->alloc<double>(c->NT);
-            const size_t per_cell = (size_t)c->m * (c->m + c->t + 1) * sizeof(double);
+            const size_t per_cell = (size_t)c->m * (c->m + c->t + 1) * (c->c32() ? sizeof(float) : sizeof(double));
             const size_t budget = (size_t)8 << 30;  // condensation workspace: at most 8 GiB
             c->aug_cells = (int)std::max<size_t>(1, std::min<size_t>(c->cells, budget / per_cell));
-            c->aug = c->alloc<double>((size_t)c->aug_cells * c->m * (c->m + c->t + 1));
+            c->aug_bytes = (size_t)c->aug_cells * per_cell;
+            c->aug = reinterpret_cast<double *>(c->alloc<char>(c->aug_bytes));
+            if (c->c32()) c->aug32 = reinterpret_cast<float *>(c->aug);
             c->aug_perm = c->alloc<int>((size_t)c->aug_cells * c->m);
             c->face_pool = c->alloc<char>((size_t)c->faces * c->fw * c->fw * tsz);
             c->face_perm = c->alloc<int>((size_t)c->faces * c->fw);
@@ -1711,6 +1746,44 @@ void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int
     });
     c->launched();
 }
+// FP32 condensation of cells [first, first + count) (count <= aug_cells): [A | B | r] assembled
+// in FP32, right-looking FP32 LU with FP32 accumulation (the L fix-up kept), the factors copied
+// to the cells' FP32 slabs for later solves, back substitution for X | y, then S = -C X stored in
+// FP32, y and C y in FP64.
+void hdg_condense_chunk32(dgh_ctx *c, const double *r, int first, int count) {
+    const int ld = c->m + c->t + 1, grid = std::min(count, c->sms * 8);
+    const size_t stride = (size_t)c->m * ld;
+    DGH_DISPATCH_N(c->n, {
+        k_hdg_assemble<N, float><<<grid, 256, 0, c->stream>>>(c->aug32, c->vol, c->fcache, c->speeds, r, c->basis, c->g,
+                                                              c->inv_step, first, count, c->overint() ? 0 : 1);
+        if (c->overint()) {
+            k_vol_block_q<N, float><<<std::min(count, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                c->aug32, ld, c->volq, c->bq, c->g, first, count);
+            c->launched();
+        }
+    });
+    c->launched();
+    launch_lu<float>(c, c->aug32, stride, c->m, ld, count, c->lu32_perm + (size_t)first * c->m, ST_SINGULAR_HDG, false,
+                     true);
+    const long long warps = (long long)count * ((c->m + 31) / 32);
+    k_slab_pack<float><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, c->stream>>>(
+        c->aug32, stride, c->m, ld, count, c->lu32 + (size_t)first * c->m * c->m);
+    k_backsolve<float><<<std::min(count, c->sms * 8), LU_THREADS, 0, c->stream>>>(c->aug32, stride, c->m, ld, count);
+    c->launched(2);
+    DGH_DISPATCH_N(c->n, {
+        k_hdg_schur<N, float, false, float><<<grid, 256, 0, c->stream>>>(c->aug32, c->fcache, c->speeds, c->S32, nullptr,
+                                                                         c->Y, c->cy, c->basis, c->g, first, count);
+    });
+    c->launched();
+}
+// Condensed right-hand side from the cells' C y (g = 0 on the projected trace).
+void hdg_rhs_from_cy(dgh_ctx *c) {
+    DGH_DISPATCH_N(c->n, {
+        const long long tot = c->NT;
+        k_hdg_rhs<N><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->cy, c->hrhs, c->g);
+    });
+    c->launched();
+}
 // Times f(variant) for variants 0 and 1 (best of two runs each) and returns the faster one.
 template <class F> int tune_pick(dgh_ctx *c, F &&f, double *ms_out) {
     cudaEvent_t a = c->event(), b = c->event();
@@ -1826,14 +1899,10 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             const long long tot = (long long)c->faces * c->fw * c->fw;
             const size_t stride = (size_t)c->fw * c->fw;
             c->face_inverse = false;
-            if (c->mixed() && c->fw <= 64 && (size_t)tot <= (size_t)c->aug_cells * c->m * (c->m + c->t + 1)) {
+            if (c->mixed() && c->fw <= 64 && (size_t)tot * sizeof(double) <= c->aug_bytes) {
                 // FP64 blocks in the condensation workspace (free until the next condensation),
                 // inverted in FP64 and stored as FP32 inverses
-                DGH_DISPATCH_N(c->n, {
-                    k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, c->aug,
-                                                                                                  c->basis, c->g);
-                });
-                c->launched();
+                face_blocks<double>(c, c->aug);
                 const size_t smem = inv_narrow_smem_bytes(c->fw);
                 allow_dynamic_smem((const void *)k_inv_narrow, smem);
                 int resident = 0;
@@ -1845,18 +1914,10 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
                 c->launched();
                 c->face_inverse = true;
             } else if (c->mixed()) {
-                DGH_DISPATCH_N(c->n, {
-                    k_face_blocks<N, float><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (float *)c->face_pool,
-                                                                                                 c->basis, c->g);
-                });
-                c->launched();
+                face_blocks<float>(c, (float *)c->face_pool);
                 launch_lu_narrow<float>(c, (float *)c->face_pool, c->fw, c->faces, c->face_perm, ST_SINGULAR);
             } else {
-                DGH_DISPATCH_N(c->n, {
-                    k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, (double *)c->face_pool,
-                                                                                                  c->basis, c->g);
-                });
-                c->launched();
+                face_blocks<double>(c, (double *)c->face_pool);
                 launch_lu_narrow<double>(c, (double *)c->face_pool, c->fw, c->faces, c->face_perm, ST_SINGULAR);
             }
             c->check_status();
@@ -1871,7 +1932,7 @@ int dgh_precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
 // ---- HybridOperator ------------------------------------------------------------------------------
 int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
     return guard(c, [&] {
-        need(c->S, "context has no HDG operator");
+        need(c->has_hdg(), "context has no HDG operator");
         Timed tm(c, DGH_TIMER_CONDENSE);
         linearise(c, u);
         const int ld = c->m + c->t + 1;
@@ -1893,6 +1954,14 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
             }
             k1_hdg_rhs<<<grid1(c->NT), K1_THREADS, 0, c->stream>>>(c->cy, c->hrhs, c->g1);
             c->launched();
+            c->check_status();
+            c->condensed = true;
+            return;
+        }
+        if (c->c32()) {
+            for (int first = 0; first < c->cells; first += c->aug_cells)
+                hdg_condense_chunk32(c, r, first, std::min(c->aug_cells, c->cells - first));
+            hdg_rhs_from_cy(c);
             c->check_status();
             c->condensed = true;
             return;
@@ -1930,12 +1999,10 @@ int dgh_hdg_block(dgh_ctx *c, int row, int col, double *host_block) {
         double *tmp = c->alloc<double>(tot);
         if (c->d1()) {
             k1_face_blocks<double><<<grid1(tot), K1_THREADS, 0, c->stream>>>(c->S, c->speeds, tmp, c->g1);
+            c->launched();
         } else {
-            DGH_DISPATCH_N(c->n, {
-                k_face_blocks<N, double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->S, c->speeds, tmp, c->basis, c->g);
-            });
+            face_blocks<double>(c, tmp);
         }
-        c->launched();
         ck(cudaMemcpyAsync(host_block, tmp + (size_t)row * c->fw * c->fw, (size_t)c->fw * c->fw * sizeof(double),
                            cudaMemcpyDeviceToHost, c->stream), "copy");
         c->sync();
@@ -1949,10 +2016,36 @@ int dgh_hdg_recover(dgh_ctx *c, const double *dl, double *du) {
         need(c->condensed, "Condense the HDG operator first");
         if (c->d1()) {
             DGH_DISPATCH_N(c->n, { k1_hdg_recover<N><<<grid1(c->N), K1_THREADS, 0, c->stream>>>(c->X, c->Y, dl, du, c->g1); });
+        } else if (c->c32()) {
+            // du = A^{-1} (-B dlambda) - y with the kept FP32 factors (= -X dlambda - y)
+            DGH_DISPATCH_N(c->n, {
+                const long long tot = (long long)c->cells * N * N;
+                k_hdg_bmul<N><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(dl, c->speeds, c->hq, c->basis, c->g);
+            });
+            c->launched();
+            launch_solve<float>(c, c->lu32, c->lu32_perm, (size_t)c->m * c->m, c->m, c->cells, c->hq, du);
+            axpby(c, 1., du, -1., c->Y, du, c->N);
+            return;
         } else {
             DGH_DISPATCH_N(c->n, { k_hdg_recover<N><<<c->cells, 256, 0, c->stream>>>(c->X, c->Y, dl, du, c->g); });
         }
         c->launched();
+    });
+}
+int dgh_hdg_retarget(dgh_ctx *c, const double *r) {
+    return guard(c, [&] {
+        need(c->condensed, "Condense the HDG operator first");
+        need(c->c32(), "Retargeting needs the kept FP32 cell factors (condense32)");
+        Timed tm(c, DGH_TIMER_CONDENSE);
+        // y = A^{-1} r with the kept factors, C y per cell, and the condensed right-hand side
+        launch_solve<float>(c, c->lu32, c->lu32_perm, (size_t)c->m * c->m, c->m, c->cells, r, c->Y);
+        DGH_DISPATCH_N(c->n, {
+            k_hdg_schur<N, double, true, float><<<std::min(c->cells, c->sms * 8), 256, 0, c->stream>>>(
+                nullptr, c->fcache, c->speeds, nullptr, nullptr, c->Y, c->cy, c->basis, c->g, 0, c->cells,
+                NFACES * NVAR * N);
+        });
+        c->launched();
+        hdg_rhs_from_cy(c);
     });
 }
 int dgh_hdg_recovered_residual(dgh_ctx *c, const double *e, double *out) {
@@ -2003,6 +2096,164 @@ int dgh_gmres_graph_enable(dgh_ctx *c, int on) {
 const double *dgh_gmres_residual(dgh_ctx *c, int op) {
     if (!c || op < 0 || op > 2) return nullptr;
     return c->gres[op];
+}
+
+}  // extern "C"
+
+// ---- Standalone block Jacobi (BlockJacobi, block_jacobi.hpp:7-47) -----------------------------------
+// A pool of `count` dense m x m blocks, factored by one of the device LU kernels and applied as
+// z = A^{-1} x per block.  It runs on a bare context that carries only what the launch helpers
+// read: the stream, the status word, the SM count and the left-looking kernel's scratch.
+struct dgh_block_jacobi {
+    dgh_ctx *c = nullptr;
+    int m = 0, count = 0, precision = 0, variant = 0;
+    void *pool = nullptr;
+    int *perm = nullptr;
+    double *ws = nullptr;  // FP64 workspace of the left-looking kernel in the mixed form
+    bool factored = false;
+};
+
+extern "C" {
+
+int dgh_block_jacobi_create(int m, int count, int precision, int variant, int device, dgh_block_jacobi **out) {
+    if (!out) return DGH_ERR_INVALID;
+    *out = nullptr;
+    auto *bj = new dgh_block_jacobi;
+    bj->c = new dgh_ctx;
+    dgh_ctx *c = bj->c;
+    const int rc = guard(c, [&] {
+        need(m >= 1 && count >= 1 && m <= 2 * LL_THREADS, "Invalid block size or count");
+        need(precision == DGH_PRECISION_FP64 || precision == DGH_PRECISION_MIXED, "Invalid precision");
+        need(variant >= 0 && variant <= 3, "Invalid factorisation variant");
+        need(variant != 0 || m % 4 == 0, "LU block width unsupported by the left-looking kernel");
+        need(variant < 2 || (m <= 64 && m % 4 == 0), "block width unsupported by the narrow LU");
+        need(variant != 3 || precision == DGH_PRECISION_MIXED, "explicit inverses are the mixed form only");
+        need(m % 4 == 0, "block width must be a multiple of 4 (slab layout)");
+        bj->m = m;
+        bj->count = count;
+        bj->precision = precision;
+        bj->variant = variant;
+        c->cfg.precision = precision;
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(DGH_ERR_CUDA, "no CUDA device available");
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        cudaDeviceProp prop{};
+        ck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+        if (prop.major < 10) fail(DGH_ERR_CUDA, "this library is built for sm_100a (B200) only");
+        c->sms = prop.multiProcessorCount;
+        c->red_grid = c->sms * RED_BLOCKS_PER_SM;
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaMallocHost((void **)&c->pinned, 4096), "cudaMallocHost");
+        c->status = c->alloc<int>(1);
+        ck(cudaMemset(c->status, 0, sizeof(int)), "memset");
+        const size_t tsz = precision == DGH_PRECISION_MIXED ? sizeof(float) : sizeof(double);
+        bj->pool = c->alloc<char>((size_t)count * m * m * tsz);
+        bj->perm = c->alloc<int>((size_t)count * m);
+        if (variant == 0) {
+            const size_t smem = lu_left_smem_bytes(m);
+            allow_dynamic_smem((const void *)k_lu_left<false>, smem);
+            int per_sm = 0;
+            ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_left<false>, LL_THREADS, smem), "occupancy");
+            c->lu_grid = c->sms * std::max(1, per_sm);
+            c->lu_tri = c->alloc<double>((size_t)c->lu_grid * ((m + LL_NB - 1) / LL_NB) * LL_TRI);
+        }
+        if (precision == DGH_PRECISION_MIXED && (variant == 0 || variant == 3))
+            bj->ws = c->alloc<double>((size_t)count * m * m);
+        c->sync();
+    });
+    if (rc != DGH_OK) {
+        g_create_error = c->err;
+        dgh_block_jacobi_destroy(bj);
+        return rc;
+    }
+    *out = bj;
+    return DGH_OK;
+}
+
+int dgh_block_jacobi_destroy(dgh_block_jacobi *bj) {
+    if (!bj) return DGH_OK;
+    dgh_ctx_destroy(bj->c);
+    delete bj;
+    return DGH_OK;
+}
+
+const char *dgh_block_jacobi_error(const dgh_block_jacobi *bj) {
+    return bj ? bj->c->err.c_str() : g_create_error.c_str();
+}
+
+int dgh_block_jacobi_factor(dgh_block_jacobi *bj, const double *blocks) {
+    if (!bj) return DGH_ERR_INVALID;
+    dgh_ctx *c = bj->c;
+    return guard(c, [&] {
+        need(blocks != nullptr, "null block pointer");
+        const int m = bj->m, count = bj->count;
+        const size_t stride = (size_t)m * m, bytes = stride * count * sizeof(double);
+        bj->factored = false;
+        if (bj->precision == DGH_PRECISION_FP64) {
+            double *pool = (double *)bj->pool;
+            ck(cudaMemcpyAsync(pool, blocks, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy blocks");
+            if (bj->variant == 0) launch_lu_left<false>(c, pool, stride, m, m, count, bj->perm, ST_SINGULAR, true);
+            else if (bj->variant == 1) launch_lu<double>(c, pool, stride, m, m, count, bj->perm, ST_SINGULAR, true);
+            else launch_lu_narrow<double>(c, pool, m, count, bj->perm, ST_SINGULAR);
+        } else {
+            float *pool = (float *)bj->pool;
+            if (bj->variant == 0 || bj->variant == 3) {
+                ck(cudaMemcpyAsync(bj->ws, blocks, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy blocks");
+                if (bj->variant == 0) {
+                    launch_lu_left<false>(c, bj->ws, stride, m, m, count, bj->perm, ST_SINGULAR, false, pool);
+                } else {
+                    const size_t smem = inv_narrow_smem_bytes(m);
+                    allow_dynamic_smem((const void *)k_inv_narrow, smem);
+                    int resident = 0;
+                    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_inv_narrow, INV_THREADS, smem),
+                       "occupancy");
+                    constexpr int wpc = INV_THREADS / 32;
+                    const int grid = std::min((count + wpc - 1) / wpc, c->sms * std::max(1, resident));
+                    k_inv_narrow<<<grid, INV_THREADS, smem, c->stream>>>(bj->ws, m, count, pool, c->status, ST_SINGULAR);
+                    c->launched();
+                }
+            } else {
+                k_round<<<(unsigned)std::min<long long>(((long long)stride * count + 255) / 256, 65535LL * 16), 256, 0,
+                          c->stream>>>(blocks, pool, (long long)stride * count);
+                c->launched();
+                if (bj->variant == 1) launch_lu<float>(c, pool, stride, m, m, count, bj->perm, ST_SINGULAR, true);
+                else launch_lu_narrow<float>(c, pool, m, count, bj->perm, ST_SINGULAR);
+            }
+        }
+        c->check_status();
+        bj->factored = true;
+    });
+}
+
+int dgh_block_jacobi_apply(dgh_block_jacobi *bj, const double *x, double *z) {
+    if (!bj) return DGH_ERR_INVALID;
+    dgh_ctx *c = bj->c;
+    return guard(c, [&] {
+        need(bj->factored, "Refresh the block-Jacobi preconditioner before applying it");
+        const int m = bj->m, count = bj->count;
+        const size_t stride = (size_t)m * m;
+        if (bj->variant == 3) {
+            constexpr int wpc = INV_APPLY_THREADS / 32;
+            const int grid = std::min((count + wpc - 1) / wpc, c->sms * 8);
+            k_inv_apply<<<grid, INV_APPLY_THREADS, 0, c->stream>>>((const float *)bj->pool, m, count, x, z);
+            c->launched();
+        } else if (bj->precision == DGH_PRECISION_MIXED) {
+            launch_solve<float>(c, (const float *)bj->pool, bj->perm, stride, m, count, x, z);
+        } else {
+            launch_solve<double>(c, (const double *)bj->pool, bj->perm, stride, m, count, x, z);
+        }
+        c->sync();
+    });
+}
+
+int dgh_block_jacobi_perm(const dgh_block_jacobi *bj, int *host_perm) {
+    if (!bj || !host_perm) return DGH_ERR_INVALID;
+    dgh_ctx *c = bj->c;
+    return guard(c, [&] {
+        need(bj->factored && bj->variant != 3, "no factored permutation");
+        ck(cudaMemcpy(host_perm, bj->perm, sizeof(int) * (size_t)bj->m * bj->count, cudaMemcpyDeviceToHost),
+           "copy perm");
+    });
 }
 
 }  // extern "C"

@@ -51,18 +51,21 @@ k_hdg_assemble(TF *__restrict__ aug, const double *__restrict__ vol, const doubl
     }
 }
 
-// From the solved columns [X | y] of every cell: S_K = -(C X) (t x t, row-major) and cy = C y.
-// IN_X: the condensation LU wrote X (m x t row-major) and y straight to their persistent arrays;
-// otherwise they are read from the augmented workspace (ld = m + t + 1) and copied out.  Each
-// thread restricts one solved column to one line of face nodes for both faces of an axis (the
-// two faces read the same line with the eL and eR weights), so every solved value is read twice
-// instead of four times.
-template <int N, typename TF, bool IN_X>
+// From the solved columns [X | y] of every cell: S_K = -(C X) (t x t, row-major, stored as TS)
+// and cy = C y.  IN_X: the condensation LU wrote X (m x t row-major) and y straight to their
+// persistent arrays; otherwise they are read from the augmented workspace (ld = m + t + 1) and
+// copied out (X only where X is not null: the FP32 condensation keeps the LU factors instead).
+// Each thread restricts one solved column to one line of face nodes for both faces of an axis
+// (the two faces read the same line with the eL and eR weights), so every solved value is read
+// twice instead of four times.  col0 = T restricts the work to the y column (cy = C y alone,
+// IN_X, for a right-hand side solved against stored factors).
+template <int N, typename TF, bool IN_X, typename TS = double>
 __global__ void __launch_bounds__(256)
 k_hdg_schur(const TF *__restrict__ aug, const double *__restrict__ fcache, const double *__restrict__ speeds,
-            double *__restrict__ S, double *__restrict__ X, double *__restrict__ y, double *__restrict__ cy,
-            Basis1D b, Grid g, int first, int count) {
+            TS *__restrict__ S, double *__restrict__ X, double *__restrict__ y, double *__restrict__ cy,
+            Basis1D b, Grid g, int first, int count, int col0 = 0) {
     constexpr int P = N * N, M = NVAR * P, FW = NVAR * N, T = NFACES * FW, LD = M + T + 1;
+    const int ncol = T + 1 - col0;
     __shared__ double G[NFACES * N * 16];
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         const int cell = first + blk;
@@ -83,11 +86,11 @@ k_hdg_schur(const TF *__restrict__ aug, const double *__restrict__ fcache, const
                     G[k * 16 + v * 4 + ww] = (sign * a[v * 4 + ww] + (v == ww ? tau : 0.)) * w;
         }
         __syncthreads();
-        const TF *A = aug + (size_t)blk * M * LD;
-        const double *Xc = X + (size_t)cell * M * T, *yc = y + (size_t)cell * M;
+        const TF *A = aug ? aug + (size_t)blk * M * LD : nullptr;
+        const double *Xc = X ? X + (size_t)cell * M * T : nullptr, *yc = y + (size_t)cell * M;
         // C applied to every solved column: restrict to the (axis, q) line, then the 4x4 derivative
-        for (int idx = threadIdx.x; idx < 2 * N * (T + 1); idx += blockDim.x) {
-            const int col = idx % (T + 1), aq = idx / (T + 1), axis = aq / N, q = aq % N;
+        for (int idx = threadIdx.x; idx < 2 * N * ncol; idx += blockDim.x) {
+            const int col = col0 + idx % ncol, aq = idx / ncol, axis = aq / N, q = aq % N;
             double rl[4], rr[4];
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -113,7 +116,7 @@ k_hdg_schur(const TF *__restrict__ aug, const double *__restrict__ fcache, const
 #pragma unroll
                     for (int w = 0; w < 4; ++w) s += rv[w] * G[sq * 16 + v * 4 + w];
                     const int row = side * FW + v * N + q;
-                    if (col < T) S[(size_t)cell * T * T + (size_t)row * T + col] = -s;
+                    if (col < T) S[(size_t)cell * T * T + (size_t)row * T + col] = (TS)(-s);
                     else cy[(size_t)cell * T + row] = s;
                 }
             }
@@ -122,8 +125,11 @@ k_hdg_schur(const TF *__restrict__ aug, const double *__restrict__ fcache, const
             for (int idx = threadIdx.x; idx < M * (T + 1); idx += blockDim.x) {
                 const int r = idx / (T + 1), c = idx % (T + 1);
                 const double val = (double)A[(size_t)r * LD + M + c];
-                if (c < T) X[(size_t)cell * M * T + (size_t)r * T + c] = val;
-                else y[(size_t)cell * M + r] = val;
+                if (c < T) {
+                    if (X) X[(size_t)cell * M * T + (size_t)r * T + c] = val;
+                } else {
+                    y[(size_t)cell * M + r] = val;
+                }
             }
     }
 }
@@ -141,8 +147,8 @@ __global__ void k_hdg_rhs(const double *__restrict__ cy, double *__restrict__ rh
 }
 
 // Face-block Jacobi blocks D + S_first[rs, rs] + S_next[rs', rs'] written row-major (fw x fw).
-template <int N, typename TF>
-__global__ void k_face_blocks(const double *__restrict__ S, const double *__restrict__ speeds,
+template <int N, typename TF, typename TS = double>
+__global__ void k_face_blocks(const TS *__restrict__ S, const double *__restrict__ speeds,
                               TF *__restrict__ pool, Basis1D b, Grid g) {
     constexpr int FW = NVAR * N, T = NFACES * FW;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -155,12 +161,57 @@ __global__ void k_face_blocks(const double *__restrict__ S, const double *__rest
         const int q = i % N;
         val = -face_weight(g, b, face, q) * (speeds[2 * (face * N + q)] + speeds[2 * (face * N + q) + 1]);
     }
-    val += S[(size_t)first * T * T + (size_t)(rs * FW + i) * T + rs * FW + j];
-    val += S[(size_t)next * T * T + (size_t)(rn * FW + i) * T + rn * FW + j];
+    val += (double)S[(size_t)first * T * T + (size_t)(rs * FW + i) * T + rs * FW + j];
+    val += (double)S[(size_t)next * T * T + (size_t)(rn * FW + i) * T + rn * FW + j];
     pool[idx] = (TF)val;
 }
 
 // Face-owned Schur apply: out_f = D_f l_f + S_first[rs rows] l(first) + S_next[rs' rows] l(next).
+template <int N>
+__global__ void __launch_bounds__(256)
+k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
+            double *__restrict__ out, Basis1D b, Grid g);
+// The same with FP32 Schur blocks (the FP32 condensation): 16-byte loads of four S values, FP64
+// products and accumulation, so the operator applied is exactly the stored FP32 S.
+template <int N>
+__global__ void __launch_bounds__(256)
+k_hdg_apply32(const float *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
+              double *__restrict__ out, Basis1D b, Grid g) {
+    constexpr int FW = NVAR * N, T = NFACES * FW, T4 = T / 4, PASSES = (T4 + 31) / 32;
+    __shared__ __align__(16) double loc[2][T];
+    const int face = blockIdx.x;
+    const int axis = face >= g.cells, first = face - axis * g.cells, next = neighbor(g, first, 2 * axis + 1);
+    for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
+        const int which = k / T, s = (k % T) / FW, j = k % FW;
+        const int cell = which ? next : first;
+        loc[which][k % T] = lam[(size_t)face_of(g, cell, s) * FW + j];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int row = warp; row < FW; row += 8) {
+        // rows of S_K are T = 16N floats (a multiple of four), so every row starts 16-byte aligned
+        const float4 *s1 = reinterpret_cast<const float4 *>(S + (size_t)first * T * T + (size_t)((2 * axis + 1) * FW + row) * T);
+        const float4 *s2 = reinterpret_cast<const float4 *>(S + (size_t)next * T * T + (size_t)((2 * axis) * FW + row) * T);
+        double acc = 0;
+#pragma unroll
+        for (int t = 0; t < PASSES; ++t) {
+            const int j = lane + 32 * t;
+            if (j < T4) {
+                const float4 a = s1[j], c = s2[j];
+                const double *x = loc[0] + 4 * j, *y = loc[1] + 4 * j;
+                acc += (double)a.x * x[0] + (double)a.y * x[1] + (double)a.z * x[2] + (double)a.w * x[3];
+                acc += (double)c.x * y[0] + (double)c.y * y[1] + (double)c.z * y[2] + (double)c.w * y[3];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            const int q = row % N;
+            const double d = -face_weight(g, b, face, q) * (speeds[2 * (face * N + q)] + speeds[2 * (face * N + q) + 1]);
+            out[(size_t)face * FW + row] = d * lam[(size_t)face * FW + row] + acc;
+        }
+    }
+}
 template <int N>
 __global__ void __launch_bounds__(256)
 k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
@@ -220,6 +271,30 @@ k_hdg_recover(const double *__restrict__ X, const double *__restrict__ y, const 
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) du[(size_t)cell * M + r] = -acc - y[(size_t)cell * M + r];
     }
+}
+
+// q = -B lambda per cell: the trace coupling column of the condensed cell system
+// (hybrid.cpp:35-43: B's column (side, v, q) holds -w tau shape_i at the face line of side),
+// so that A^{-1} q - y = -X lambda - y is the recovery of hybrid.cpp:97-105 without X.
+template <int N>
+__global__ void k_hdg_bmul(const double *__restrict__ lam, const double *__restrict__ speeds, double *__restrict__ out,
+                           Basis1D b, Grid g) {
+    constexpr int P = N * N, FW = NVAR * N;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)g.cells * P) return;
+    const int cell = idx / P, node = idx % P, ix = node % N, iy = node / N;
+    double acc[4] = {0, 0, 0, 0};
+    for (int side = 0; side < NFACES; ++side) {
+        const int face = face_of(g, cell, side);
+        const int q = side < 2 ? iy : ix, i = side < 2 ? ix : iy;
+        const double ei = (side % 2 ? b.eR : b.eL)[i];
+        const double tau = speeds[2 * (face * N + q) + (side % 2 ? 0 : 1)];
+        const double stab = face_weight(g, b, face, q) * tau;
+#pragma unroll
+        for (int v = 0; v < NVAR; ++v) acc[v] += stab * ei * lam[(size_t)face * FW + v * N + q];
+    }
+#pragma unroll
+    for (int v = 0; v < NVAR; ++v) out[(size_t)cell * NVAR * P + v * P + node] = acc[v];
 }
 
 // DG residual implied by the Schur error e: -B D^{-1} e lifted into each cell (hybrid.cpp:106-121).

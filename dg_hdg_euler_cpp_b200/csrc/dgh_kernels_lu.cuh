@@ -232,12 +232,14 @@ __device__ __forceinline__ void trailing_dmma(double *__restrict__ A, int ld, in
 // right of the panel are read through the panel's row permutation when its U12 tile and the
 // trailing rows are formed (a row moved by the panel's pivoting comes from the panel's top
 // rows, which are written only after the trailing update, so the gather is race-free), and the
-// L columns of earlier panels are permuted once at the end (lfix, skipped for the augmented
-// HDG matrices, whose L factor is not needed after the forward elimination).
+// L columns of earlier panels are permuted once at the end (the L fix-up, flag bit 1; the FP64
+// augmented HDG matrices skip it, as their L factor is not needed after the forward
+// elimination, while the FP32 condensation keeps its factors for later solves).  Flag bit 0
+// converts the factored block in place to the slab layout of k_lu_solve (ld == m only).
 template <typename T, int NB, int TC>
 __global__ void __launch_bounds__(LU_THREADS)
 k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restrict__ perm_out, int *status,
-     int singular_bit, int slab_out) {
+     int singular_bit, int flags) {
     constexpr int PP = NB + 1;
     static_assert(LU_THREADS % TC == 0 && NB % (LU_THREADS / TC) == 0, "tile shape");
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -314,7 +316,7 @@ k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restr
         }
         // ---- L fix-up: panel q's L rows were written in the arrangement after panel q; gather
         // them into the final arrangement (piv) through the inverse arrangement of that time.
-        if (slab_out) {
+        if (flags & 2) {
             for (int i = tid; i < m; i += LU_THREADS) {
                 src[i] = i;  // arrangement: position -> original row
                 inv[i] = i;  // original row -> position
@@ -349,7 +351,7 @@ k_lu(T *__restrict__ pool, size_t stride, int m, int ld, int count, int *__restr
         __syncthreads();
         if (tid == 0 && bad) atomicOr(status, singular_bit);
         // ---- in-place conversion to the slab layout read by k_lu_solve (ld == m only)
-        if (slab_out) {
+        if (flags & 1) {
             constexpr int W = SlabVec<T>::W;
             for (int r0 = 0; r0 < m; r0 += 32) {
                 const int nt = min(32, m - r0);
@@ -797,6 +799,33 @@ k_lu_solve_t(const T *__restrict__ pool, const int *__restrict__ perm, size_t st
         for (int i = lane; i < m; i += 32) z[(size_t)blk * m + pm[i]] = (double)y[i];
         __syncwarp();
     }
+}
+
+// y = (float) x, elementwise (grid-stride).
+__global__ void k_round(const double *__restrict__ x, float *__restrict__ y, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
+}
+
+// Copy of the factored m x m part of each augmented matrix (row length ld) into the slab
+// layout of k_lu_solve (a pool of m x m blocks): one warp per 32-row slab, 16-byte stores.
+template <typename T>
+__global__ void k_slab_pack(const T *__restrict__ src, size_t stride, int m, int ld, int count, T *__restrict__ dst) {
+    constexpr int W = SlabVec<T>::W;
+    const int slabs = (m + 31) / 32, lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= (long long)count * slabs) return;
+    const int blk = (int)(warp / slabs), s = (int)(warp % slabs), r0 = 32 * s, nt = min(32, m - r0);
+    const T *A = src + (size_t)blk * stride + (size_t)r0 * ld;
+    T *out = dst + (size_t)blk * m * m + (size_t)r0 * m;
+    for (int g = 0; g < m / W; ++g)
+        if (lane < nt) {
+            typename SlabVec<T>::V v;
+            T *e = reinterpret_cast<T *>(&v);
+#pragma unroll
+            for (int w = 0; w < W; ++w) e[w] = A[(size_t)lane * ld + g * W + w];
+            *reinterpret_cast<typename SlabVec<T>::V *>(out + (size_t)g * nt * W + lane * W) = v;
+        }
 }
 
 // Multi-RHS back substitution U X = Y in place on columns [m, ld) of each factored matrix.

@@ -36,6 +36,8 @@ struct dgh_integrator {
     int stage = 0, steps_done = 0, stages = 1;
     bool residual_ready = false;
     dgh_run_stats run{};
+    // the reference's fixed limits (time_integrator.cpp:130,165): Schur attempts, line-search halvings
+    int hdg_attempts = 4, line_search = 30;
     // discrete adjoint: recorded trajectory (dt per step, frozen speeds per stage, checkpoints)
     struct Adjoint {
         int steps = 0, every = 0, stages = 0;
@@ -92,13 +94,49 @@ struct dgh_integrator {
             ck(dgh_gmres(ctx, DGH_OP_DG, rhs, direction, cfg.max_linear, cfg.linear_tolerance, &iterations, &relative));
             const double *res = dgh_gmres_residual(ctx, DGH_OP_DG);
             ck(dgh_axpby(ctx, -1., res, 0., res, eq_err, N));
+        } else if (cfg.condense32) {
+            // FP32 condensation: the condensed system approximates the DG linearisation to FP32
+            // accuracy, so J du = -r is solved by iterative refinement in FP64.  Each pass solves
+            // the Schur system for the current DG residual, recovers the correction with the kept
+            // FP32 cell factors, adds it, and forms the true residual e = J du + r with the FP64
+            // J*v; the next pass retargets the condensation to e.  A pass's Schur tolerance goes
+            // no lower than the estimated FP32 floor of one pass (below it GMRES iterations buy
+            // nothing) nor than what the acceptance target still needs.
+            ck(dgh_hdg_refresh_projected(ctx, state, residual));
+            ck(dgh_hdg_rhs(ctx, rhs));
+            ck(dgh_block_jacobi_refresh(ctx, DGH_OP_HDG));
+            double floor_est = 1e-6, current = norm;
+            bool valid = false;
+            for (int pass = 0; pass < 2 * hdg_attempts && !valid; ++pass) {
+                const double tolerance = std::max({cfg.linear_tolerance, floor_est, .3 * target / current});
+                int cur = 0;
+                double rel = 0;
+                ck(dgh_gmres(ctx, DGH_OP_HDG, rhs, tdir, cfg.max_linear, tolerance, &cur, &rel));
+                iterations += cur;
+                relative = rel;
+                ck(dgh_hdg_recover(ctx, tdir, pass == 0 ? direction : indep));
+                if (pass > 0) ck(dgh_axpby(ctx, 1., direction, 1., indep, direction, N));
+                ck(dgh_dg_apply(ctx, direction, eq_err));
+                ck(dgh_axpby(ctx, 1., eq_err, 1., residual, eq_err, N));
+                const double next = dual(eq_err);
+                if (next <= target) {
+                    valid = true;
+                } else {
+                    const double achieved = next / current;
+                    if (achieved > 10 * tolerance) floor_est = std::min(.1, achieved);
+                    current = next;
+                    ck(dgh_hdg_retarget(ctx, eq_err));
+                    ck(dgh_hdg_rhs(ctx, rhs));
+                }
+            }
+            if (!valid) throw Failure{DGH_ERR_SOLVER, "Recovered DG residual criterion failed after Schur refinement"};
         } else {
             ck(dgh_hdg_refresh_projected(ctx, state, residual));
             ck(dgh_hdg_rhs(ctx, rhs));
             ck(dgh_block_jacobi_refresh(ctx, DGH_OP_HDG));
             double tolerance = cfg.linear_tolerance;
             bool valid = false;
-            for (int attempt = 0; attempt < 4; ++attempt) {
+            for (int attempt = 0; attempt < hdg_attempts; ++attempt) {
                 int cur = 0;
                 double rel = 0;
                 ck(dgh_gmres(ctx, DGH_OP_HDG, rhs, tdir, cfg.max_linear, tolerance, &cur, &rel));
@@ -129,7 +167,7 @@ struct dgh_integrator {
         }
         double damping = 1.;
         bool accepted = false;
-        for (int search = 0; search < 30; ++search) {
+        for (int search = 0; search < line_search; ++search) {
             ck(dgh_axpby(ctx, 1., state, damping, direction, trial, N));
             int ok = 0;
             ck(dgh_admissible(ctx, trial, &ok));
@@ -221,6 +259,13 @@ int dgh_integrator_destroy(dgh_integrator *it) {
 }
 
 double *dgh_integrator_state(dgh_integrator *it) { return it ? it->state : nullptr; }
+
+int dgh_integrator_set_limits(dgh_integrator *it, int hdg_attempts, int line_search) {
+    if (!it || hdg_attempts < 0 || line_search < 0) return DGH_ERR_INVALID;
+    it->hdg_attempts = hdg_attempts;
+    it->line_search = line_search;
+    return DGH_OK;
+}
 
 // time_integrator.cpp:48-213 (the full run).  The integrator reads its configuration from the
 // context it was created on.

@@ -232,6 +232,10 @@ class Solver:
         self._call("dgh_hdg_recover", _ptr(dlam), _ptr(out))
         return out
 
+    def hdg_retarget(self, r):
+        """Retarget the FP32-condensed system to volume residual r (dgh_hdg_retarget)."""
+        self._call("dgh_hdg_retarget", _ptr(r))
+
     def hdg_recovered_residual(self, e):
         out = self.vec()
         self._call("dgh_hdg_recovered_residual", _ptr(e), _ptr(out))
@@ -308,9 +312,65 @@ class Integrator:
     def state_ptr(self) -> int:
         return int(self.lib.dgh_integrator_state(self.h))
 
+    def set_limits(self, hdg_attempts: int = 4, line_search: int = 30):
+        """Override the Schur attempts and Armijo halvings (dgh_integrator_set_limits)."""
+        self._rc(self.lib.dgh_integrator_set_limits(self.h, hdg_attempts, line_search))
+
     def close(self):
         if self.h:
             self.lib.dgh_integrator_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BlockJacobi:
+    """A standalone pool of dense blocks factored on the device (BlockJacobi,
+    block_jacobi.hpp:7-47): factor(blocks) with one of the LU kernels, apply(x) = A^{-1} x per
+    block.  variant 0 left-looking FP64 tensor-pipe LU, 1 right-looking blocked LU, 2 one-warp LU
+    (m <= 64), 3 FP64 LU with FP32 explicit inverses (m <= 64, mixed)."""
+
+    def __init__(self, m: int, count: int, precision: str = "fp64", variant: int = 0, device: int = 0):
+        import torch
+
+        self.torch = torch
+        self.lib = _lib.load()
+        self.m, self.count = m, count
+        self.device = torch.device("cuda", device)
+        h = ctypes.c_void_p()
+        rc = self.lib.dgh_block_jacobi_create(m, count, PRECISIONS[precision], variant, device, ctypes.byref(h))
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_block_jacobi_error(None).decode())
+        self.h = h
+
+    def _rc(self, rc):
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_block_jacobi_error(self.h).decode())
+
+    def factor(self, blocks: np.ndarray):
+        b = self.torch.as_tensor(np.ascontiguousarray(blocks, dtype=np.float64).reshape(-1), device=self.device)
+        self.torch.cuda.synchronize(self.device)
+        self._rc(self.lib.dgh_block_jacobi_factor(self.h, _ptr(b)))
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        xt = self.torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device=self.device)
+        z = self.torch.zeros_like(xt)
+        self.torch.cuda.synchronize(self.device)
+        self._rc(self.lib.dgh_block_jacobi_apply(self.h, _ptr(xt), _ptr(z)))
+        return z.cpu().numpy()
+
+    def perm(self) -> np.ndarray:
+        out = np.zeros(self.m * self.count, dtype=np.int32)
+        self._rc(self.lib.dgh_block_jacobi_perm(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return out.reshape(self.count, self.m)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dgh_block_jacobi_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -75,6 +75,7 @@ typedef struct dgh_config {
     int autotune;     /* 2D: time the factorisation variants on the first refresh (per degree) */
     int preconditioner; /* 0 block Jacobi; 1 block ILU(0), natural ordering (1D only,        */
                         /* common/src/linalg/block_ilu.cpp:15-84)                            */
+    int condense32;     /* 2D HDG: 1 = FP32 condensation (see dgh_hdg_retarget); 0 = FP64     */
 } dgh_config;
 
 /* config.hpp:7-18 defaults: nx=ny=8, k=3, restart 30, max_linear 1500, max_newton 30,
@@ -170,6 +171,18 @@ int dgh_hdg_apply(dgh_ctx *ctx, const double *lambda, double *out); /* hybrid.cp
 int dgh_hdg_block(dgh_ctx *ctx, int row, int col, double *host_block); /* hybrid.cpp:83-96, row == col */
 int dgh_hdg_recover(dgh_ctx *ctx, const double *dlambda, double *du); /* hybrid.cpp:97-105 */
 int dgh_hdg_recovered_residual(dgh_ctx *ctx, const double *e, double *out); /* hybrid.cpp:106-121 */
+/* FP32 condensation (dgh_config.condense32 = 1; no counterpart in the reference, whose
+ * condensation is FP64: hybrid.cpp:56-72).  dgh_hdg_refresh_projected then factors every cell
+ * matrix A_K in FP32 with FP32 accumulation, keeps those factors, and stores the Schur blocks
+ * S_K = -C A_K^{-1} B in FP32 (no X is stored); the Schur apply reads the FP32 blocks with FP64
+ * products, and dgh_hdg_recover computes A_K^{-1}(-B dlambda) - y with the kept factors.  The
+ * condensed system then approximates the DG linearisation to FP32 accuracy, so the integrator
+ * solves the DG Newton system by iterative refinement: after each Schur solve and recovery it
+ * forms the true DG residual e = J du + r with the FP64 J*v, and retargets the condensed system
+ * to e for the next correction, until the reference's acceptance target holds.
+ * dgh_hdg_retarget: y = A_K^{-1} r per cell with the kept factors, C y, and the condensed
+ * right-hand side for volume residual r (dgh_hdg_rhs returns it); the factors and S are reused. */
+int dgh_hdg_retarget(dgh_ctx *ctx, const double *r);
 
 /* ---- GMRES (gmres.cpp:17-86) ---------------------------------------------------------------- */
 /* Right-preconditioned restarted GMRES(restart) with CGS2 in the M^-1 (DG) or inverse trace
@@ -227,6 +240,30 @@ int dgh_newton_update(dgh_integrator *it, dgh_update_stats *stats);
 int dgh_newton_update_host(dgh_integrator *it, double *host_state, dgh_update_stats *stats);
 /* Device pointer to the integrator's current Newton state (size dgh_sizes()[0]). */
 double *dgh_integrator_state(dgh_integrator *it);
+/* Overrides the reference's fixed limits: the HDG Schur-tolerance attempts (4,
+ * time_integrator.cpp:130-149) and the Armijo halvings (30, time_integrator.cpp:165-176).  Lower
+ * limits make the failure paths ("Recovered DG residual criterion failed after Schur
+ * refinement", "Newton line search failed") reachable from ordinary inputs, for tests. */
+int dgh_integrator_set_limits(dgh_integrator *it, int hdg_attempts, int line_search);
+
+/* ---- Standalone block Jacobi (BlockJacobi, common/include/euler/linalg/block_jacobi.hpp:7-47) ----
+ * `count` dense m x m blocks (m a multiple of 4, at most 512) factored with row partial pivoting
+ * (the first largest |a| wins ties, as LAPACK getrf / Eigen PartialPivLU) by one device LU kernel,
+ * then applied as z = A^{-1} x block by block (block_jacobi.hpp:24-39).  blocks, x and z are device
+ * pointers; blocks are row-major FP64 and are copied (the caller keeps them).  variant: 0 the
+ * left-looking FP64 LU on the tensor pipe, 1 the right-looking blocked LU, 2 the one-warp LU for
+ * narrow blocks (m <= 64), 3 FP64 LU with explicit inverses stored in FP32 (m <= 64, mixed only).
+ * precision DGH_PRECISION_MIXED stores the factors in FP32 (variant 1 and 2 factor in FP32).  A
+ * block with a zero, subnormal or non-finite pivot fails with DGH_ERR_SINGULAR ("Singular block
+ * Jacobi factor", block_jacobi.hpp:16-18).  dgh_block_jacobi_perm copies the row permutation
+ * (position i of block b holds original row perm[b m + i]). */
+typedef struct dgh_block_jacobi dgh_block_jacobi;
+int dgh_block_jacobi_create(int m, int count, int precision, int variant, int device, dgh_block_jacobi **out);
+int dgh_block_jacobi_destroy(dgh_block_jacobi *bj);
+const char *dgh_block_jacobi_error(const dgh_block_jacobi *bj);
+int dgh_block_jacobi_factor(dgh_block_jacobi *bj, const double *blocks);
+int dgh_block_jacobi_apply(dgh_block_jacobi *bj, const double *x, double *z);
+int dgh_block_jacobi_perm(const dgh_block_jacobi *bj, int *host_perm);
 
 /* ---- Batched uneven problems (no counterpart in the reference) ---------------------------------
  * Independent member problems, each with its own dgh_config (mesh, degree, method DG or HDG,
