@@ -48,6 +48,8 @@ FORMS = {
     "fp64": ("fp64", 0, "FP64 everywhere"),
     "mixed": ("mixed", 0, "FP32 block-Jacobi factors and solves"),
     "mixed32": ("mixed", 1, "FP32 block-Jacobi factors and FP32 HDG condensation with FP64 refinement"),
+    "mixed16": ("mixed16", 0, "DG cell factors stored in FP16 with per-row scales, solved in FP32 (below the "
+                              "FP32 the task names: an extra form)"),
 }
 
 
@@ -161,6 +163,8 @@ def allmax(pg, torch, value: float) -> float:
 # ------------------------------------------------------------------------------ our arm
 def algorithmic_bytes(kind: str, m: int, cells: int, fw: int, faces: int, t: int, precision: str) -> float:
     """Bytes one launch of the dominant kernel must move (factors read once, rhs and result)."""
+    if kind == "dg" and precision == "mixed16":  # FP16 slabs (rows padded to 8), perm, row scales, rhs, result
+        return cells * (m * ((m + 7) // 8 * 8) * 2 + m * 4 + m * 4 + 2 * m * 8)
     s = 8 if precision == "fp64" else 4
     if kind == "dg":  # k_lu_solve over E blocks: m^2 factors, m perm ints, rhs and result
         return cells * (m * m * s + m * 4 + 2 * m * 8)
@@ -272,8 +276,9 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
     if method == "dg":
         kb = algorithmic_bytes("dg", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
         tk = kernel_timers["precond"]
-        kernel = "k_lu_solve<%s> (block-Jacobi solve, one launch per Krylov iteration)" % (
-            "double" if precision == "fp64" else "float")
+        kernel = ("k_lu_solve_half (block-Jacobi solve from FP16 slabs" if precision == "mixed16" else
+                  "k_lu_solve<%s> (block-Jacobi solve" % ("double" if precision == "fp64" else "float")) + \
+            ", one launch per Krylov iteration)"
     else:
         kb = algorithmic_bytes("hdg_schur", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
         tk = kernel_timers["operator"]

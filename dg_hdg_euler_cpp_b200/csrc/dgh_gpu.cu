@@ -204,7 +204,9 @@ struct dgh_ctx {
         ck(cudaGetLastError(), "kernel launch");
     }
     void sync() { ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
-    bool mixed() const { return cfg.precision == DGH_PRECISION_MIXED; }
+    bool mixed() const { return cfg.precision != DGH_PRECISION_FP64; }
+    bool half16() const { return cfg.precision == DGH_PRECISION_MIXED16; }
+    float *dg_scale = nullptr;  // FP16 DG factors: per-row reciprocal scales of U
     bool d1() const { return dim == 1; }
     bool overint() const { return dim == 2 && Q > n; }
     bool has_dg() const { return cfg.method == DGH_METHOD_DG || cfg.method == DGH_METHOD_BOTH; }
@@ -410,6 +412,19 @@ void launch_solve_t(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, 
     c->launched();
 }
 
+// The DG cell blocks from their FP16 slabs (one warp per block, like launch_solve).
+void launch_solve_half(dgh_ctx *c, const double *x, double *z) {
+    constexpr int wpc = SOLVE_THREADS / 32;
+    const size_t smem = sizeof(float) * (size_t)pad8(c->m) * wpc;
+    const int want = (c->cells + wpc - 1) / wpc;
+    int resident = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve_half, SOLVE_THREADS, smem), "occupancy");
+    const int grid = std::min(want, c->sms * std::max(1, resident));
+    k_lu_solve_half<<<grid, SOLVE_THREADS, smem, c->stream>>>((const __half *)c->dg_pool, c->dg_scale, c->dg_perm, c->m,
+                                                               c->cells, x, z);
+    c->launched();
+}
+
 // 1D blocks (m <= 27 and 3 x 3): one warp per block, four warps per CTA.
 template <typename TF>
 void launch_small_lu(dgh_ctx *c, TF *pool, size_t stride, int m, int ld, int count, int *perm, bool backsolve) {
@@ -452,6 +467,7 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     if (op == DGH_OP_DG_T) {
         need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->m * c->m;
+        need(!c->half16(), "The transposed solve needs FP64 or FP32 factors");
         if (c->mixed()) launch_solve_t<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
         else launch_solve_t<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
         return;
@@ -459,7 +475,8 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     if (op == DGH_OP_DG) {
         need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->m * c->m;
-        if (c->mixed()) launch_solve<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+        if (c->half16()) launch_solve_half(c, x, z);
+        else if (c->mixed()) launch_solve<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
         else launch_solve<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
     } else {
         need(c->face_factored, "Refresh the block-Jacobi preconditioner before applying it");
@@ -1055,7 +1072,8 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
              "Invalid solver tolerance or wave-speed safety");
         need(k.method >= 0 && k.method <= 2, "Method must be dg, hdg, or both");
         need(k.dim == 1 || (k.testcase >= 0 && k.testcase <= 2), "Invalid testcase");
-        need(k.precision == 0 || k.precision == 1, "Invalid precision");
+        need(k.precision >= 0 && k.precision <= 2, "Invalid precision");
+        need(k.precision != DGH_PRECISION_MIXED16 || k.dim == 2, "FP16 factor storage is a 2D option");
         need(k.restart <= KR_MAXK - 1, "restart must be at most 31 on the device GMRES");
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(DGH_ERR_CUDA, "no CUDA device available");
@@ -1183,7 +1201,12 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->launched(2);
         const size_t tsz = c->mixed() ? sizeof(float) : sizeof(double);
         if (c->has_dg()) {
-            c->dg_pool = c->alloc<char>((size_t)c->cells * c->m * c->m * tsz);
+            if (c->half16()) {
+                c->dg_pool = c->alloc<char>((size_t)c->cells * c->m * pad8(c->m) * sizeof(__half));
+                c->dg_scale = c->alloc<float>((size_t)c->cells * c->m);
+            } else {
+                c->dg_pool = c->alloc<char>((size_t)c->cells * c->m * c->m * tsz);
+            }
             c->dg_perm = c->alloc<int>((size_t)c->cells * c->m);
         }
         if (c->has_hdg()) {
@@ -1660,6 +1683,28 @@ std::map<std::tuple<int, int, int>, int> g_tune_cache;  // (kind, n, precision) 
 void dg_factor(dgh_ctx *c, int variant, int first, int count) {
     const size_t stride = (size_t)c->m * c->m;
     const int grid = std::min(count, c->sms * 8);
+    if (c->half16()) {  // FP64 left-looking in the workspace, then FP16 slabs with row scales
+        const int mp = pad8(c->m);
+        for (int f = first; f < first + count; f += c->dg_ws_cells) {
+            const int cnt = std::min(c->dg_ws_cells, first + count - f);
+            DGH_DISPATCH_N(c->n, {
+                k_dg_assemble<N, double><<<std::min(cnt, c->sms * 8), 256, 0, c->stream>>>(
+                    c->dg_ws, c->vol, c->fcache, c->speeds, c->basis, c->g, c->inv_step, f, cnt, c->overint() ? 0 : 1);
+                if (c->overint()) {
+                    k_vol_block_q<N, double><<<std::min(cnt, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                        c->dg_ws, c->m, c->volq, c->bq, c->g, f, cnt);
+                    c->launched();
+                }
+            });
+            c->launched();
+            launch_lu_left<false>(c, c->dg_ws, stride, c->m, c->m, cnt, c->dg_perm + (size_t)f * c->m, ST_SINGULAR, false);
+            const long long warps = (long long)cnt * ((c->m + 31) / 32);
+            k_pack_half<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, c->stream>>>(
+                c->dg_ws, c->m, cnt, (__half *)c->dg_pool + (size_t)f * c->m * mp, c->dg_scale + (size_t)f * c->m);
+            c->launched();
+        }
+        return;
+    }
     if (c->mixed()) {
         if (variant == 0) {  // FP64 left-looking in the workspace, FP32 slabs out, chunked
             for (int f = first; f < first + count; f += c->dg_ws_cells) {
@@ -1885,6 +1930,7 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
         if (op == DGH_OP_DG) {
             need(c->dg_pool, "context has no DG operator");
             need(c->linearised, "Refresh the volume Jacobian before assembling a block");
+            if (c->dg_variant < 0 && c->half16()) c->dg_variant = 0;  // one factorisation form
             if (c->dg_variant < 0) {
                 const int sample = std::min(c->cells, std::max(c->lu_grid, 1) * 4);
                 c->dg_variant = tuned_variant(c, 0, [&](int v) { dg_factor(c, v, 0, sample); }, c->tune_ms);

@@ -10,6 +10,8 @@
 #pragma once
 #include "dgh_common.cuh"
 
+#include <cuda_fp16.h>
+
 namespace dgh {
 
 template <typename T> __device__ inline T tabs(T x) { return x < T(0) ? -x : x; }
@@ -703,6 +705,122 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
                         const T u = (act && lane <= jj) ? S[slab_at<T>(nt, lane, r0 + jj)] : T(1);
                         if (lane == jj) t = t / u;
                         const T yj = __shfl_sync(0xffffffffu, t, jj);
+                        if (lane < jj) t -= u * yj;
+                    }
+                }
+                if (act) y[r0 + lane] = t;
+                __syncwarp();
+            }
+        }
+        for (int i = lane; i < m; i += 32) z[(size_t)blk * m + i] = (double)y[i];
+        __syncwarp();
+    }
+}
+
+// ---- 16-bit factor storage (the DG cell blocks, DGH_PRECISION_MIXED16) -------------------------
+// FP16 slabs with 8 columns per 16-byte group and rows padded to mp = m rounded up to 8 (zeros
+// past column m): element (32 s + i, j) at 32 s mp + (j / 8) nt 8 + 8 i + j % 8.  The strictly
+// lower part holds L (|L| <= 1 under partial pivoting); each row's upper part U(i, i..m-1) is
+// stored divided by that row's largest |U(i, j)|, whose reciprocal is kept as an FP32 row scale,
+// so every stored U row peaks at 1 and stays in FP16's normal range.
+constexpr int H_W = 8;
+__host__ __device__ constexpr int pad8(int m) { return (m + 7) / 8 * 8; }
+
+// Packs row-major factored FP64 blocks (LU in place, row length m, rows in position order) into
+// the FP16 slabs and row scales: one warp per 32-row slab of a block, lane i owning row 32 s + i.
+__global__ void k_pack_half(const double *__restrict__ src, int m, int count, __half *__restrict__ dst,
+                            float *__restrict__ row_scale) {
+    const int mp = pad8(m), slabs = (m + 31) / 32, lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= (long long)count * slabs) return;
+    const int blk = (int)(warp / slabs), s = (int)(warp % slabs), r0 = 32 * s, nt = min(32, m - r0);
+    if (lane >= nt) return;
+    const int row = r0 + lane;
+    const double *ar = src + (size_t)blk * m * m + (size_t)row * m;
+    __half *out = dst + (size_t)blk * m * mp + (size_t)r0 * mp;
+    double big = 0;
+    for (int j = row; j < m; ++j) big = fmax(big, fabs(ar[j]));
+    const double inv = big > 0 ? 1. / big : 1.;
+    row_scale[(size_t)blk * m + row] = (float)inv;
+    for (int g = 0; g < mp / H_W; ++g) {
+        __align__(16) __half v[H_W];
+#pragma unroll
+        for (int w = 0; w < H_W; ++w) {
+            const int j = g * H_W + w;
+            const double a = j < m ? ar[j] : 0.;
+            v[w] = __double2half(j >= row ? a * inv : a);
+        }
+        *reinterpret_cast<uint4 *>(out + (size_t)g * nt * H_W + lane * H_W) = *reinterpret_cast<const uint4 *>(v);
+    }
+}
+
+// z = A^{-1} b per block from the FP16 slabs: k_lu_solve's structure (one warp per block, lane
+// i owns row 32 s + i, four 16-byte loads in flight, shuffled diagonal triangles) with FP32
+// arithmetic; the backward sweep multiplies each row's right-hand side by its row scale.
+__global__ void __launch_bounds__(SOLVE_THREADS, 5)
+k_lu_solve_half(const __half *__restrict__ pool, const float *__restrict__ row_scale, const int *__restrict__ perm,
+                int m, int count, const double *__restrict__ rhs, double *__restrict__ z) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int mp = pad8(m), lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    float *y = reinterpret_cast<float *>(smraw) + (size_t)wib * mp;
+    const float4 *yv = reinterpret_cast<const float4 *>(y);
+    const int warps = gridDim.x * (SOLVE_THREADS / 32);
+    const int slabs = (m + 31) / 32;
+    auto dot8 = [&](const uint4 &a, int g) {
+        const __half2 *h = reinterpret_cast<const __half2 *>(&a);
+        const float4 y0 = yv[2 * g], y1 = yv[2 * g + 1];
+        const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]);
+        const float2 f2 = __half22float2(h[2]), f3 = __half22float2(h[3]);
+        return (f0.x * y0.x + f0.y * y0.y) + (f1.x * y0.z + f1.y * y0.w) + (f2.x * y1.x + f2.y * y1.y) +
+               (f3.x * y1.z + f3.y * y1.w);
+    };
+    for (int blk = blockIdx.x * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
+        const __half *A = pool + (size_t)blk * m * mp;
+        const int *pm = perm + (size_t)blk * m;
+        const float *rs = row_scale + (size_t)blk * m;
+        const double *b = rhs + (size_t)blk * m;
+        for (int i = lane; i < mp; i += 32) y[i] = i < m ? (float)b[pm[i]] : 0.f;
+        __syncwarp();
+        for (int dir = 0; dir < 2; ++dir) {
+            for (int si = 0; si < slabs; ++si) {
+                const int s = dir == 0 ? si : slabs - 1 - si;
+                const int r0 = 32 * s, nt = min(32, m - r0), hi = r0 + nt;
+                const __half *S = A + (size_t)r0 * mp;
+                const uint4 *Sv = reinterpret_cast<const uint4 *>(S);
+                const bool act = lane < nt;
+                float acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+                if (act) {
+                    // forward: the groups left of the slab; backward: the groups right of it (the
+                    // last slab, whose end may fall inside a group, has none)
+                    const int g1 = dir == 0 ? r0 / H_W : mp / H_W;
+                    int g = dir == 0 ? 0 : (hi >= m ? mp / H_W : hi / H_W);
+                    for (; g + 4 <= g1; g += 4) {
+                        const uint4 a0 = Sv[(size_t)g * nt + lane], a1 = Sv[(size_t)(g + 1) * nt + lane];
+                        const uint4 a2 = Sv[(size_t)(g + 2) * nt + lane], a3 = Sv[(size_t)(g + 3) * nt + lane];
+                        acc0 += dot8(a0, g);
+                        acc1 += dot8(a1, g + 1);
+                        acc2 += dot8(a2, g + 2);
+                        acc3 += dot8(a3, g + 3);
+                    }
+                    for (; g < g1; ++g) acc0 += dot8(Sv[(size_t)g * nt + lane], g);
+                }
+                float t = 0.f;
+                if (act) t = (dir == 0 ? y[r0 + lane] : y[r0 + lane] * rs[r0 + lane]) - ((acc0 + acc1) + (acc2 + acc3));
+                auto at = [&](int jj) {  // stored entry (row r0 + lane, column r0 + jj)
+                    const int j = r0 + jj;
+                    return __half2float(S[(size_t)(j / H_W) * nt * H_W + lane * H_W + j % H_W]);
+                };
+                if (dir == 0) {
+                    for (int jj = 0; jj < nt; ++jj) {
+                        const float l = (act && lane > jj) ? at(jj) : 0.f;
+                        const float yj = __shfl_sync(0xffffffffu, t, jj);
+                        t -= l * yj;
+                    }
+                } else {
+                    for (int jj = nt - 1; jj >= 0; --jj) {
+                        const float u = (act && lane <= jj) ? at(jj) : 1.f;
+                        if (lane == jj) t = t / u;
+                        const float yj = __shfl_sync(0xffffffffu, t, jj);
                         if (lane < jj) t -= u * yj;
                     }
                 }

@@ -1,7 +1,7 @@
 // dgh2d: command-line front end of the B200 solver, flag- and CSV-compatible with the
 // reference's dg_hdg_2d (its flags and their error texts: dg_hdg_2d/src/config.cpp:23-122; its
 // output files and columns: dg_hdg_2d/src/main.cpp:7-108).  Additional flags: --precision
-// fp64|mixed (block-Jacobi factor precision), --condensation fp64|fp32, --graph, --autotune and
+// fp64|mixed|mixed16 (block-Jacobi factor precision), --condensation fp64|fp32, --graph, --autotune and
 // --device N.
 #include "cli.hpp"
 
@@ -22,7 +22,7 @@ constexpr const char *kUsage =
     "--ordering natural --restart N --max-linear N --max-newton N\n"
     "--ntol R --ltol R --safety S --prefix PATH\n"
     "--integrator ssp-dirk3|be --newton-steps N --warmup-updates N\n"
-    "--graph --autotune --timing-only --check-update --no-save-solution --precision fp64|mixed\n"
+    "--graph --autotune --timing-only --check-update --no-save-solution --precision fp64|mixed|mixed16\n"
     "--condensation fp64|fp32 --device N\n";
 
 Settings settings_from(int argc, char **argv) {
@@ -54,7 +54,8 @@ Settings settings_from(int argc, char **argv) {
         text("--integrator", [&](const std::string &v) { integrator_word = v; }),
         text("--prefix", [&](const std::string &v) { s.prefix = v; }),
         text("--precision", [&](const std::string &v) {
-            c.precision = pick(v, {"fp64", "mixed"}, "Invalid precision") ? DGH_PRECISION_MIXED : DGH_PRECISION_FP64;
+            const int level = pick(v, {"fp64", "mixed", "mixed16"}, "Invalid precision");
+            c.precision = level == 2 ? DGH_PRECISION_MIXED16 : level == 1 ? DGH_PRECISION_MIXED : DGH_PRECISION_FP64;
         }),
         text("--condensation", [&](const std::string &v) {
             c.condense32 = pick(v, {"fp64", "fp32"}, "Invalid condensation precision");

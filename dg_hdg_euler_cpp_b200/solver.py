@@ -18,7 +18,7 @@ from . import _lib
 METHODS = {"dg": 0, "hdg": 1, "both": 2}
 INTEGRATORS = {"ssp-dirk3": 0, "be": 1}
 TESTCASES = {"diagonal": 0, "wave": 1, "axis": 2}
-PRECISIONS = {"fp64": 0, "mixed": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed16": 2}
 PRECONDITIONERS = {"block-jacobi": 0, "block-ilu0": 1}
 OPS = {"dg": 0, "hdg": 1, "dg_t": 2}
 

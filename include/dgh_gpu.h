@@ -49,9 +49,14 @@ typedef enum dgh_status {
 enum { DGH_METHOD_DG = 0, DGH_METHOD_HDG = 1, DGH_METHOD_BOTH = 2 };
 enum { DGH_INTEGRATOR_DIRK3 = 0, DGH_INTEGRATOR_BE = 1 };
 enum { DGH_TEST_DIAGONAL = 0, DGH_TEST_WAVE = 1, DGH_TEST_AXIS = 2 };
-/* Precision of the block-Jacobi factors and their solves.  Residuals, J*v, the Schur apply,
- * the HDG condensation, Arnoldi and the least-squares problem are always FP64. */
-enum { DGH_PRECISION_FP64 = 0, DGH_PRECISION_MIXED = 1 };
+/* Precision of the block-Jacobi factors and their solves.  Residuals, J*v, Arnoldi and the
+ * least-squares problem are always FP64 (the Schur apply and the condensation too, unless
+ * dgh_config.condense32).  MIXED: FP32 factors and solves.  MIXED16 (2D; no counterpart in the
+ * reference, and below the FP32 its mixed-precision plan names): the DG cell factors are computed
+ * in FP64 and stored in FP16, each row of U divided by its largest entry (the row scale kept in
+ * FP32), and solved in FP32; the HDG face blocks are as in MIXED.  The transposed solve
+ * (DGH_OP_DG_T) needs FP64 or FP32 factors. */
+enum { DGH_PRECISION_FP64 = 0, DGH_PRECISION_MIXED = 1, DGH_PRECISION_MIXED16 = 2 };
 /* Operators for the preconditioner and GMRES: the DG Jacobian J, the condensed Schur operator,
  * and the DG adjoint J^T (with the transposed block-Jacobi preconditioner). */
 enum { DGH_OP_DG = 0, DGH_OP_HDG = 1, DGH_OP_DG_T = 2 };

@@ -87,7 +87,7 @@ def test_256_initial_residual_and_dt(k):
 
 
 @pytest.mark.parametrize("method,precision", [("dg", "fp64"), ("hdg", "fp64"), ("dg", "mixed"), ("hdg", "mixed"),
-                                              ("hdg", "mixed32")])
+                                              ("hdg", "mixed32"), ("dg", "mixed16")])
 def test_256_k8_speed_protocol_all_updates(method, precision):
     """Full-size 256^2 k=8 BE CFL 5 (the speed configuration), all four Newton updates of the
     reference's speed protocol against its archived history: the residual rms at the start of
