@@ -29,7 +29,7 @@ class dgh_config(ctypes.Structure):
         ("method", ctypes.c_int), ("integrator", ctypes.c_int), ("testcase", ctypes.c_int),
         ("precision", ctypes.c_int), ("check_update", ctypes.c_int), ("device", ctypes.c_int),
         ("dim", ctypes.c_int), ("autotune", ctypes.c_int),
-        ("preconditioner", ctypes.c_int), ("condense32", ctypes.c_int),
+        ("preconditioner", ctypes.c_int), ("condense32", ctypes.c_int), ("forcing", ctypes.c_int),
     ]
 
 

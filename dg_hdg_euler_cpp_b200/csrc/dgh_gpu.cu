@@ -1054,6 +1054,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         need(k.preconditioner == 0 || k.preconditioner == 1, "Invalid block preconditioner");
         need(k.preconditioner == 0 || k.dim == 1, "2D currently supports block-jacobi only");
         need(k.condense32 == 0 || (k.condense32 == 1 && k.dim == 2), "FP32 condensation is a 2D HDG option (0 or 1)");
+        need(k.forcing == 0 || k.forcing == 1, "Invalid forcing (0 or 1)");
         // config.cpp:6-22 (dg_hdg_1d/src/config.cpp:6-21 in 1D)
         need(k.nx >= 3 && (k.dim == 1 || k.ny >= 3) && k.degree >= 0 && k.degree <= 8 && k.quadrature >= 0,
              "Invalid mesh or degree");
@@ -1791,10 +1792,42 @@ void hdg_condense_chunk(dgh_ctx *c, int variant, const double *r, int first, int
     });
     c->launched();
 }
-// FP32 condensation of cells [first, first + count) (count <= aug_cells): [A | B | r] assembled
-// in FP32, right-looking FP32 LU with FP32 accumulation (the L fix-up kept), the factors copied
-// to the cells' FP32 slabs for later solves, back substitution for X | y, then S = -C X stored in
-// FP32, y and C y in FP64.
+// Cells per chunk of the condensation workspace for augmented matrices of element type T.
+template <typename T> int aug_chunk(const dgh_ctx *c) {
+    return (int)std::max<size_t>(1, std::min<size_t>(c->cells, c->aug_bytes / ((size_t)c->m * (c->m + c->t + 1) *
+                                                                                 sizeof(T))));
+}
+// FP32-storage condensation of cells [first, first + count), variant 0: [A | B | r] assembled in
+// FP64, the left-looking LU on the FP64 tensor pipe with the fused right-hand-side solve, the
+// factors rounded into the cells' FP32 slabs, then S = -C X stored in FP32, y and C y in FP64.
+void hdg_condense_chunk32_tc(dgh_ctx *c, const double *r, int first, int count) {
+    const int ld = c->m + c->t + 1, grid = std::min(count, c->sms * 8);
+    const size_t stride = (size_t)c->m * ld;
+    DGH_DISPATCH_N(c->n, {
+        k_hdg_assemble<N, double><<<grid, 256, 0, c->stream>>>(c->aug, c->vol, c->fcache, c->speeds, r, c->basis, c->g,
+                                                               c->inv_step, first, count, c->overint() ? 0 : 1);
+        if (c->overint()) {
+            k_vol_block_q<N, double><<<std::min(count, c->sms * 4), Q_THREADS, 0, c->stream>>>(
+                c->aug, ld, c->volq, c->bq, c->g, first, count);
+            c->launched();
+        }
+    });
+    c->launched();
+    int *perm = c->lu32_perm + (size_t)first * c->m;
+    launch_lu_left<true>(c, c->aug, stride, c->m, ld, count, perm, ST_SINGULAR_HDG, false);
+    const long long warps = (long long)count * ((c->m + 31) / 32);
+    k_slab_pack<double, float><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, c->stream>>>(
+        c->aug, stride, c->m, ld, count, c->lu32 + (size_t)first * c->m * c->m, perm);
+    c->launched();
+    DGH_DISPATCH_N(c->n, {
+        k_hdg_schur<N, double, false, float><<<grid, 256, 0, c->stream>>>(c->aug, c->fcache, c->speeds, c->S32, nullptr,
+                                                                          c->Y, c->cy, c->basis, c->g, first, count);
+    });
+    c->launched();
+}
+// Variant 1: [A | B | r] assembled in FP32, right-looking FP32 LU with FP32 accumulation (the L
+// fix-up kept), the factors copied to the cells' FP32 slabs for later solves, back substitution
+// for X | y, then S = -C X stored in FP32, y and C y in FP64.
 void hdg_condense_chunk32(dgh_ctx *c, const double *r, int first, int count) {
     const int ld = c->m + c->t + 1, grid = std::min(count, c->sms * 8);
     const size_t stride = (size_t)c->m * ld;
@@ -1811,7 +1844,7 @@ void hdg_condense_chunk32(dgh_ctx *c, const double *r, int first, int count) {
     launch_lu<float>(c, c->aug32, stride, c->m, ld, count, c->lu32_perm + (size_t)first * c->m, ST_SINGULAR_HDG, false,
                      true);
     const long long warps = (long long)count * ((c->m + 31) / 32);
-    k_slab_pack<float><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, c->stream>>>(
+    k_slab_pack<float, float><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, c->stream>>>(
         c->aug32, stride, c->m, ld, count, c->lu32 + (size_t)first * c->m * c->m);
     k_backsolve<float><<<std::min(count, c->sms * 8), LU_THREADS, 0, c->stream>>>(c->aug32, stride, c->m, ld, count);
     c->launched(2);
@@ -2005,8 +2038,19 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
             return;
         }
         if (c->c32()) {
-            for (int first = 0; first < c->cells; first += c->aug_cells)
-                hdg_condense_chunk32(c, r, first, std::min(c->aug_cells, c->cells - first));
+            // variant 0: FP64 tensor-pipe LU, FP32 storage; 1: FP32 LU (autotuned per degree)
+            auto chunk = [&](int v, int first, int count) {
+                if (v == 0) hdg_condense_chunk32_tc(c, r, first, count);
+                else hdg_condense_chunk32(c, r, first, count);
+            };
+            if (c->hdg_variant < 0) {
+                const int sample = std::min(aug_chunk<double>(c), std::max(c->lu_grid, 1) * 4);
+                c->hdg_variant = tuned_variant(c, 2, [&](int v) { chunk(v, 0, sample); }, c->tune_ms + 2);
+                c->check_status();
+            }
+            const int per = c->hdg_variant == 0 ? aug_chunk<double>(c) : aug_chunk<float>(c);
+            for (int first = 0; first < c->cells; first += per)
+                chunk(c->hdg_variant, first, std::min(per, c->cells - first));
             hdg_rhs_from_cy(c);
             c->check_status();
             c->condensed = true;

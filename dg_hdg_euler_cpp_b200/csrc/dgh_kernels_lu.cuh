@@ -926,24 +926,28 @@ __global__ void k_round(const double *__restrict__ x, float *__restrict__ y, lon
 }
 
 // Copy of the factored m x m part of each augmented matrix (row length ld) into the slab
-// layout of k_lu_solve (a pool of m x m blocks): one warp per 32-row slab, 16-byte stores.
-template <typename T>
-__global__ void k_slab_pack(const T *__restrict__ src, size_t stride, int m, int ld, int count, T *__restrict__ dst) {
-    constexpr int W = SlabVec<T>::W;
+// layout of k_lu_solve (a pool of m x m blocks in TD): one warp per 32-row slab, 16-byte stores.
+// Position i's factor row is source row i, or, with perm, source row perm[i] (the left-looking
+// LU leaves its factors in original-row order).
+template <typename TS, typename TD>
+__global__ void k_slab_pack(const TS *__restrict__ src, size_t stride, int m, int ld, int count, TD *__restrict__ dst,
+                            const int *__restrict__ perm = nullptr) {
+    constexpr int W = SlabVec<TD>::W;
     const int slabs = (m + 31) / 32, lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= (long long)count * slabs) return;
     const int blk = (int)(warp / slabs), s = (int)(warp % slabs), r0 = 32 * s, nt = min(32, m - r0);
-    const T *A = src + (size_t)blk * stride + (size_t)r0 * ld;
-    T *out = dst + (size_t)blk * m * m + (size_t)r0 * m;
-    for (int g = 0; g < m / W; ++g)
-        if (lane < nt) {
-            typename SlabVec<T>::V v;
-            T *e = reinterpret_cast<T *>(&v);
+    if (lane >= nt) return;
+    const int row = perm ? perm[(size_t)blk * m + r0 + lane] : r0 + lane;
+    const TS *ar = src + (size_t)blk * stride + (size_t)row * ld;
+    TD *out = dst + (size_t)blk * m * m + (size_t)r0 * m;
+    for (int g = 0; g < m / W; ++g) {
+        typename SlabVec<TD>::V v;
+        TD *e = reinterpret_cast<TD *>(&v);
 #pragma unroll
-            for (int w = 0; w < W; ++w) e[w] = A[(size_t)lane * ld + g * W + w];
-            *reinterpret_cast<typename SlabVec<T>::V *>(out + (size_t)g * nt * W + lane * W) = v;
-        }
+        for (int w = 0; w < W; ++w) e[w] = (TD)ar[g * W + w];
+        *reinterpret_cast<typename SlabVec<TD>::V *>(out + (size_t)g * nt * W + lane * W) = v;
+    }
 }
 
 // Multi-RHS back substitution U X = Y in place on columns [m, ld) of each factored matrix.

@@ -470,6 +470,8 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
         }
 
         if (AUG) {
+            if (perm_out)  // the factors stay in original-row order: position i is row piv[i]
+                for (int i = tid; i < m; i += LL_THREADS) perm_out[(size_t)blk * m + i] = piv[i];
             // ---- right-hand sides: forward with L, backward with U, 32 columns at a time
             for (int j0 = m; j0 < ld; j0 += LL_NB) {
                 const int ncols = min(LL_NB, ld - j0);

@@ -23,7 +23,7 @@ constexpr const char *kUsage =
     "--ntol R --ltol R --safety S --prefix PATH\n"
     "--integrator ssp-dirk3|be --newton-steps N --warmup-updates N\n"
     "--graph --autotune --timing-only --check-update --no-save-solution --precision fp64|mixed|mixed16\n"
-    "--condensation fp64|fp32 --device N\n";
+    "--condensation fp64|fp32 --forcing 0|1 --device N\n";
 
 Settings settings_from(int argc, char **argv) {
     Settings s;
@@ -60,6 +60,7 @@ Settings settings_from(int argc, char **argv) {
         text("--condensation", [&](const std::string &v) {
             c.condense32 = pick(v, {"fp64", "fp32"}, "Invalid condensation precision");
         }),
+        text("--forcing", [&](const std::string &v) { c.forcing = pick(v, {"0", "1"}, "Invalid forcing"); }),
         text("--linear", [&](const std::string &v) { direct = pick(v, {"gmres", "direct"}, "Invalid linear solver"); }),
         text("--ordering", [&](const std::string &v) { pick(v, {"natural", "colamd"}, "Invalid ordering"); }),
         text("--precond", [&](const std::string &v) {

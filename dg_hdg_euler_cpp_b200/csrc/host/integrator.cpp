@@ -85,13 +85,22 @@ struct dgh_integrator {
         const double allowance =
             128 * std::numeric_limits<double>::epsilon() * ((snorm(state) + old_norm) / tau + norm);
         const double target = std::max(10 * cfg.linear_tolerance * norm, allowance);
+        // With dgh_config.forcing = 1 the linear solves stop at an absolute floor below which no
+        // later test can see the difference: half the round-off allowance of the acceptance
+        // target, and a tenth of the nonlinear tolerance in the same norm (so the Newton loop's
+        // own convergence test is unaffected).  forcing = 0 keeps the reference's relative ltol.
+        const double floor_abs =
+            cfg.forcing ? std::min(.5 * allowance,
+                                   .1 * cfg.nonlinear_tolerance * std::max(1., initial_rms) * std::sqrt(lx * ly))
+                        : 0.;
+        const double gmres_tol = norm > 0 ? std::max(cfg.linear_tolerance, floor_abs / norm) : cfg.linear_tolerance;
         int iterations = 0;
         double relative = 0;
         if (method == DGH_METHOD_DG) {
             ck(dgh_dg_refresh(ctx, state));
             ck(dgh_axpby(ctx, -1., residual, 0., residual, rhs, N));
             ck(dgh_block_jacobi_refresh(ctx, DGH_OP_DG));
-            ck(dgh_gmres(ctx, DGH_OP_DG, rhs, direction, cfg.max_linear, cfg.linear_tolerance, &iterations, &relative));
+            ck(dgh_gmres(ctx, DGH_OP_DG, rhs, direction, cfg.max_linear, gmres_tol, &iterations, &relative));
             const double *res = dgh_gmres_residual(ctx, DGH_OP_DG);
             ck(dgh_axpby(ctx, -1., res, 0., res, eq_err, N));
         } else if (cfg.condense32) {
@@ -99,16 +108,19 @@ struct dgh_integrator {
             // accuracy, so J du = -r is solved by iterative refinement in FP64.  Each pass solves
             // the Schur system for the current DG residual, recovers the correction with the kept
             // FP32 cell factors, adds it, and forms the true residual e = J du + r with the FP64
-            // J*v; the next pass retargets the condensation to e.  A pass's Schur tolerance goes
-            // no lower than the estimated FP32 floor of one pass (below it GMRES iterations buy
-            // nothing) nor than what the acceptance target still needs.
+            // J*v; the next pass retargets the condensation to e.  The passes stop once e is as
+            // small as the FP64 solve's GMRES leaves it (ltol |r|, or the forcing floor), which is
+            // below the acceptance target.  A pass's Schur tolerance goes no lower than the
+            // estimated FP32 floor of one pass (below it GMRES iterations buy nothing) nor than
+            // what the stop still needs.
+            const double stop = std::max(cfg.linear_tolerance * norm, floor_abs);
             ck(dgh_hdg_refresh_projected(ctx, state, residual));
             ck(dgh_hdg_rhs(ctx, rhs));
             ck(dgh_block_jacobi_refresh(ctx, DGH_OP_HDG));
             double floor_est = 1e-6, current = norm;
             bool valid = false;
             for (int pass = 0; pass < 2 * hdg_attempts && !valid; ++pass) {
-                const double tolerance = std::max({cfg.linear_tolerance, floor_est, .3 * target / current});
+                const double tolerance = std::max({cfg.linear_tolerance, floor_est, .3 * stop / current});
                 int cur = 0;
                 double rel = 0;
                 ck(dgh_gmres(ctx, DGH_OP_HDG, rhs, tdir, cfg.max_linear, tolerance, &cur, &rel));
@@ -119,7 +131,7 @@ struct dgh_integrator {
                 ck(dgh_dg_apply(ctx, direction, eq_err));
                 ck(dgh_axpby(ctx, 1., eq_err, 1., residual, eq_err, N));
                 const double next = dual(eq_err);
-                if (next <= target) {
+                if (next <= stop) {
                     valid = true;
                 } else {
                     const double achieved = next / current;
@@ -134,7 +146,7 @@ struct dgh_integrator {
             ck(dgh_hdg_refresh_projected(ctx, state, residual));
             ck(dgh_hdg_rhs(ctx, rhs));
             ck(dgh_block_jacobi_refresh(ctx, DGH_OP_HDG));
-            double tolerance = cfg.linear_tolerance;
+            double tolerance = gmres_tol;
             bool valid = false;
             for (int attempt = 0; attempt < hdg_attempts; ++attempt) {
                 int cur = 0;

@@ -81,6 +81,9 @@ typedef struct dgh_config {
     int preconditioner; /* 0 block Jacobi; 1 block ILU(0), natural ordering (1D only,        */
                         /* common/src/linalg/block_ilu.cpp:15-84)                            */
     int condense32;     /* 2D HDG: 1 = FP32 condensation (see dgh_hdg_retarget); 0 = FP64     */
+    int forcing;        /* linear solve stop: 0 = the reference's relative ltol; 1 = also stop */
+                        /* at an absolute floor: min(allowance / 2, ntol max(1, r0) sqrt(lx ly) / 10) */
+                        /* (time_integrator.cpp:143-147's allowance; no counterpart otherwise) */
 } dgh_config;
 
 /* config.hpp:7-18 defaults: nx=ny=8, k=3, restart 30, max_linear 1500, max_newton 30,

@@ -166,3 +166,35 @@ def test_condense32_cli_64x64_k2_accuracy_run():
     assert summ["newton_iterations"] == conv["newton_iterations"]
     for key in ("rho_L2", "momentum_x_L2", "momentum_y_L2", "energy_L2"):
         assert abs(float(summ[key]) - float(conv[key])) <= 1e-9 * float(conv[key]), key
+
+
+def test_forcing_floor_cli_64x64_k2_accuracy_run():
+    """The 64^2 Q2 DIRK3 accuracy run with the forcing floor (linear solves stop at the absolute
+    level no later test sees) and the FP32 forms: Newton counts equal to the archived run's, the
+    Newton rows on the history rule down to the 1e-10 r0 floor, the L2 errors to 1e-9."""
+    import json
+
+    argv = json.loads((GOLDEN / "acc_n64.command.json").read_text())[1:]
+    flags, i = [], 0
+    while i < len(argv):
+        if argv[i] in ("--alpha-deg", "--prefix"):
+            i += 2
+            continue
+        flags.append(argv[i])
+        i += 1
+    with tempfile.TemporaryDirectory() as tmp:
+        res = run_cli([*flags, "--condensation", "fp32", "--precision", "mixed16", "--forcing", "1", "--graph",
+                       "--prefix", f"{tmp}/r"])
+        assert res.returncode == 0, res.stderr + res.stdout
+        ours = read_csv(f"{tmp}/r_iterations.csv")
+        summ = {r["method"]: r for r in read_csv(f"{tmp}/r_summary.csv")}
+    ref = read_csv(GOLDEN / "acc_n64_iterations.csv")
+    conv = {(r["method"], r["nx"]): r for r in read_csv(GOLDEN / "acc_convergence.csv")}
+    for method in ("dg", "hdg"):
+        assert_history_close([r for r in ours if r["method"] == method], [r for r in ref if r["method"] == method],
+                             rtol=1e-8, krylov_slack=10 ** 6)
+        c = conv[(method, "64")]
+        assert summ[method]["newton_iterations"] == c["newton_iterations"]
+        assert int(summ[method]["krylov_iterations"]) < int(c["krylov_iterations"])
+        for key in ("rho_L2", "momentum_x_L2", "momentum_y_L2", "energy_L2"):
+            assert abs(float(summ[method][key]) - float(c[key])) <= 1e-9 * float(c[key]), key
