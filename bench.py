@@ -176,7 +176,7 @@ def algorithmic_bytes(kind: str, m: int, cells: int, fw: int, faces: int, t: int
     if kind == "dg":  # k_lu_solve over E blocks: m^2 factors, m perm ints, rhs and result
         return cells * (m * m * s + m * 4 + 2 * m * 8)
     if kind == "hdg_schur":  # k_hdg_apply: every S_K read once, lambda gathered, result written
-        return cells * t * t * 8 + faces * fw * 8 * 3
+        return cells * t * t * s + faces * fw * 8 * 3
     raise ValueError(kind)
 
 
@@ -288,7 +288,8 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
                   "k_lu_solve<%s> (block-Jacobi solve" % ("double" if precision == "fp64" else "float")) + \
             ", one launch per Krylov iteration)"
     else:
-        kb = algorithmic_bytes("hdg_schur", s.block, s.cells, s.face_width, s.faces, s.local_trace, precision)
+        kb = algorithmic_bytes("hdg_schur", s.block, s.cells, s.face_width, s.faces, s.local_trace,
+                               "mixed" if FORMS[precision][1] else "fp64")
         tk = kernel_timers["operator"]
         kernel = ("k_hdg_apply32 (face-owned Schur apply, FP32 Schur blocks" if FORMS[precision][1] else
                   "k_hdg_apply (face-owned Schur apply") + ", one launch per Krylov iteration)"

@@ -804,21 +804,33 @@ k_lu_solve_half(const __half *__restrict__ pool, const float *__restrict__ row_s
                     }
                     for (; g < g1; ++g) acc0 += dot8(Sv[(size_t)g * nt + lane], g);
                 }
+                // the slab's diagonal 32 x 32 block: this lane's row, four 16-byte groups loaded at
+                // once (r0 is a multiple of 32, so the block starts a group)
+                uint4 dg[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    dg[q] = (act && 8 * q < nt) ? Sv[(size_t)(r0 / H_W + q) * nt + lane] : make_uint4(0, 0, 0, 0);
                 float t = 0.f;
                 if (act) t = (dir == 0 ? y[r0 + lane] : y[r0 + lane] * rs[r0 + lane]) - ((acc0 + acc1) + (acc2 + acc3));
-                auto at = [&](int jj) {  // stored entry (row r0 + lane, column r0 + jj)
-                    const int j = r0 + jj;
-                    return __half2float(S[(size_t)(j / H_W) * nt * H_W + lane * H_W + j % H_W]);
+                auto at = [&](int jj) {  // stored entry (row r0 + lane, column r0 + jj), jj a constant
+                    const uint4 &v = dg[jj >> 3];
+                    const int w = (jj >> 1) & 3;
+                    const unsigned word = w == 0 ? v.x : w == 1 ? v.y : w == 2 ? v.z : v.w;
+                    return __half2float(__ushort_as_half((unsigned short)((jj & 1) ? word >> 16 : word & 0xffffu)));
                 };
                 if (dir == 0) {
-                    for (int jj = 0; jj < nt; ++jj) {
-                        const float l = (act && lane > jj) ? at(jj) : 0.f;
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) {
+                        if (jj >= nt) break;
+                        const float l = lane > jj ? at(jj) : 0.f;
                         const float yj = __shfl_sync(0xffffffffu, t, jj);
                         t -= l * yj;
                     }
                 } else {
-                    for (int jj = nt - 1; jj >= 0; --jj) {
-                        const float u = (act && lane <= jj) ? at(jj) : 1.f;
+#pragma unroll
+                    for (int jj = 31; jj >= 0; --jj) {
+                        if (jj >= nt) continue;
+                        const float u = lane <= jj ? at(jj) : 1.f;
                         if (lane == jj) t = t / u;
                         const float yj = __shfl_sync(0xffffffffu, t, jj);
                         if (lane < jj) t -= u * yj;

@@ -6,7 +6,11 @@ stores S in FP32, so its operators match the FP64 ones to FP32 accuracy: 2e-5 re
 (FP32 LU of blocks up to 324 wide, conditioning ~1e2).  The Newton updates are refined in FP64
 on the DG system to the reference's acceptance target, so whole updates and runs match the
 FP64 results to 1e-10 (states) and the archived histories under the history rule of
-tests/conftest.py.
+tests/conftest.py, with rtol 1e-8 for Newton rows above the rounding floor: a row's residual
+depends on the previous update's linear solve, which every form stops at ltol = 1e-12 relative to
+the previous residual (~0.4), i.e. within ~4e-13 absolute; on rows near 1e-4 that is a few 1e-9
+relative however the Krylov path differs.  The FP64 form, whose Krylov path is the reference's,
+holds 1e-10.
 """
 import ctypes
 import subprocess
@@ -134,7 +138,7 @@ def test_condense32_cli_4x4_histories(case, extra):
         summ = read_csv(f"{tmp}/run_summary.csv")
     ref = read_csv(GOLDEN / f"c4x4_{case}_iterations.csv")
     # Krylov counts of the refined form are the sum over its passes: not compared
-    assert_history_close(ours, ref, krylov_slack=10 ** 6)
+    assert_history_close(ours, ref, rtol=1e-8, krylov_slack=10 ** 6)
     for a, b in zip(summ, read_csv(GOLDEN / f"c4x4_{case}_summary.csv")):
         assert a["newton_iterations"] == b["newton_iterations"]
         for key in ("rho_L2", "momentum_x_L2", "momentum_y_L2", "energy_L2"):
@@ -161,7 +165,7 @@ def test_condense32_cli_64x64_k2_accuracy_run():
         ours = read_csv(f"{tmp}/r_iterations.csv")
         summ = read_csv(f"{tmp}/r_summary.csv")[0]
     ref = [r for r in read_csv(GOLDEN / "acc_n64_iterations.csv") if r["method"] == "hdg"]
-    assert_history_close(ours, ref, krylov_slack=10 ** 6)
+    assert_history_close(ours, ref, rtol=1e-8, krylov_slack=10 ** 6)
     conv = {(r["method"], r["nx"]): r for r in read_csv(GOLDEN / "acc_convergence.csv")}[("hdg", "64")]
     assert summ["newton_iterations"] == conv["newton_iterations"]
     for key in ("rho_L2", "momentum_x_L2", "momentum_y_L2", "energy_L2"):

@@ -6,7 +6,10 @@ Tolerances: the preconditioner solve matches the oracle's FP64 block Jacobi to 5
 (FP16 keeps 11 significant bits; the triangular sweeps of up to 324 rows amplify that by the
 blocks' conditioning, ~1e2 at these steps); GMRES on the FP64 operator still reaches the same
 1e-12 tolerance, so its solution agrees with the oracle's to 1e-9 and whole runs match the
-archived histories under the history rule of tests/conftest.py.
+archived histories under the history rule of tests/conftest.py with rtol 1e-8 above the rounding
+floor (a row's residual depends on the previous update's linear solve, stopped at ltol = 1e-12
+relative to the previous residual: a few 1e-9 relative on rows near 1e-4 for any Krylov path
+other than the reference's).
 """
 import subprocess
 import tempfile
@@ -86,7 +89,7 @@ def test_half_factor_cli_4x4_histories(case, extra):
         ours = read_csv(f"{tmp}/run_iterations.csv")
         summ = read_csv(f"{tmp}/run_summary.csv")[0]
     ref = [r for r in read_csv(GOLDEN / f"c4x4_{case}_iterations.csv") if r["method"] == "dg"]
-    assert_history_close(ours, ref, krylov_slack=10 ** 6)  # FP16 factors change the Krylov counts
+    assert_history_close(ours, ref, rtol=1e-8, krylov_slack=10 ** 6)  # FP16 factors change the Krylov counts
     refs = [r for r in read_csv(GOLDEN / f"c4x4_{case}_summary.csv") if r["method"] == "dg"][0]
     assert summ["newton_iterations"] == refs["newton_iterations"]
     for key in ("rho_L2", "momentum_x_L2", "momentum_y_L2", "energy_L2"):

@@ -6,6 +6,7 @@ residual histories, Krylov counts, L2 errors and nodal solutions.
 """
 import ctypes
 import json
+import os
 import tempfile
 from pathlib import Path
 
@@ -117,7 +118,9 @@ def test_64x64_k2_first_dirk3_step(oracle_mod):
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("k", [2, 8])
+@pytest.mark.parametrize("k", [2, pytest.param(8, marks=pytest.mark.skipif(
+    not os.environ.get("DGH_SLOW_ORACLE"), reason="minutes of CPU; set DGH_SLOW_ORACLE=1 (the device test "
+    "test_256_initial_residual_and_dt pins k = 8 against the same archived row)"))])
 def test_256_first_update_residual_and_dt(oracle_mod, k):
     """Speed run 256^2 (BE CFL5): initial projected state, frozen speeds, dt and first rms."""
     ref = read_csv(GOLDEN / f"speed256_k{k}_dg_iterations.csv")[0]
