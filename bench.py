@@ -68,6 +68,9 @@ def parse():
     p.add_argument("--nx", type=int, default=256)
     p.add_argument("--k", type=int, default=8)
     p.add_argument("--ltol", type=float, default=1e-12)
+    p.add_argument("--restart", type=int, default=20)
+    p.add_argument("--n512", action="store_true",
+                   help="also time the reduced forms on the reference's 512^2 k=8 GMRES(30) speed run")
     p.add_argument("--configs", default="dg:mixed,dg:mixed16,hdg:mixed32,hdg:mixed,dg:fp64,hdg:fp64,"
                                         "dg:mixed16-af,hdg:mixed32-af",
                    help="method:form pairs; forms: " + ", ".join(f"{k} ({v[3]})" for k, v in FORMS.items()))
@@ -206,7 +209,7 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
     K, W = args.steps, args.warmup
     s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=4,
                method=method, precision=FORMS[precision][0], condense32=FORMS[precision][1],
-               forcing=FORMS[precision][2], restart=20,
+               forcing=FORMS[precision][2], restart=args.restart,
                max_linear=1500, ntol=args.ltol, ltol=args.ltol,
                safety=1.1, device=local, autotune=1 if args.autotune else 0)
     s.gmres_graph(not args.stepped)
@@ -652,6 +655,19 @@ def main():
         line["e2e"] = {"value": world * tot_upd / e2e_s, "unit": "updates/s",
                        "h2d_bytes_per_step": results[head[0]]["e2e"]["h2d_bytes_per_step"],
                        "d2h_bytes_per_step": results[head[0]]["e2e"]["d2h_bytes_per_step"]}
+    if rank == 0 and world == 1 and args.n512:
+        import copy
+
+        big = copy.copy(args)
+        big.nx, big.restart, big.steps, big.warmup, big.stepped = 512, 30, 3, 0, False
+        n512 = {}
+        for method, form in (("dg", "mixed16"), ("hdg", "mixed32")):
+            out, _ = run_config(big, method, form, torch, pg, peaks, False, rank, local, False)
+            n512[f"{method}_{form}"] = {k: out[k] for k in ("updates_per_s", "ms_per_update", "krylov", "krylov_update1",
+                                                              "rms", "device_gb")}
+        n512["reference_single_thread_s_per_update"] = {"dg": 12369.562758, "hdg": 2336.131207,
+                                                        "source": "RESULTS.md:198,202 (Xeon 8268, one thread, FP64)"}
+        line["breakdown"]["n512_k8_gmres30"] = n512
     if rank == 0 and world == 1 and not args.no_batch:
         line["breakdown"]["uneven_batch_16"] = uneven_batch(torch, local, graph=not args.stepped)
     if rank == 0 and world == 1 and not args.no_graph_check:

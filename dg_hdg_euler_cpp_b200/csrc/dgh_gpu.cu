@@ -207,6 +207,8 @@ struct dgh_ctx {
     bool mixed() const { return cfg.precision != DGH_PRECISION_FP64; }
     bool half16() const { return cfg.precision == DGH_PRECISION_MIXED16; }
     float *dg_scale = nullptr;  // FP16 DG factors: per-row reciprocal scales of U
+    double *dg_slots = nullptr; // reduced-precision DG factorisation: one FP64 slot per resident LU CTA
+    int dg_slot_count = 0;
     bool d1() const { return dim == 1; }
     bool overint() const { return dim == 2 && Q > n; }
     bool has_dg() const { return cfg.method == DGH_METHOD_DG || cfg.method == DGH_METHOD_BOTH; }
@@ -364,6 +366,39 @@ void launch_lu_left(dgh_ctx *c, double *pool, size_t stride, int m, int ld, int 
                                                           slab_out ? 1 : 0, out32, x_out, y_out);
     c->launched();
 }
+// The DG blocks of cells [first, first + count) assembled and factored in one persistent launch
+// (k_lu_left's fused mode: each CTA assembles a cell into its own FP64 slot, factors it there and
+// writes FP32 slabs, or FP16 slabs with row scales).  Collocated volume rule only.
+template <int N> void launch_dg_fused(dgh_ctx *c, int first, int count) {
+    const size_t smem = lu_left_smem_bytes(c->m);
+    allow_dynamic_smem((const void *)k_lu_left<false, N>, smem);
+    int per_sm = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_left<false, N>, LL_THREADS, smem), "occupancy");
+    const int grid = std::min(count, std::min(c->dg_slot_count, c->sms * std::max(1, per_sm)));
+    need(grid <= c->lu_grid, "fused factorisation grid exceeds the LU scratch");
+    LLFuse fu;
+    fu.vol = c->vol;
+    fu.fcache = c->fcache;
+    fu.speeds = c->speeds;
+    fu.slots = c->dg_slots;
+    fu.b = c->basis;
+    fu.g = c->g;
+    fu.inv_step = c->inv_step;
+    fu.first = first;
+    const size_t mp8 = pad8(c->m);
+    float *out32 = nullptr;
+    if (c->half16()) {
+        fu.out16 = (__half *)c->dg_pool + (size_t)first * c->m * mp8;
+        fu.scale16 = c->dg_scale + (size_t)first * c->m;
+    } else {
+        out32 = (float *)c->dg_pool + (size_t)first * c->m * c->m;
+    }
+    k_lu_left<false, N><<<grid, LL_THREADS, smem, c->stream>>>(c->dg_slots, (size_t)c->m * c->m, c->m, c->m, count,
+                                                                c->lu_tri, c->dg_perm + (size_t)first * c->m, c->status,
+                                                                ST_SINGULAR, 0, out32, nullptr, nullptr, fu);
+    c->launched();
+}
+
 // Narrow blocks (m <= 64): one warp per block in shared memory.
 template <typename TF>
 void launch_lu_narrow(dgh_ctx *c, TF *pool, int m, int count, int *perm, int bit) {
@@ -1250,10 +1285,15 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->gdev = c->alloc<GmresDev>(1);
         ck(cudaMemset(c->V, 0, sizeof(double) * (size_t)c->vld * (k.restart + 1)), "memset");
         if (c->has_dg() && c->mixed()) {
-            const size_t per_cell = (size_t)c->m * c->m * sizeof(double);
-            const size_t budget = (size_t)8 << 30;  // FP64 factor workspace: at most 8 GiB
-            c->dg_ws_cells = (int)std::max<size_t>(1, std::min<size_t>(c->cells, budget / per_cell));
-            c->dg_ws = c->alloc<double>((size_t)c->dg_ws_cells * c->m * c->m);
+            if (c->overint()) {  // chunked: assembly with the over-integrated volume terms, then the LU
+                const size_t per_cell = (size_t)c->m * c->m * sizeof(double);
+                const size_t budget = (size_t)8 << 30;  // FP64 factor workspace: at most 8 GiB
+                c->dg_ws_cells = (int)std::max<size_t>(1, std::min<size_t>(c->cells, budget / per_cell));
+                c->dg_ws = c->alloc<double>((size_t)c->dg_ws_cells * c->m * c->m);
+            } else {  // one persistent fused launch: an FP64 slot per resident CTA (two per SM)
+                c->dg_slot_count = std::min(c->cells, 2 * c->sms);
+                c->dg_slots = c->alloc<double>((size_t)c->dg_slot_count * c->m * c->m);
+            }
         }
         if (c->has_dg() || c->has_hdg()) {
             const size_t smem = lu_left_smem_bytes(c->m);
@@ -1684,6 +1724,11 @@ std::map<std::tuple<int, int, int>, int> g_tune_cache;  // (kind, n, precision) 
 void dg_factor(dgh_ctx *c, int variant, int first, int count) {
     const size_t stride = (size_t)c->m * c->m;
     const int grid = std::min(count, c->sms * 8);
+    if (c->mixed() && (c->half16() || variant == 0) && !c->overint()) {
+        // one persistent launch: assemble + FP64 left-looking LU per CTA slot, reduced output
+        DGH_DISPATCH_N(c->n, { launch_dg_fused<N>(c, first, count); });
+        return;
+    }
     if (c->half16()) {  // FP64 left-looking in the workspace, then FP16 slabs with row scales
         const int mp = pad8(c->m);
         for (int f = first; f < first + count; f += c->dg_ws_cells) {

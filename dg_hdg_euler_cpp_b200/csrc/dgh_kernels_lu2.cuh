@@ -22,9 +22,25 @@
 // Pivoting: the first largest |a| in position order wins ties (LAPACK getrf, Eigen
 // PartialPivLU), with LAPACK swap semantics, so the pivot sequence is the reference's.
 #pragma once
+#include "dgh_kernels_dg.cuh"
 #include "dgh_kernels_lu.cuh"
 
 namespace dgh {
+
+// Fused DG mode of k_lu_left (FN = nodes per direction > 0): the kernel walks all cells in one
+// persistent launch, assembling each cell's block (k_dg_assemble's entries, collocated volume
+// rule) into its CTA's private FP64 slot, factoring it there and writing the reduced-precision
+// factors out (FP32 slabs to out32, or FP16 slabs with row scales to out16 / scale16).
+struct LLFuse {
+    const double *vol = nullptr, *fcache = nullptr, *speeds = nullptr;
+    double *slots = nullptr;  // gridDim.x slots of m * m doubles
+    __half *out16 = nullptr;
+    float *scale16 = nullptr;
+    Basis1D b;
+    Grid g;
+    double inv_step = 0;
+    int first = 0;  // cell of block 0 (outputs and perm_out are offset by the caller)
+};
 
 constexpr int LL_NB = 32;              // panel width and chunk size
 constexpr int LL_AP = 36;              // shared pitch of the panel (= 4 mod 16: conflict-free fragments)
@@ -207,11 +223,11 @@ __device__ __forceinline__ void ll_warp_argmax(double &bv, int &bp, int &bs) {
 // is in columns m..ld-1, or, with x_out, in x_out (m x (ld - m - 1) row-major per matrix) and
 // y_out (m per matrix); the A part holds the factors in original-row order (not used later).
 // tri: per-CTA scratch of ceil(m/32) * LL_TRI doubles.
-template <bool AUG>
+template <bool AUG, int FN = 0>
 __global__ void __launch_bounds__(LL_THREADS, 2)
 k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, double *__restrict__ tri_all,
           int *__restrict__ perm_out, int *status, int singular_bit, int slab_out, float *__restrict__ out32,
-          double *__restrict__ x_out, double *__restrict__ y_out) {
+          double *__restrict__ x_out, double *__restrict__ y_out, LLFuse fu = LLFuse()) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int mp = (m + LL_NB - 1) / LL_NB * LL_NB, P = mp / LL_NB;
     double *acc = reinterpret_cast<double *>(smraw);  // mp rows x LL_AP
@@ -225,8 +241,22 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
     constexpr int NW = LL_THREADS / 32;
     double *tri = tri_all + (size_t)blockIdx.x * P * LL_TRI;
 
+    __shared__ Basis1D fsb;
+    if constexpr (FN > 0) stage_basis<FN>(fu.b, fsb);
     for (int blk = blockIdx.x; blk < count; blk += gridDim.x) {
         double *A = pool + (size_t)blk * stride;
+        if constexpr (FN > 0) {
+            // assemble the cell's block into this CTA's slot (tables in the panel area)
+            constexpr int FP = FN * FN, FM = NVAR * FP;
+            A = fu.slots + (size_t)blockIdx.x * FM * FM;
+            double *jx = acc, *jy = jx + FP * 16, *fj = jy + FP * 16;
+            __syncthreads();
+            cell_tables<FN, false>(fu.first + blk, fu.vol, fu.fcache, fu.speeds, fsb, fu.g, jx, jy, fj);
+            __syncthreads();
+            for (int idx = tid; idx < FM * FM; idx += LL_THREADS)
+                A[idx] = cell_block_entry<FN>(idx / FM, idx % FM, jx, jy, fj, fsb, fu.g, fu.inv_step, true);
+            __syncthreads();
+        }
         for (int i = tid; i < mp; i += LL_THREADS) piv[i] = i < m ? i : 0;
         if (tid == 0) bad = 0;
         __syncthreads();
@@ -508,6 +538,44 @@ k_lu_left(double *__restrict__ pool, size_t stride, int m, int ld, int count, do
                 }
                 __syncthreads();
             }
+        } else if (FN > 0 && fu.out16) {
+            // ---- FP16 slabs with row scales (k_pack_half's layout) from the original-row storage:
+            // stage 32 position rows, each row's largest |U| by a warp, then 8-column groups
+            const int sp = ll_stage_pitch(m), mp8 = pad8(m);
+            double *stage = acc;
+            __shared__ float rsc[32];
+            __half *out = fu.out16 + (size_t)blk * m * mp8;
+            for (int r0 = 0; r0 < m; r0 += 32) {
+                const int nt = min(32, m - r0);
+                for (int rr = warp; rr < nt; rr += NW) ll_stage_row(stage + (size_t)rr * sp, A + (size_t)piv[r0 + rr] * ld, m);
+                __syncthreads();
+                for (int rr = warp; rr < nt; rr += NW) {
+                    double big = 0;
+                    for (int j = r0 + rr + lane; j < m; j += 32) big = fmax(big, fabs(stage[(size_t)rr * sp + j]));
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) big = fmax(big, __shfl_xor_sync(0xffffffffu, big, o));
+                    if (lane == 0) {
+                        rsc[rr] = big > 0 ? (float)(1. / big) : 1.f;
+                        fu.scale16[(size_t)blk * m + r0 + rr] = rsc[rr];
+                    }
+                }
+                __syncthreads();
+                for (int gg = warp; gg < mp8 / H_W; gg += NW)
+                    for (int rr = lane; rr < nt; rr += 32) {
+                        __align__(16) __half v[H_W];
+                        const double inv = (double)rsc[rr];
+#pragma unroll
+                        for (int w = 0; w < H_W; ++w) {
+                            const int j = gg * H_W + w;
+                            const double a = j < m ? stage[(size_t)rr * sp + j] : 0.;
+                            v[w] = __double2half(j >= r0 + rr ? a * inv : a);
+                        }
+                        *reinterpret_cast<uint4 *>(out + (size_t)r0 * mp8 + (size_t)gg * nt * H_W + rr * H_W) =
+                            *reinterpret_cast<const uint4 *>(v);
+                    }
+                __syncthreads();
+            }
+            for (int i = tid; i < m; i += LL_THREADS) perm_out[(size_t)blk * m + i] = piv[i];
         } else if (out32) {
             // ---- FP32 slabs straight from the original-row storage: stage 32 position rows
             // (16-byte loads, several in flight per thread), then each lane converts one row's

@@ -153,3 +153,41 @@ def test_advance_matches_oracle_dirk3_both_methods(oracle_mod):
         assert abs(st_g["krylov_iterations"] - st_o["krylov_iterations"]) <= 2 * st_o["newton_iterations"]
         assert st_g["conservation_drift"] <= 1e-11
         s.close()
+
+
+@pytest.mark.parametrize("method,precision", [("dg", "mixed16"), ("hdg", "mixed32")])
+def test_512_k8_speed_protocol_reduced_forms(method, precision):
+    """512^2 k = 8 (262,144 cells of 324 unknowns), BE CFL 5, GMRES(30): the reference's 512^2
+    speed run (speed_test/results/2d_n512_restart30_*), four Newton updates of the reduced forms
+    that fit one B200 (FP16 DG factors: 56 GB; FP32 condensation: 110 GB of kept cell factors),
+    against the archived residual history on the history rule (1e-10 relative above 1e-6 r0,
+    the 1e-10 r0 floor below)."""
+    import ctypes
+
+    from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
+
+    ref = read_csv(GOLDEN / f"speed512_k8_{method}_iterations.csv")
+    assert len(ref) == 4
+    s = Solver(nx=512, ny=512, k=8, cfl=5.0, integrator="be", steps=1, newton_steps=4, method=method, restart=30,
+               precision=FORMS[precision][0], condense32=FORMS[precision][1])
+    s.gmres_graph(True)
+    it = Integrator(s, method)
+    dt = it.stage_begin(s.initial())
+    assert abs(dt - float(ref[0]["dt"])) <= 1e-15 * dt
+    rows = [it.update() for _ in range(4)]
+    print("\n", method, precision, s.device_bytes() / 1e9, "GB",
+          [(r["krylov_iterations"], r["residual_physical_rms"], r["iteration_s"]) for r in rows])
+    r0 = float(ref[0]["residual_physical_rms"])
+    for k, row in enumerate(rows):
+        x, y = row["residual_physical_rms"], float(ref[k]["residual_physical_rms"])
+        if y > 1e-6 * r0:
+            assert abs(x - y) <= 1e-10 * y, (k, x, y)
+        else:
+            assert abs(x - y) <= 1e-10 * r0, (k, x, y)
+    state = s.vec()
+    s.lib.dgh_axpby(s.h, 1.0, ctypes.c_void_p(it.state_ptr()), 0.0, ctypes.c_void_p(it.state_ptr()),
+                    ctypes.c_void_p(state.data_ptr()), state.numel())
+    s.lib.dgh_sync(s.h)
+    assert s.residual_rms(s.residual(state)) <= 1e-10 * r0
+    it.close()
+    s.close()

@@ -50,14 +50,17 @@ def test_ilu0_colamd_is_not_restated(tmp_path):
     assert res.returncode != 0 and "COLAMD" in (res.stderr + res.stdout)
 
 
-def test_2d_ilu0_solves_the_dg_newton_system_in_fewer_iterations():
+@pytest.mark.parametrize("nx,ny,k,ratio", [(6, 5, 2, 2.0), (16, 16, 2, 4.0), (8, 8, 4, 4.0)])
+def test_2d_ilu0_solves_the_dg_newton_system_in_fewer_iterations(nx, ny, k, ratio):
     """Block ILU(0) on the 2D cartesian block graph (no reference counterpart: the 2D front end
-    accepts block-jacobi only): the preconditioned GMRES reaches the same solution of the first
-    BE Newton system as block Jacobi, in a fraction of the Krylov iterations."""
+    accepts block-jacobi only): the preconditioned GMRES(20) reaches the same solution of the
+    first BE Newton system at CFL 5 as block Jacobi, in at most 1/ratio of the Krylov iterations
+    (about 5x fewer from 16^2 up: the measurement behind the cost comparison of a device 2D
+    ILU(0) against block Jacobi)."""
     import numpy as np
     import oracle_py
 
-    o = oracle_py.Oracle("--nx 6 --ny 5 --k 2 --cfl 5 --integrator be --steps 1 --restart 20")
+    o = oracle_py.Oracle(f"--nx {nx} --ny {ny} --k {k} --cfl 5 --integrator be --steps 1 --restart 20")
     u = o.initial()
     o.set_stage(u, 5.0 / o.freeze(u))
     r = o.residual(u)
@@ -68,4 +71,4 @@ def test_2d_ilu0_solves_the_dg_newton_system_in_fewer_iterations():
     xi, ki, reli, _ = o.gmres(2, -r, 20, 2000, 1e-12)
     assert relb <= 1e-12 and reli <= 1e-12
     assert np.max(np.abs(xi - xb)) <= 1e-9 * np.max(np.abs(xb))
-    assert 0 < ki < kb / 2, (ki, kb)
+    assert 0 < ki <= kb / ratio, (ki, kb)
