@@ -78,6 +78,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-graph-check", action="store_true", help="skip the GMRES graph-vs-stepped comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the 16-member uneven batch")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the DIRK3 discrete-adjoint configuration")
     p.add_argument("--stepped", action="store_true",
                    help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
@@ -368,6 +369,36 @@ def graph_comparison(torch, local: int):
                                        "speedup": res[False][0] / res[True][0],
                                        "krylov": [r["krylov_iterations"] for r in res[True][1]],
                                        "bitwise_equal_history": same}
+    return out
+
+
+def discrete_adjoint(torch, local: int) -> dict:
+    """The discrete-adjoint configuration: 128^2 cells, k = 4, SSP-DIRK3 at CFL 2 for 20 steps,
+    checkpoints every 5 steps, objective sum M rho^2 at the final time: wall time of one gradient
+    (forward run with checkpoints, recomputed segments, J^T GMRES per stage) and its counts.  The
+    gradient's check against central finite differences is tests/test_gpu_adjoint.py's."""
+    from dg_hdg_euler_cpp_b200 import _lib
+    from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
+
+    s = Solver(nx=128, ny=128, k=4, cfl=2.0, integrator="ssp-dirk3", steps=20, method="dg", restart=20, device=local)
+    s.gmres_graph(True)
+    it = Integrator(s, "dg")
+    u0 = s.initial().cpu().numpy()
+    grad = np.zeros(s.size)
+    st = _lib.dgh_adjoint_stats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = s.lib.dgh_dirk3_adjoint(it.h, 20, 5, u0.ctypes.data_as(ctypes.c_void_p), grad.ctypes.data_as(ctypes.c_void_p),
+                                 ctypes.byref(st))
+    sec = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(s.lib.dgh_integrator_error(it.h).decode())
+    out = {"config": "128x128 k=4 SSP-DIRK3 CFL 2, 20 steps, checkpoints every 5, J = sum M rho^2",
+           "gradient_seconds": sec, "objective": st.objective, "forward_newton_updates": st.forward_newton,
+           "adjoint_krylov": st.adjoint_krylov, "checkpoints": st.checkpoints, "recomputed_steps": st.recomputed_steps}
+    it.close()
+    s.close()
+    torch.cuda.empty_cache()
     return out
 
 
@@ -668,6 +699,8 @@ def main():
         n512["reference_single_thread_s_per_update"] = {"dg": 12369.562758, "hdg": 2336.131207,
                                                         "source": "RESULTS.md:198,202 (Xeon 8268, one thread, FP64)"}
         line["breakdown"]["n512_k8_gmres30"] = n512
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        line["breakdown"]["discrete_adjoint_128_k4"] = discrete_adjoint(torch, local)
     if rank == 0 and world == 1 and not args.no_batch:
         line["breakdown"]["uneven_batch_16"] = uneven_batch(torch, local, graph=not args.stepped)
     if rank == 0 and world == 1 and not args.no_graph_check:
