@@ -171,53 +171,54 @@ template <int N>
 __global__ void __launch_bounds__(256)
 k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
             double *__restrict__ out, Basis1D b, Grid g);
-// The same with FP32 Schur blocks (the FP32 condensation): 16-byte loads of four S values, FP64
-// products and accumulation, so the operator applied is exactly the stored FP32 S.
+// The same with FP32 Schur blocks (the FP32 condensation), products and sums in FP64, so the
+// operator applied is exactly the stored FP32 S.  The FP32 -> FP64 widening is done on the
+// integer pipe: a float's bit pattern shifted right by 3 (sign kept) and its low mantissa bits
+// shifted into the low word is the double v * 2^-896, exactly, for every finite v (zero and
+// subnormals included); the gathered trace values are stored scaled by 2^896, so each product
+// is exact and no conversion instruction is issued per S entry.  (Non-finite S entries would
+// not survive this widening; the condensation's factor check rejects non-finite factors.)
+__device__ __forceinline__ double widen_scaled(float f) {
+    const unsigned b = __float_as_uint(f);
+    return __hiloint2double((int)(((b & 0x7fffffffu) >> 3) | (b & 0x80000000u)), (int)(b << 29));
+}
 template <int N>
 __global__ void __launch_bounds__(256)
 k_hdg_apply32(const float *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
               double *__restrict__ out, Basis1D b, Grid g) {
     constexpr int FW = NVAR * N, T = NFACES * FW, T4 = T / 4, PASSES = (T4 + 31) / 32;
+    constexpr double kScale = 0x1p896;  // undoes the 2^-896 of widen_scaled
     __shared__ __align__(16) double loc[2][T];
     const int face = blockIdx.x;
     const int axis = face >= g.cells, first = face - axis * g.cells, next = neighbor(g, first, 2 * axis + 1);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // rows of S_K are T = 16N floats (a multiple of four), so every row starts 16-byte aligned;
-    // the face's rows of each cell are one contiguous run of FW rows
-    const float4 *S1 = reinterpret_cast<const float4 *>(S + (size_t)first * T * T + (size_t)(2 * axis + 1) * FW * T);
-    const float4 *S2 = reinterpret_cast<const float4 *>(S + (size_t)next * T * T + (size_t)(2 * axis) * FW * T);
-    // a warp's rows are warp, warp + 8, ...: the next row's loads are issued before the current
-    // row is reduced, and the first row's before the trace gather and its barrier
-    float4 a[PASSES], c[PASSES];
-    auto fetch = [&](int row) {
-#pragma unroll
-        for (int t = 0; t < PASSES; ++t) {
-            const int j = lane + 32 * t;
-            if (row < FW && j < T4) {
-                a[t] = S1[(size_t)row * T4 + j];
-                c[t] = S2[(size_t)row * T4 + j];
-            }
-        }
-    };
-    fetch(warp);
     for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
         const int which = k / T, s = (k % T) / FW, j = k % FW;
         const int cell = which ? next : first;
-        loc[which][k % T] = lam[(size_t)face_of(g, cell, s) * FW + j];
+        loc[which][k % T] = kScale * lam[(size_t)face_of(g, cell, s) * FW + j];
     }
     __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int row = warp; row < FW; row += 8) {
+        // rows of S_K are T = 16N floats (a multiple of four), so every row starts 16-byte aligned
+        const float4 *s1 = reinterpret_cast<const float4 *>(S + (size_t)first * T * T + (size_t)((2 * axis + 1) * FW + row) * T);
+        const float4 *s2 = reinterpret_cast<const float4 *>(S + (size_t)next * T * T + (size_t)((2 * axis) * FW + row) * T);
         double acc = 0;
 #pragma unroll
         for (int t = 0; t < PASSES; ++t) {
             const int j = lane + 32 * t;
             if (j < T4) {
+                const float4 a = s1[j], c = s2[j];
                 const double *x = loc[0] + 4 * j, *y = loc[1] + 4 * j;
-                acc += (double)a[t].x * x[0] + (double)a[t].y * x[1] + (double)a[t].z * x[2] + (double)a[t].w * x[3];
-                acc += (double)c[t].x * y[0] + (double)c[t].y * y[1] + (double)c[t].z * y[2] + (double)c[t].w * y[3];
+                acc = fma(widen_scaled(a.x), x[0], acc);
+                acc = fma(widen_scaled(a.y), x[1], acc);
+                acc = fma(widen_scaled(a.z), x[2], acc);
+                acc = fma(widen_scaled(a.w), x[3], acc);
+                acc = fma(widen_scaled(c.x), y[0], acc);
+                acc = fma(widen_scaled(c.y), y[1], acc);
+                acc = fma(widen_scaled(c.z), y[2], acc);
+                acc = fma(widen_scaled(c.w), y[3], acc);
             }
         }
-        fetch(row + 8);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) {
