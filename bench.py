@@ -79,6 +79,7 @@ def parse():
     p.add_argument("--no-graph-check", action="store_true", help="skip the GMRES graph-vs-stepped comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the 16-member uneven batch")
     p.add_argument("--no-adjoint", action="store_true", help="skip the DIRK3 discrete-adjoint configuration")
+    p.add_argument("--no-ilu", action="store_true", help="skip the 2D block ILU(0) against block Jacobi comparison")
     p.add_argument("--stepped", action="store_true",
                    help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
@@ -429,6 +430,45 @@ def discrete_adjoint(torch, local: int) -> dict:
     return out
 
 
+def ilu_comparison(torch, local: int, nx: int = 128, k: int = 8) -> dict:
+    """2D block ILU(0) (natural ordering, FP32 factors) against block Jacobi (FP32 factors) on
+    the speed protocol at nx^2 k = 8: protocol update 1 untimed, updates 2-3 timed; per form the
+    ms per update, its Krylov counts, the factorisation and the per-application preconditioner
+    time (CUDA-event timers of a stepped update)."""
+    from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
+
+    out = {"mesh": f"{nx}x{nx} k={k}", "protocol": "BE CFL 5 GMRES(20), updates 2-3 after an untimed update 1"}
+    for pc in ("block-jacobi", "block-ilu0"):
+        s = Solver(nx=nx, ny=nx, k=k, cfl=5.0, integrator="be", steps=1, newton_steps=4, method="dg", restart=20,
+                   precision="mixed", precond=pc, device=local)
+        it = Integrator(s, "dg")
+        u0 = s.initial()
+        it.stage_begin(u0)
+        it.update()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rows = [it.update() for _ in range(2)]
+        torch.cuda.synchronize()
+        sec = (time.perf_counter() - t0) / 2
+        it.stage_begin(u0)
+        s.lib.dgh_timing_enable(s.h, 1)
+        first = it.update()
+        tm = {}
+        for name, cat in (("precond", 0), ("factor", 3)):
+            tot, cnt = ctypes.c_double(), ctypes.c_int64()
+            s.lib.dgh_timing_read(s.h, cat, ctypes.byref(tot), ctypes.byref(cnt))
+            tm[name] = {"ms": tot.value, "launches": cnt.value}
+        s.lib.dgh_timing_enable(s.h, 0)
+        out[pc] = {"ms_per_update": 1000.0 * sec, "krylov": [r["krylov_iterations"] for r in rows],
+                   "krylov_update1": first["krylov_iterations"], "factor_ms": tm["factor"]["ms"],
+                   "precond_ms_per_application": tm["precond"]["ms"] / max(1, tm["precond"]["launches"]),
+                   "device_gb": s.device_bytes() / 1e9}
+        it.close()
+        s.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: bool = True):
     """The uneven batch (members from seeds 0..members-1: k in {2,4,6,8}, N^2 meshes with N in
     {32,64,96,128}, DG or HDG, amplitude-scaled initial states, BE CFL 5, GMRES(30), mixed
@@ -728,6 +768,8 @@ def main():
         n512["reference_single_thread_s_per_update"] = {"dg": 12369.562758, "hdg": 2336.131207,
                                                         "source": "RESULTS.md:198,202 (Xeon 8268, one thread, FP64)"}
         line["breakdown"]["n512_k8_gmres30"] = n512
+    if rank == 0 and world == 1 and not args.no_ilu:
+        line["breakdown"]["ilu2d_vs_block_jacobi"] = ilu_comparison(torch, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
         line["breakdown"]["discrete_adjoint_128_k4"] = discrete_adjoint(torch, local)
     if rank == 0 and world == 1 and not args.no_batch:

@@ -6,6 +6,7 @@
 #include "dgh_gpu.h"
 #include "dgh_kernels_1d.cuh"
 #include "dgh_kernels_ilu1d.cuh"
+#include "dgh_kernels_ilu2d.cuh"
 #include "dgh_kernels_dg.cuh"
 #include "dgh_kernels_hdg.cuh"
 #include "dgh_kernels_init.cuh"
@@ -14,7 +15,10 @@
 #include "dgh_kernels_lu2.cuh"
 #include "dgh_kernels_q.cuh"
 
+#include <cublas_v2.h>
+
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -137,6 +141,30 @@ struct dgh_ctx {
         int *upd_off = nullptr, *upd_target = nullptr, *upd_upper = nullptr, *perm = nullptr;
         void *vals = nullptr;
     } ilu_dg, ilu_hdg;
+    // 2D block ILU(0) of the DG operator on the periodic cartesian block graph, natural ordering:
+    // per row (cell) the diagonal block and the 4 neighbour blocks in increasing column order
+    // (the lower ones first); forward and backward level schedules; per forward level and lower
+    // slot order q the batched products of the factorisation (pointer arrays on the device)
+    struct Ilu2 {
+        bool on = false;
+        void *diag = nullptr, *offd = nullptr;  // factor storage (FP64, or FP32 in the mixed forms)
+        int *nlower = nullptr, *ncol = nullptr, *frows = nullptr, *brows = nullptr, *pairs = nullptr;
+        void **cdst = nullptr;                  // coupling block of pair k
+        std::vector<int> fptr, bptr;            // level offsets into frows / brows
+        struct Batch {
+            int n = 0;
+            void **a = nullptr, **b = nullptr, **c = nullptr;
+        };
+        struct Step {
+            Batch mult, update;
+        };
+        std::vector<std::array<Step, 4>> steps;
+        void *scratch = nullptr;
+        double *aug = nullptr, *inv = nullptr, *ydummy = nullptr, *work = nullptr;
+        int *perm = nullptr;
+        cublasHandle_t blas = nullptr;
+    } ilu2;
+    bool ilu2d() const { return ilu() && dim == 2; }
     bool ilu() const { return cfg.preconditioner == 1; }
     // left-looking FP64 LU: per-CTA scratch of the panels' L_qq^{-1}, U_qq^{-1}; FP64 workspace
     // for the mixed-precision DG blocks (factored in FP64 in chunks, stored as FP32 slabs)
@@ -476,6 +504,212 @@ void launch_small_solve(dgh_ctx *c, const TF *pool, const int *perm, int m, int 
     c->launched();
 }
 
+// ---- 2D block ILU(0) of the DG operator ---------------------------------------------------------
+void blas_ck(cublasStatus_t e, const char *what) {
+    if (e != CUBLAS_STATUS_SUCCESS) fail(DGH_ERR_CUDA, std::string(what) + ": cuBLAS status " + std::to_string((int)e));
+}
+// The pattern, level schedules and batched-product pointer arrays (block_ilu.cpp:15-45 on the
+// cartesian block graph: every row couples to itself and its four face neighbours).
+void ilu2_build(dgh_ctx *c) {
+    auto &L = c->ilu2;
+    const int E = c->cells, m = c->m;
+    const size_t mm = (size_t)m * m, tsz = c->mixed() ? sizeof(float) : sizeof(double);
+    std::vector<int> ncol(4 * (size_t)E), nlower(E), lev(E, 0), blev(E, 0);
+    for (int i = 0; i < E; ++i) {
+        int nb[4];
+        for (int sd = 0; sd < 4; ++sd) nb[sd] = neighbor(c->g, i, sd);
+        std::sort(nb, nb + 4);
+        need(nb[0] != nb[1] && nb[1] != nb[2] && nb[2] != nb[3] && nb[0] != i && nb[3] != i,
+             "block ILU(0) needs distinct face neighbours (nx, ny >= 3)");
+        int nl = 0;
+        for (int k = 0; k < 4; ++k) {
+            ncol[4 * (size_t)i + k] = nb[k];
+            nl += nb[k] < i;
+        }
+        nlower[i] = nl;
+        for (int k = 0; k < nl; ++k) lev[i] = std::max(lev[i], lev[nb[k]] + 1);
+    }
+    for (int i = E - 1; i >= 0; --i)
+        for (int k = nlower[i]; k < 4; ++k) blev[i] = std::max(blev[i], blev[ncol[4 * (size_t)i + k]] + 1);
+    auto by_level = [&](const std::vector<int> &lv, std::vector<int> &ptr) {
+        const int nlev = *std::max_element(lv.begin(), lv.end()) + 1;
+        ptr.assign(nlev + 1, 0);
+        for (int i = 0; i < E; ++i) ++ptr[lv[i] + 1];
+        for (int l = 0; l < nlev; ++l) ptr[l + 1] += ptr[l];
+        std::vector<int> rows(E), fill(ptr.begin(), ptr.end() - 1);
+        for (int i = 0; i < E; ++i) rows[fill[lv[i]]++] = i;  // natural order inside a level
+        return rows;
+    };
+    const std::vector<int> frows = by_level(lev, L.fptr), brows = by_level(blev, L.bptr);
+    L.diag = c->alloc<char>((size_t)E * mm * tsz);
+    L.offd = c->alloc<char>((size_t)E * 4 * mm * tsz);
+    auto diag_at = [&](int i) { return (void *)((char *)L.diag + (size_t)i * mm * tsz); };
+    auto offd_at = [&](int i, int k) { return (void *)((char *)L.offd + ((size_t)4 * i + k) * mm * tsz); };
+    auto slot_in = [&](int i, int col) {  // position of col among row i's neighbours, -1 = diagonal
+        if (col == i) return -1;
+        for (int k = 0; k < 4; ++k)
+            if (ncol[4 * (size_t)i + k] == col) return k;
+        return -2;
+    };
+    // coupling pairs (cell, side) with their destination blocks
+    std::vector<int> pairs;
+    std::vector<void *> cdst;
+    for (int i = 0; i < E; ++i)
+        for (int sd = 0; sd < 4; ++sd) {
+            pairs.push_back(i);
+            pairs.push_back(sd);
+            cdst.push_back(offd_at(i, slot_in(i, neighbor(c->g, i, sd))));
+        }
+    // batched products per forward level and lower slot order (block_ilu.cpp:48-61)
+    const int nlev = (int)L.fptr.size() - 1;
+    L.steps.assign(nlev, {});
+    std::vector<void *> ptrs;
+    struct Pending { int l, q; bool update; size_t off; int n; };
+    std::vector<Pending> pend;
+    size_t max_mult = 1;
+    int max_rows = 1;
+    for (int l = 0; l < nlev; ++l) {
+        max_rows = std::max(max_rows, L.fptr[l + 1] - L.fptr[l]);
+        for (int q = 0; q < 4; ++q) {
+            std::vector<void *> a, b, cc, ua, ub, uc;
+            int k = 0;
+            for (int r = L.fptr[l]; r < L.fptr[l + 1]; ++r) {
+                const int i = frows[r];
+                if (q >= nlower[i]) continue;
+                const int j = ncol[4 * (size_t)i + q];
+                a.push_back(offd_at(i, q));
+                b.push_back(diag_at(j));
+                cc.push_back(reinterpret_cast<void *>((size_t)k++));  // scratch index, resolved below
+                for (int u = nlower[j]; u < 4; ++u) {  // the upper blocks of row j
+                    const int col = ncol[4 * (size_t)j + u], t = slot_in(i, col);
+                    if (t == -2) continue;
+                    ua.push_back(offd_at(i, q));
+                    ub.push_back(offd_at(j, u));
+                    uc.push_back(t == -1 ? diag_at(i) : offd_at(i, t));
+                }
+            }
+            max_mult = std::max(max_mult, (size_t)k);
+            auto add = [&](std::vector<void *> &x, std::vector<void *> &y, std::vector<void *> &z, bool upd) {
+                if (x.empty()) return;
+                pend.push_back({l, q, upd, ptrs.size(), (int)x.size()});
+                ptrs.insert(ptrs.end(), x.begin(), x.end());
+                ptrs.insert(ptrs.end(), y.begin(), y.end());
+                ptrs.insert(ptrs.end(), z.begin(), z.end());
+            };
+            add(a, b, cc, false);
+            add(ua, ub, uc, true);
+        }
+    }
+    L.scratch = c->alloc<char>(max_mult * mm * tsz);
+    for (const auto &pd : pend)  // scratch indices of the products -> addresses
+        if (!pd.update)
+            for (int k = 0; k < pd.n; ++k) {
+                void *&slot = ptrs[pd.off + 2 * pd.n + k];
+                slot = (char *)L.scratch + (size_t)reinterpret_cast<size_t>(slot) * mm * tsz;
+            }
+    void **dev = c->alloc<void *>(std::max<size_t>(ptrs.size() + cdst.size(), 1));
+    ck(cudaMemcpy(dev, ptrs.data(), ptrs.size() * sizeof(void *), cudaMemcpyHostToDevice), "upload ILU pointers");
+    ck(cudaMemcpy(dev + ptrs.size(), cdst.data(), cdst.size() * sizeof(void *), cudaMemcpyHostToDevice),
+       "upload ILU pointers");
+    L.cdst = dev + ptrs.size();
+    for (const auto &pd : pend) {
+        auto &bt = pd.update ? L.steps[pd.l][pd.q].update : L.steps[pd.l][pd.q].mult;
+        bt.n = pd.n;
+        bt.a = dev + pd.off;
+        bt.b = dev + pd.off + pd.n;
+        bt.c = dev + pd.off + 2 * pd.n;
+    }
+    auto upload_int = [&](const std::vector<int> &v) {
+        int *d = c->alloc<int>(v.size());
+        ck(cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice), "upload ILU pattern");
+        return d;
+    };
+    L.ncol = upload_int(ncol);
+    L.nlower = upload_int(nlower);
+    L.frows = upload_int(frows);
+    L.brows = upload_int(brows);
+    L.pairs = upload_int(pairs);
+    L.aug = c->alloc<double>((size_t)max_rows * m * (2 * m + 1));
+    L.inv = c->alloc<double>((size_t)max_rows * mm);
+    L.ydummy = c->alloc<double>((size_t)max_rows * m);
+    L.perm = c->alloc<int>((size_t)max_rows * m);
+    L.work = c->alloc<double>(c->N);
+    blas_ck(cublasCreate(&L.blas), "cublasCreate");
+    blas_ck(cublasSetStream(L.blas, c->stream), "cublasSetStream");
+    L.on = true;
+}
+// C = alpha A B + beta C for every triple of the batch (row-major m x m blocks: the column-major
+// product C^T = B^T A^T).
+template <typename TF> void ilu2_gemm(dgh_ctx *c, const dgh_ctx::Ilu2::Batch &bt, TF alpha, TF beta) {
+    const int m = c->m;
+    if constexpr (sizeof(TF) == 8)
+        blas_ck(cublasDgemmBatched(c->ilu2.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &alpha, (const double *const *)bt.b, m,
+                                   (const double *const *)bt.a, m, &beta, (double *const *)bt.c, m, bt.n),
+                "cublasDgemmBatched");
+    else
+        blas_ck(cublasSgemmBatched(c->ilu2.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &alpha, (const float *const *)bt.b, m,
+                                   (const float *const *)bt.a, m, &beta, (float *const *)bt.c, m, bt.n),
+                "cublasSgemmBatched");
+    c->launched();
+}
+// BlockPreconditioner::refresh + factorize (block_ilu.cpp:48-61) level by level: every pattern
+// block assembled, then per level and lower slot order L_p = A_p A_jj^{-1} and the updates
+// A_it -= L_p A_ju, then the level's diagonal blocks inverted (FP64 pivoted LU).
+template <typename TF> void ilu2_factor(dgh_ctx *c) {
+    auto &L = c->ilu2;
+    const int m = c->m, E = c->cells;
+    TF *diag = (TF *)L.diag;
+    DGH_DISPATCH_N(c->n, {
+        k_dg_assemble<N, TF><<<std::min(E, c->sms * 8), 256, 0, c->stream>>>(diag, c->vol, c->fcache, c->speeds, c->basis,
+                                                                            c->g, c->inv_step, 0, E, c->overint() ? 0 : 1);
+        if (c->overint()) {
+            k_vol_block_q<N, TF><<<std::min(E, c->sms * 4), Q_THREADS, 0, c->stream>>>(diag, m, c->volq, c->bq, c->g, 0, E);
+            c->launched();
+        }
+        k_dg_coupling<N, TF><<<std::min(4 * E, c->sms * 8), 256, 0, c->stream>>>((TF *const *)L.cdst, L.pairs, 4 * E,
+                                                                                c->fcache, c->speeds, c->basis, c->g);
+    });
+    c->launched(2);
+    const int nlev = (int)L.fptr.size() - 1;
+    for (int l = 0; l < nlev; ++l) {
+        for (int q = 0; q < 4; ++q) {
+            const auto &st = L.steps[l][q];
+            if (st.mult.n) {
+                ilu2_gemm<TF>(c, st.mult, TF(1), TF(0));
+                k_copy_blocks<TF><<<std::min(st.mult.n, c->sms * 4), 256, 0, c->stream>>>(
+                    (TF *const *)st.mult.a, (const TF *const *)st.mult.c, st.mult.n, m * m);
+                c->launched();
+            }
+            if (st.update.n) ilu2_gemm<TF>(c, st.update, TF(-1), TF(1));
+        }
+        const int cnt = L.fptr[l + 1] - L.fptr[l];
+        const int *rows = L.frows + L.fptr[l];
+        k_ilu_stage_inverse<TF><<<std::min(cnt, c->sms * 4), 256, 0, c->stream>>>(L.aug, diag, rows, cnt, m);
+        c->launched();
+        launch_lu_left<true>(c, L.aug, (size_t)m * (2 * m + 1), m, 2 * m + 1, cnt, L.perm, ST_SINGULAR, false, nullptr,
+                             L.inv, L.ydummy);
+        k_ilu_store_inverse<TF><<<std::min(cnt, c->sms * 4), 256, 0, c->stream>>>(diag, L.inv, rows, cnt, m);
+        c->launched();
+    }
+}
+// block_ilu.cpp:62-84: forward sweep with L, backward sweep with U and the diagonal inverses.
+template <typename TF> void ilu2_apply(dgh_ctx *c, const double *x, double *z) {
+    auto &L = c->ilu2;
+    const int m = c->m;
+    ck(cudaMemcpyAsync(L.work, x, c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    for (int l = 1; l + 1 < (int)L.fptr.size(); ++l) {  // level 0 rows have no lower neighbours
+        const int cnt = L.fptr[l + 1] - L.fptr[l];
+        k_ilu2_forward<TF><<<cnt, 256, sizeof(double) * 4 * m, c->stream>>>(L.frows + L.fptr[l], cnt, L.nlower, L.ncol,
+                                                                            (const TF *)L.offd, L.work, m);
+    }
+    for (int l = 0; l + 1 < (int)L.bptr.size(); ++l) {
+        const int cnt = L.bptr[l + 1] - L.bptr[l];
+        k_ilu2_backward<TF><<<cnt, 256, sizeof(double) * 5 * m, c->stream>>>(
+            L.brows + L.bptr[l], cnt, L.nlower, L.ncol, (const TF *)L.offd, (const TF *)L.diag, L.work, z, m);
+    }
+    c->launched((int)L.fptr.size() - 2 + (int)L.bptr.size() - 1);
+}
+
 void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     Timed tm(c, DGH_TIMER_PRECOND);
     if (c->d1()) {
@@ -503,8 +737,15 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
         need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->m * c->m;
         need(!c->half16(), "The transposed solve needs FP64 or FP32 factors");
+        need(!c->ilu2d(), "The transposed block ILU(0) is not built");
         if (c->mixed()) launch_solve_t<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
         else launch_solve_t<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+        return;
+    }
+    if (op == DGH_OP_DG && c->ilu2d()) {
+        need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
+        if (c->mixed()) ilu2_apply<float>(c, x, z);
+        else ilu2_apply<double>(c, x, z);
         return;
     }
     if (op == DGH_OP_DG) {
@@ -1087,7 +1328,8 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         const dgh_config &k = *cfg;
         need(k.dim == 1 || k.dim == 2, "Invalid dimension (1 or 2)");
         need(k.preconditioner == 0 || k.preconditioner == 1, "Invalid block preconditioner");
-        need(k.preconditioner == 0 || k.dim == 1, "2D currently supports block-jacobi only");
+        need(k.preconditioner == 0 || k.dim == 1 || k.method == DGH_METHOD_DG,
+             "2D block ILU(0) is built for the DG operator only (method dg)");
         need(k.condense32 == 0 || (k.condense32 == 1 && k.dim == 2), "FP32 condensation is a 2D HDG option (0 or 1)");
         need(k.forcing == 0 || k.forcing == 1, "Invalid forcing (0 or 1)");
         // config.cpp:6-22 (dg_hdg_1d/src/config.cpp:6-21 in 1D)
@@ -1236,7 +1478,9 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         k_fill_trace_mass<<<(unsigned)((c->NT + tb - 1) / tb), tb, 0, c->stream>>>(c->inv_trace_mass, c->basis, c->g, n, c->NT);
         c->launched(2);
         const size_t tsz = c->mixed() ? sizeof(float) : sizeof(double);
-        if (c->has_dg()) {
+        if (c->has_dg() && c->ilu2d()) {  // block ILU(0) factors instead of the block-Jacobi pool
+            c->dg_perm = c->alloc<int>((size_t)c->cells * c->m);
+        } else if (c->has_dg()) {
             if (c->half16()) {
                 c->dg_pool = c->alloc<char>((size_t)c->cells * c->m * pad8(c->m) * sizeof(__half));
                 c->dg_scale = c->alloc<float>((size_t)c->cells * c->m);
@@ -1304,6 +1548,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
             const int P = (c->m + LL_NB - 1) / LL_NB;
             c->lu_tri = c->alloc<double>((size_t)c->lu_grid * P * LL_TRI);
         }
+        if (c->has_dg() && c->ilu2d()) ilu2_build(c);
         c->sync();
     });
     if (rc != DGH_OK) {
@@ -1327,6 +1572,7 @@ int dgh_ctx_destroy(dgh_ctx *c) {
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto &g : c->cycle)
         if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (c->ilu2.blas) cublasDestroy(c->ilu2.blas);
     if (c->aux) cudaStreamDestroy(c->aux);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1687,9 +1933,29 @@ int dgh_dg_apply_T(dgh_ctx *c, const double *w, double *jtw) {
 int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
     return guard(c, [&] {
         need(c->linearised, "Refresh the volume Jacobian before assembling a block");
-        need(row == col && row >= 0 && row < c->cells, "Only diagonal cell blocks are exposed on the device");
+        need(row >= 0 && row < c->cells && col >= 0 && col < c->cells, "Invalid block index");
+        int side = -1;
+        if (row != col && !c->d1())
+            for (int sd = 0; sd < 4; ++sd)
+                if (neighbor(c->g, row, sd) == col) side = sd;
+        need(row == col || side >= 0, "Only diagonal and face-neighbour cell blocks exist on the device");
         double *tmp = c->alloc<double>((size_t)c->m * c->m);
-        if (c->d1()) {
+        if (side >= 0) {  // coupling block (dg_operator.cpp:22-48, col != row)
+            double **dst = c->alloc<double *>(1);
+            int *pair = c->alloc<int>(2);
+            const int hp[2] = {row, side};
+            ck(cudaMemcpy(dst, &tmp, sizeof(double *), cudaMemcpyHostToDevice), "copy");
+            ck(cudaMemcpy(pair, hp, sizeof hp, cudaMemcpyHostToDevice), "copy");
+            DGH_DISPATCH_N(c->n, {
+                k_dg_coupling<N, double><<<1, 256, 0, c->stream>>>(dst, pair, 1, c->fcache, c->speeds, c->basis, c->g);
+            });
+            c->sync();
+            for (void *q : {(void *)pair, (void *)dst}) {  // the two small allocations, newest first
+                ck(cudaFree(q), "cudaFree");
+                c->owned.pop_back();
+                c->bytes -= 16;
+            }
+        } else if (c->d1()) {
             DGH_DISPATCH_N(c->n, {
                 k1_dg_assemble<N, double><<<grid1((long long)c->m * c->m), K1_THREADS, 0, c->stream>>>(
                     tmp, c->vol, c->fcache, c->b1, c->g1, c->inv_step, row, 1);
@@ -2005,7 +2271,14 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             (dg ? c->dg_factored : c->face_factored) = true;
             return;
         }
-        if (op == DGH_OP_DG) {
+        if (op == DGH_OP_DG && c->ilu2d()) {
+            need(c->ilu2.on, "context has no DG operator");
+            need(c->linearised, "Refresh the volume Jacobian before assembling a block");
+            if (c->mixed()) ilu2_factor<float>(c);
+            else ilu2_factor<double>(c);
+            c->check_status();
+            c->dg_factored = true;
+        } else if (op == DGH_OP_DG) {
             need(c->dg_pool, "context has no DG operator");
             need(c->linearised, "Refresh the volume Jacobian before assembling a block");
             if (c->dg_variant < 0 && c->half16()) c->dg_variant = 0;  // one factorisation form

@@ -18,7 +18,7 @@ struct Settings {
 constexpr const char *kUsage =
     "2D periodic tensor-product Euler DG / condensed HDG on one B200\n"
     "--nx NX --ny NY --testcase diagonal|wave|axis --k K --quad Q --cfl C (--T T | --steps N)\n"
-    "--method dg|hdg|both --linear gmres --precond block-jacobi\n"
+    "--method dg|hdg|both --linear gmres --precond block-jacobi|block-ilu0 (dg)\n"
     "--ordering natural --restart N --max-linear N --max-newton N\n"
     "--ntol R --ltol R --safety S --prefix PATH\n"
     "--integrator ssp-dirk3|be --newton-steps N --warmup-updates N\n"
@@ -30,6 +30,7 @@ Settings settings_from(int argc, char **argv) {
     dgh_config &c = s.cfg;
     dgh_config_default(&c);
     int time_given = 0, steps_given = 0, direct = 0, method = -1, integrator = DGH_INTEGRATOR_DIRK3, testcase = 0;
+    int ilu = 0, colamd = 0;
     std::string method_word = "both", integrator_word = "ssp-dirk3", testcase_word = "diagonal";
     using namespace dghcli;
     const std::vector<Flag> flags = {
@@ -62,9 +63,10 @@ Settings settings_from(int argc, char **argv) {
         }),
         text("--forcing", [&](const std::string &v) { c.forcing = pick(v, {"0", "1"}, "Invalid forcing"); }),
         text("--linear", [&](const std::string &v) { direct = pick(v, {"gmres", "direct"}, "Invalid linear solver"); }),
-        text("--ordering", [&](const std::string &v) { pick(v, {"natural", "colamd"}, "Invalid ordering"); }),
+        text("--ordering", [&](const std::string &v) { colamd = pick(v, {"natural", "colamd"}, "Invalid ordering"); }),
         text("--precond", [&](const std::string &v) {
-            pick(v, {"block-jacobi"}, "2D currently supports block-jacobi only");
+            // block-ilu0 is this front end's extension (the reference's 2D front end has block Jacobi only)
+            ilu = pick(v, {"block-jacobi", "block-ilu0"}, "2D currently supports block-jacobi only");
         }),
         on("--no-save-solution", [&] { s.save_solution = false; }),
         on("--timing-only", [&] { s.timing_only = true; }),
@@ -80,6 +82,9 @@ Settings settings_from(int argc, char **argv) {
     testcase = pick(testcase_word, {"diagonal", "wave", "axis"}, "Invalid testcase");
     method = pick(method_word, {"dg", "hdg", "both"}, "Method must be dg, hdg, or both");
     require(!direct, "The dense --linear direct reference is a CPU-only check; use gmres");
+    require(!(ilu && colamd), "The device solver implements the natural block ordering only");
+    require(!ilu || method == 0, "2D block ILU(0) is built for the DG operator only (method dg)");
+    c.preconditioner = ilu;
     c.integrator = integrator;
     c.testcase = testcase == 0 ? DGH_TEST_DIAGONAL : testcase == 1 ? DGH_TEST_WAVE : DGH_TEST_AXIS;
     s.methods = method == 0 ? DGH_METHOD_DG : method == 1 ? DGH_METHOD_HDG : DGH_METHOD_BOTH;

@@ -221,6 +221,11 @@ int oracle_dg_precond_refresh_ilu(void *hv) {
     });
 }
 // op 0: DG Jv with block-Jacobi; op 1: Schur apply with face block-Jacobi; op 2: DG Jv with the
+// z = M^{-1} x with the 2D block ILU(0) factors of oracle_dg_precond_refresh_ilu
+int oracle_dg_precond_apply_ilu(void *hv, const double *x, double *z) {
+    auto *h = static_cast<Handle *>(hv);
+    return guard([&] { Vec o; h->ilu_dg->apply(vec(x, h->p->size()), o); out(o, z); });
+}
 // 2D block ILU(0) of oracle_dg_precond_refresh_ilu
 int oracle_gmres(void *hv, int op, int restart, const double *rhs, double *x, int limit, double tol,
                  int *iters, double *rel, double *residual) {

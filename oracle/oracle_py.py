@@ -178,6 +178,12 @@ class Oracle:
         """2D block ILU(0) of the DG Jacobian on the cartesian block graph (GMRES op 2)."""
         self._call("oracle_dg_precond_refresh_ilu")
 
+    def dg_precond_apply_ilu(self, x) -> np.ndarray:
+        """z = M^{-1} x with the 2D block ILU(0) factors of dg_precond_refresh_ilu."""
+        o = np.zeros(self.size)
+        self._call("oracle_dg_precond_apply_ilu", _p(np.ascontiguousarray(x)), _p(o))
+        return o
+
     def dg_precond_apply(self, x) -> np.ndarray:
         o = np.zeros(self.size)
         self._call("oracle_dg_precond_apply", _p(np.ascontiguousarray(x)), _p(o))
@@ -358,6 +364,12 @@ class Oracle1D:
 
     def dg_precond_refresh(self) -> None:
         self._call("oracle1d_dg_precond_refresh")
+
+    def dg_precond_apply_ilu(self, x) -> np.ndarray:
+        """z = M^{-1} x with the 2D block ILU(0) factors of dg_precond_refresh_ilu."""
+        o = np.zeros(self.size)
+        self._call("oracle_dg_precond_apply_ilu", _p(np.ascontiguousarray(x)), _p(o))
+        return o
 
     def dg_precond_apply(self, x) -> np.ndarray:
         return self._vol("oracle1d_dg_precond_apply", x)

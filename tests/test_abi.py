@@ -103,14 +103,17 @@ def test_1d_cli_validates_flags_before_device_work():
 
 def test_2d_cli_validates_flags_before_device_work():
     """The 2D front end parses dg_hdg_2d's flags with the reference's texts (config.cpp:23-122):
-    block-jacobi is its only 2D preconditioner, and the dense direct solve stays a CPU check."""
+    block-jacobi is the reference's only 2D preconditioner (block-ilu0 is this front end's DG-only
+    extension, natural ordering), and the dense direct solve stays a CPU check."""
     import subprocess
 
     from dg_hdg_euler_cpp_b200 import BIN_PATH
 
     if not BIN_PATH.exists():
         pytest.skip("dgh2d not built")
-    for args, msg in [(["--precond", "block-ilu0"], "2D currently supports block-jacobi only"),
+    for args, msg in [(["--precond", "block-ilu1"], "2D currently supports block-jacobi only"),
+                      (["--precond", "block-ilu0"], "DG operator only"),
+                      (["--precond", "block-ilu0", "--method", "dg", "--ordering", "colamd"], "natural block ordering"),
                       (["--linear", "direct"], "CPU-only"), (["--ordering", "rcm"], "Invalid ordering"),
                       (["--T", ".1", "--steps", "2"], "Choose either --T or --steps"),
                       (["--integrator", "rk4"], "Invalid integrator"), (["--testcase", "vortex"], "Invalid testcase"),
