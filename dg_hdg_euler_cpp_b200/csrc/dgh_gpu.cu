@@ -160,7 +160,7 @@ struct dgh_ctx {
         };
         std::vector<std::array<Step, 4>> steps;
         void *scratch = nullptr;
-        double *aug = nullptr, *inv = nullptr, *ydummy = nullptr, *work = nullptr;
+        double *aug = nullptr, *inv = nullptr, *ydummy = nullptr, *work = nullptr, *tvec = nullptr;
         int *perm = nullptr;
         cublasHandle_t blas = nullptr;
     } ilu2;
@@ -634,6 +634,7 @@ void ilu2_build(dgh_ctx *c) {
     L.ydummy = c->alloc<double>((size_t)max_rows * m);
     L.perm = c->alloc<int>((size_t)max_rows * m);
     L.work = c->alloc<double>(c->N);
+    L.tvec = c->alloc<double>(c->N);
     blas_ck(cublasCreate(&L.blas), "cublasCreate");
     blas_ck(cublasSetStream(L.blas, c->stream), "cublasSetStream");
     L.on = true;
@@ -692,22 +693,30 @@ template <typename TF> void ilu2_factor(dgh_ctx *c) {
         c->launched();
     }
 }
-// block_ilu.cpp:62-84: forward sweep with L, backward sweep with U and the diagonal inverses.
+// block_ilu.cpp:62-84: forward sweep with L, backward sweep with U and the diagonal inverses,
+// level by level; every level's block rows are split over CTAs of ILU_ROWS output rows.
 template <typename TF> void ilu2_apply(dgh_ctx *c, const double *x, double *z) {
     auto &L = c->ilu2;
-    const int m = c->m;
+    const int m = c->m, chunks = (m + ILU_ROWS - 1) / ILU_ROWS;
+    const TF *offd = (const TF *)L.offd, *diag = (const TF *)L.diag;
     ck(cudaMemcpyAsync(L.work, x, c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    int launches = 0;
     for (int l = 1; l + 1 < (int)L.fptr.size(); ++l) {  // level 0 rows have no lower neighbours
         const int cnt = L.fptr[l + 1] - L.fptr[l];
-        k_ilu2_forward<TF><<<cnt, 256, sizeof(double) * 4 * m, c->stream>>>(L.frows + L.fptr[l], cnt, L.nlower, L.ncol,
-                                                                            (const TF *)L.offd, L.work, m);
+        k_ilu2_rows<TF, 0><<<cnt * chunks, 256, sizeof(double) * 4 * m, c->stream>>>(
+            L.frows + L.fptr[l], cnt, chunks, L.nlower, L.ncol, offd, diag, L.work, L.tvec, z, m);
+        ++launches;
     }
     for (int l = 0; l + 1 < (int)L.bptr.size(); ++l) {
         const int cnt = L.bptr[l + 1] - L.bptr[l];
-        k_ilu2_backward<TF><<<cnt, 256, sizeof(double) * 5 * m, c->stream>>>(
-            L.brows + L.bptr[l], cnt, L.nlower, L.ncol, (const TF *)L.offd, (const TF *)L.diag, L.work, z, m);
+        const int *rows = L.brows + L.bptr[l];
+        k_ilu2_rows<TF, 1><<<cnt * chunks, 256, sizeof(double) * 4 * m, c->stream>>>(rows, cnt, chunks, L.nlower, L.ncol,
+                                                                                     offd, diag, L.work, L.tvec, z, m);
+        k_ilu2_rows<TF, 2><<<cnt * chunks, 256, sizeof(double) * m, c->stream>>>(rows, cnt, chunks, L.nlower, L.ncol,
+                                                                                 offd, diag, L.work, L.tvec, z, m);
+        launches += 2;
     }
-    c->launched((int)L.fptr.size() - 2 + (int)L.bptr.size() - 1);
+    c->launched(launches);
 }
 
 void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {

@@ -2,7 +2,7 @@
 // ordering (common/src/linalg/block_ilu.cpp:15-84 restated for the 2D operator; the reference's
 // 2D front end offers block Jacobi only).  Kernels: the face coupling blocks of DGOperator::block
 // (dg_operator.cpp:22-48, col != row), the level-scheduled forward and backward sweeps of the
-// application, and the gathers of the factorisation.  The batched block products of the
+// application, and the block copies and inverse staging of the factorisation.  The batched block products of the
 // factorisation are plain GEMMs (cuBLAS), and the diagonal inverses come from k_lu_left.
 #pragma once
 #include "dgh_kernels_dg.cuh"
@@ -97,66 +97,57 @@ __global__ void k_ilu_store_inverse(TF *__restrict__ diag, const double *__restr
     }
 }
 
-// Block row product acc[r] = sum_j blk[r][j] x[j] for the CTA's m rows: warp per row, lanes over
-// the row's contiguous entries, FP64 accumulation.
-template <typename TF>
-__device__ inline double row_dot(const TF *__restrict__ row, const double *__restrict__ x, int m) {
-    const int lane = threadIdx.x & 31;
-    double acc = 0;
-    for (int j = lane; j < m; j += 32) acc += (double)row[j] * x[j];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    return acc;
-}
+// The sweeps of one level, split over CTAs: CTA (k, chunk) computes output rows
+// [ILU_ROWS chunk, ILU_ROWS (chunk + 1)) of the level's k-th block row, one warp per output row
+// with 16-byte loads of the block rows (all blocks of the output row in flight together) and the
+// right-hand-side segments staged in shared memory.
+//   MODE 0 (forward, block_ilu.cpp:70-74):   work_i -= sum_{lower p} L_p work_col(p)
+//   MODE 1 (backward, the upper products):   t_i = work_i - sum_{upper p} U_p z_col(p)
+//   MODE 2 (backward, the diagonal):         z_i = A_ii^{-1} t_i
+constexpr int ILU_ROWS = 32;
+template <typename TF> struct IluVec;
+template <> struct IluVec<double> { using V = double2; static constexpr int W = 2; };
+template <> struct IluVec<float> { using V = float4; static constexpr int W = 4; };
 
-// Forward sweep of one level (block_ilu.cpp:70-74): for each listed row i,
-// work_i -= sum over its lower slots p of L_p work_col(p).  One CTA per row.
-template <typename TF>
+template <typename TF, int MODE>
 __global__ void __launch_bounds__(256)
-k_ilu2_forward(const int *__restrict__ rows, int count, const int *__restrict__ nlower, const int *__restrict__ ncol,
-               const TF *__restrict__ offd, double *__restrict__ work, int m) {
-    extern __shared__ double xs[];  // the lower neighbours' work segments, 4 m at most
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = blockIdx.x; k < count; k += gridDim.x) {
-        const int i = rows[k], nl = nlower[i];
-        __syncthreads();
-        for (int p = 0; p < nl; ++p)
-            for (int j = threadIdx.x; j < m; j += blockDim.x) xs[p * m + j] = work[(size_t)ncol[4 * i + p] * m + j];
-        __syncthreads();
-        for (int r = warp; r < m; r += blockDim.x / 32) {
-            double s = 0;
-            for (int p = 0; p < nl; ++p) s += row_dot(offd + ((size_t)(4 * i + p) * m + r) * m, xs + p * m, m);
-            if (lane == 0) work[(size_t)i * m + r] -= s;
-        }
+k_ilu2_rows(const int *__restrict__ rows, int count, int chunks, const int *__restrict__ nlower,
+            const int *__restrict__ ncol, const TF *__restrict__ offd, const TF *__restrict__ diag,
+            double *work, double *__restrict__ t, double *__restrict__ z, int m) {
+    using V = typename IluVec<TF>::V;
+    constexpr int W = IluVec<TF>::W;
+    extern __shared__ __align__(16) double xs[];  // up to 4 segments of m
+    const int k = blockIdx.x / chunks, chunk = blockIdx.x % chunks;
+    if (k >= count) return;
+    const int i = rows[k], nl = nlower[i];
+    const int p0 = MODE == 0 ? 0 : MODE == 1 ? nl : 0, p1 = MODE == 0 ? nl : MODE == 1 ? 4 : 1;
+    for (int p = p0; p < p1; ++p) {
+        const double *src = MODE == 0 ? work + (size_t)ncol[4 * i + p] * m
+                            : MODE == 1 ? z + (size_t)ncol[4 * i + p] * m : t + (size_t)i * m;
+        for (int j = threadIdx.x; j < m; j += blockDim.x) xs[(p - p0) * m + j] = src[j];
     }
-}
-
-// Backward sweep of one level (block_ilu.cpp:75-80): for each listed row i,
-// z_i = A_ii^{-1} (work_i - sum over its upper slots p of U_p z_col(p)), the inverse stored over
-// the diagonal block.  One CTA per row.
-template <typename TF>
-__global__ void __launch_bounds__(256)
-k_ilu2_backward(const int *__restrict__ rows, int count, const int *__restrict__ nlower, const int *__restrict__ ncol,
-                const TF *__restrict__ offd, const TF *__restrict__ diag, const double *__restrict__ work,
-                double *__restrict__ z, int m) {
-    extern __shared__ double xs[];  // the upper neighbours' z segments (4 m at most), then t (m)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *t = xs + 4 * m;
-    for (int k = blockIdx.x; k < count; k += gridDim.x) {
-        const int i = rows[k], nl = nlower[i];
-        __syncthreads();
-        for (int p = nl; p < 4; ++p)
-            for (int j = threadIdx.x; j < m; j += blockDim.x) xs[p * m + j] = z[(size_t)ncol[4 * i + p] * m + j];
-        __syncthreads();
-        for (int r = warp; r < m; r += blockDim.x / 32) {
-            double s = 0;
-            for (int p = nl; p < 4; ++p) s += row_dot(offd + ((size_t)(4 * i + p) * m + r) * m, xs + p * m, m);
-            if (lane == 0) t[r] = work[(size_t)i * m + r] - s;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, G = m / W;
+    for (int r = chunk * ILU_ROWS + warp; r < min(m, (chunk + 1) * ILU_ROWS); r += blockDim.x / 32) {
+        double acc = 0;
+        for (int p = p0; p < p1; ++p) {
+            const TF *blk = MODE == 2 ? diag + (size_t)i * m * m : offd + (size_t)(4 * i + p) * m * m;
+            const V *row = reinterpret_cast<const V *>(blk + (size_t)r * m);
+            const double *x = xs + (p - p0) * m;
+            for (int g = lane; g < G; g += 32) {
+                const V a = row[g];
+                const TF *e = reinterpret_cast<const TF *>(&a);
+#pragma unroll
+                for (int w = 0; w < W; ++w) acc += (double)e[w] * x[g * W + w];
+            }
         }
-        __syncthreads();
-        for (int r = warp; r < m; r += blockDim.x / 32) {
-            const double s = row_dot(diag + ((size_t)i * m + r) * m, t, m);
-            if (lane == 0) z[(size_t)i * m + r] = s;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            const size_t at = (size_t)i * m + r;
+            if (MODE == 0) work[at] -= acc;
+            else if (MODE == 1) t[at] = work[at] - acc;
+            else z[at] = acc;
         }
     }
 }

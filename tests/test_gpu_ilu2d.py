@@ -26,7 +26,9 @@ def direction(n, a=.31, b=.79):
 
 
 def rel(a, b):
-    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / np.max(np.abs(b)))
+    a, b = np.asarray(a), np.asarray(b)
+    scale = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / scale) if scale > 0 else float(np.max(np.abs(a)))
 
 
 def neighbours(cell, nx, ny):
