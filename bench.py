@@ -11,10 +11,12 @@ warm-up update), updates 2-4 timed.  Per configuration (method x precision):
   timed   : K updates, in ceil(K/3) protocol units; each unit's timed updates are bracketed by
             barrier + synchronize and CUDA events on the library's stream, and the K timed
             updates are always protocol updates 2-4 (never post-convergence updates 5+).
-value = (K_dg + K_hdg) / (t_dg + t_hdg) for the mixed-precision (FP32 block-Jacobi factors,
-FP64 everything else) DG and HDG solves; the FP64 forms and the per-method numbers are in
-"breakdown", and the mixed-vs-FP64 speed-up, state error and Krylov change per method at the
-top level.  e2e repeats the timed updates through the C ABI with host buffers
+value = (K_dg + K_hdg) / (t_dg + t_hdg) over the fastest reduced-precision DG form and the
+fastest reduced-precision HDG form that keep the reference's linear tolerance (FORMS below,
+forcing 0); the same over the forms that may also stop at the acceptance round-off floor is
+"with_forcing_floor".  The FP64 forms and the per-form numbers are in "breakdown", and each
+reduced form's speed-up, state error and Krylov change against FP64 at the top level.  e2e
+repeats the headline forms' timed updates through the C ABI with host buffers
 (dgh_newton_update_host: state H2D, update, state D2H every step).
 
 cpu_baseline and --impl reference time the reference algorithm's CPU implementation (the oracle
@@ -720,7 +722,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot_ms / tot_upd, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (FP32 block-Jacobi factors, and FP32 condensation in mixed32, in the reduced forms)", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64 (reduced forms: FP32 block-Jacobi factors, FP16 DG factors in mixed16, FP32 "
+                 "condensation in mixed32; residuals, J.v, Arnoldi and acceptance in FP64)", "data": "synthetic",
         "config": {"workload": f"{args.nx}x{args.nx} k={args.k} rotated simple wave, BE CFL5, GMRES(20), exact "
                                f"block-Jacobi, ntol=ltol={args.ltol:g}, one Newton update per step, timed updates "
                                f"are protocol updates 2-4 of ceil(K/3) reset-and-warm units; value combines "
