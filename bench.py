@@ -475,8 +475,10 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
     """The uneven batch (members from seeds 0..members-1: k in {2,4,6,8}, N^2 meshes with N in
     {32,64,96,128}, DG or HDG, amplitude-scaled initial states, BE CFL 5, GMRES(30), mixed
     precision): `updates` Newton updates of every member run one member at a time, then all
-    members together through dgh_batch; member-updates per second for both and whether every
-    member's rows agree bitwise between the two."""
+    members together through dgh_batch (independent solves, each member on its own stream), then
+    through dgh_batch with the DG members' GMRES solves in lockstep (every Arnoldi phase one
+    launch over them); member-updates per second for each and whether every member's rows agree
+    bitwise with its one-at-a-time run."""
     from dg_hdg_euler_cpp_b200.solver import Batch, batch_member, perturb
 
     draws = [batch_member(s) for s in range(members)]
@@ -486,8 +488,9 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
         return [perturb(b.initial(j), cfgs[i]["nx"], cfgs[i]["ny"], cfgs[i]["k"], draws[i]["amplitude"])
                 for j, i in enumerate(idx)]
 
-    def timed(b, u0):
+    def timed(b, u0, lockstep=False):
         b.gmres_graph(graph)
+        b.lockstep(lockstep)
         b.stage_begin(u0)
         b.update()  # warm-up update, then restart the stage
         b.stage_begin(u0)
@@ -512,10 +515,16 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
         b.lib.dgh_device_bytes(b.member_ctx(i), ctypes.byref(by))
         dev_gb += by.value / 1e9
     bat_s, bat_rows = timed(b, states(b, list(range(members))))
+    lock_s, lock_rows = timed(b, states(b, list(range(members))), lockstep=True)
+    lock_report = b.lockstep_report()
     b.close()
     torch.cuda.empty_cache()
-    same = all(bat_rows[u][i][k] == seq_rows[i][u][k] for i in range(members) for u in range(updates)
-               for k in ("krylov_iterations", "residual_physical_rms", "damping"))
+
+    def same_as_single(rows):
+        return all(rows[u][i][k] == seq_rows[i][u][k] for i in range(members) for u in range(updates)
+                   for k in ("krylov_iterations", "residual_physical_rms", "damping"))
+
+    same = same_as_single(bat_rows)
     work = members * updates
     return {"members": [{"seed": d["seed"], "k": d["config"]["k"], "n": d["config"]["nx"], "method": d["config"]["method"],
                          "amplitude": d["amplitude"], "krylov": [seq_rows[i][u]["krylov_iterations"]
@@ -525,7 +534,16 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
             "one_at_a_time_s": seq_s, "batched_s": bat_s,
             "one_at_a_time_member_updates_per_s": work / seq_s, "batched_member_updates_per_s": work / bat_s,
             "speedup": seq_s / bat_s, "bitwise_equal_rows": same,
-            "gmres_cycles": "cuda_graph" if graph else "stepped"}
+            "gmres_cycles": "cuda_graph" if graph else "stepped",
+            "lockstep": {"seconds": lock_s, "member_updates_per_s": work / lock_s,
+                         "speedup_vs_one_at_a_time": seq_s / lock_s,
+                         "bitwise_equal_rows": same_as_single(lock_rows),
+                         "dg_members": sum(1 for c in cfgs if c["method"] == "dg"),
+                         "group": lock_report,
+                         "note": "DG members' GMRES cycles in lockstep, " +
+                                 ("each restart cycle one CUDA graph launch whose Arnoldi steps run while any member "
+                                  "continues" if graph else "stepped: the host reads one continue flag per member per "
+                                  "Arnoldi step") + "; HDG members solve independently"}}
 
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}

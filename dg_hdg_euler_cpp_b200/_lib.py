@@ -113,6 +113,8 @@ SIGNATURES = {
     "dgh_hdg_retarget": (ctypes.c_int, [_VP, _VP]),
     "dgh_gmres": (ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, ctypes.c_int, ctypes.c_double, _I, _D]),
     "dgh_autotune_report": (ctypes.c_int, [_VP, _D]),
+    "dgh_autotune_shapes": (ctypes.c_int, [_VP, _D]),
+    "dgh_shape_set": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "dgh_gmres_graph_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dgh_gmres_residual": (_VP, [_VP, ctypes.c_int]),
     "dgh_integrator_create": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_VP)]),
@@ -140,6 +142,14 @@ SIGNATURES = {
     "dgh_batch_stage_begin": (ctypes.c_int, [_VP, _VP, _D, _I]),
     "dgh_batch_newton_update": (ctypes.c_int, [_VP, ctypes.POINTER(dgh_update_stats), _I]),
     "dgh_batch_download": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
+    "dgh_batch_lockstep": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "dgh_batch_lockstep_report": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
+    "dgh_lockstep_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.POINTER(_VP)]),
+    "dgh_lockstep_destroy": (ctypes.c_int, [_VP]),
+    "dgh_lockstep_error": (ctypes.c_char_p, []),
+    "dgh_lockstep_begin": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "dgh_lockstep_leave": (ctypes.c_int, [_VP, _VP]),
+    "dgh_lockstep_report": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "dgh_residual_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             _VP, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),
 }

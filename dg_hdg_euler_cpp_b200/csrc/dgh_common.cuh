@@ -15,6 +15,18 @@ constexpr int NVAR = 4;
 constexpr int NFACES = 4;
 constexpr int MAXN = 9;
 
+// Explicitly rounded arithmetic.  The compiler never fuses these into FMAs of its own choosing,
+// so a kernel body written with them computes the same bits in every kernel it is inlined into
+// (the single-problem kernels and the batched kernels of a lockstep batch share their bodies).
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
 // Status bits raised by kernels; the host maps each to the reference's require() text.
 enum StatusBits : int {
     ST_FROZEN_FACE = 1 << 0,   // "Invalid frozen face state"          physics.cpp:108-109

@@ -13,11 +13,13 @@
 #include "dgh_kernels_krylov.cuh"
 #include "dgh_kernels_lu.cuh"
 #include "dgh_kernels_lu2.cuh"
+#include "dgh_kernels_lockstep.cuh"
 #include "dgh_kernels_q.cuh"
 
 #include <cublas_v2.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <array>
 #include <cmath>
 #include <cstddef>
@@ -174,11 +176,21 @@ struct dgh_ctx {
     // tuning times
     int dg_variant = -1, hdg_variant = -1;
     double tune_ms[4] = {0, 0, 0, 0};
+    // grid shape of the DG block solves (solve_grid; -1 until the first DG refresh) and its tuning times
+    int solve_shape = -1;
+    double solve_ms[2] = {0, 0};
+    // CTAs per SM of the fused DG factorisation (1 or 2; -1 until the first fused refresh): with
+    // 1 the per-CTA FP64 slots fit L2, with 2 twice the warps hide the panel latencies
+    int fused_ctas = -1;
+    double fused_ms[2] = {0, 0};
     // GMRES
     double *V = nullptr, *gw = nullptr, *gz = nullptr, *gres[3] = {nullptr, nullptr, nullptr}, *gcoef = nullptr;
     double *g_rhs = nullptr, *g_x = nullptr;  // the solve's own copies of rhs and x (fixed graph operands)
     GmresDev *gdev = nullptr;
     long long vld = 0;
+    // lockstep batch this context's DG GMRES solves join while a session is open (-1: none)
+    dgh_lockstep *ls = nullptr;
+    int ls_index = -1;
     // one captured restart cycle per operator (conditional Arnoldi steps), rebuilt when the
     // captured stage scalar (1/tau, a kernel argument of J*v) changes
     struct CycleGraph {
@@ -268,6 +280,51 @@ struct dgh_ctx {
             if (s & ST_LU_INPUT) fail(DGH_ERR_SINGULAR, "Nonfinite block LU input");
             fail(DGH_ERR_CUDA, "unknown device status");
         }
+    }
+};
+
+// A lockstep group of DG GMRES solves (dgh_kernels_lockstep.cuh): the member contexts in table
+// order (sorted by degree, so every degree and every factor layout is one contiguous range of
+// the table), the launch plan, and the rendezvous of a session, in which each expected member
+// brings one DG GMRES solve.  The member that completes the count issues the whole lockstep
+// solve on the group's stream; the others wait, then continue on their own streams.
+struct dgh_lockstep {
+    int device = 0, restart = 0, precision = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t finished = nullptr;
+    std::vector<dgh_ctx *> members;
+    struct Range {
+        int first = 0, count = 0, key = 0, blocks = 0;
+        size_t smem = 0;
+    };
+    std::vector<Range> degrees;  // J·v launches: key = n (nodes per direction)
+    std::vector<Range> layouts;  // block solves: key 0 FP64, 1 FP32, 2 FP32 narrow (m < 64), 3 FP16
+    int red_total = 0;
+    LsMember *table = nullptr, *host = nullptr;  // device table and its pinned host image
+    int *flags = nullptr, *flags_host = nullptr;
+    LsTail *tails = nullptr, *tails_host = nullptr;
+    struct Slot {
+        bool arrived = false, withdrawn = false, trivial = false;
+        double tol = 0, rhs_norm = 0, rel = 0;
+        int limit = 0, iters = 0, code = DGH_OK;
+        std::string msg;
+        cudaEvent_t ready = nullptr;
+    };
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv;
+    bool open = false;
+    int expected = 0, arrived = 0, withdrawn = 0;
+    uint64_t generation = 0;
+    int64_t sessions = 0, cycles = 0, steps = 0, launches = 0;
+    // the restart cycle captured once as a CUDA graph (used when every member replays its own
+    // cycles as graphs): the kernels read the member table, so one graph serves every session
+    cudaGraphExec_t cycle = nullptr;
+    cudaStream_t aux = nullptr;
+    int graph_fixed = 0, graph_step = 0;
+    void launched(int k = 1) {
+        launches += k;
+        ck(cudaGetLastError(), "kernel launch");
     }
 };
 
@@ -402,7 +459,8 @@ template <int N> void launch_dg_fused(dgh_ctx *c, int first, int count) {
     allow_dynamic_smem((const void *)k_lu_left<false, N>, smem);
     int per_sm = 0;
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_left<false, N>, LL_THREADS, smem), "occupancy");
-    const int grid = std::min(count, std::min(c->dg_slot_count, c->sms * std::max(1, per_sm)));
+    const int per = std::min(std::max(1, per_sm), c->fused_ctas > 0 ? c->fused_ctas : 2);
+    const int grid = std::min(count, std::min(c->dg_slot_count, c->sms * per));
     need(grid <= c->lu_grid, "fused factorisation grid exceeds the LU scratch");
     LLFuse fu;
     fu.vol = c->vol;
@@ -440,26 +498,38 @@ void launch_lu_narrow(dgh_ctx *c, TF *pool, int m, int count, int *perm, int bit
     k_lu_narrow<TF><<<grid, NARROW_THREADS, smem, c->stream>>>(pool, m, count, perm, c->status, bit);
     c->launched();
 }
+// Grid of a one-warp-per-block solve over `count` blocks with `wpc` warps per CTA and `resident`
+// CTAs per SM.  Shape 0 fills every resident CTA slot, so the last round of blocks runs on the
+// few warps whose share is one block larger; shape 1 takes the fewest CTAs that keep the same
+// number of rounds, so every warp solves the same number of blocks (a few one less) with fewer
+// warps in flight.  Which is faster depends on the degree and the block count (the autotuner's
+// solve-shape kind).
+int solve_grid(const dgh_ctx *c, long long count, int wpc, int resident, int shape) {
+    const long long want = (count + wpc - 1) / wpc;
+    const long long full = std::min<long long>(want, (long long)c->sms * std::max(1, resident));
+    if (shape != 1 || full <= 0) return (int)full;
+    const long long rounds = (count + full * wpc - 1) / (full * wpc);
+    return (int)((count + wpc * rounds - 1) / (wpc * rounds));
+}
 // One warp per block; enough warps for every SM to keep its warp slots (and their loads) busy.
 // FP32 blocks narrower than two slabs (the HDG face blocks) use the register-held diagonal rows.
 template <typename TF, bool DIAG>
 void launch_solve_as(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
-                     double *z) {
+                     double *z, int shape) {
     constexpr int wpc = SOLVE_THREADS / 32;
     const size_t smem = sizeof(TF) * (size_t)m * wpc;
-    const int want = (count + wpc - 1) / wpc;
     int resident = 0;
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve<TF, DIAG>, SOLVE_THREADS, smem), "occupancy");
-    const int grid = std::min(want, c->sms * std::max(1, resident));
+    const int grid = solve_grid(c, count, wpc, resident, shape);
     k_lu_solve<TF, DIAG><<<grid, SOLVE_THREADS, smem, c->stream>>>(pool, perm, stride, m, count, x, z);
     c->launched();
 }
 template <typename TF>
 void launch_solve(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, int m, int count, const double *x,
-                  double *z) {
+                  double *z, int shape = 0) {
     if constexpr (sizeof(TF) == 4)
-        if (m < 64) return launch_solve_as<TF, true>(c, pool, perm, stride, m, count, x, z);
-    launch_solve_as<TF, false>(c, pool, perm, stride, m, count, x, z);
+        if (m < 64) return launch_solve_as<TF, true>(c, pool, perm, stride, m, count, x, z, shape);
+    launch_solve_as<TF, false>(c, pool, perm, stride, m, count, x, z, shape);
 }
 
 template <typename TF>
@@ -476,13 +546,12 @@ void launch_solve_t(dgh_ctx *c, const TF *pool, const int *perm, size_t stride, 
 }
 
 // The DG cell blocks from their FP16 slabs (one warp per block, like launch_solve).
-void launch_solve_half(dgh_ctx *c, const double *x, double *z) {
+void launch_solve_half(dgh_ctx *c, const double *x, double *z, int shape) {
     constexpr int wpc = SOLVE_THREADS / 32;
     const size_t smem = sizeof(float) * (size_t)pad8(c->m) * wpc;
-    const int want = (c->cells + wpc - 1) / wpc;
     int resident = 0;
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_lu_solve_half, SOLVE_THREADS, smem), "occupancy");
-    const int grid = std::min(want, c->sms * std::max(1, resident));
+    const int grid = solve_grid(c, c->cells, wpc, resident, shape);
     k_lu_solve_half<<<grid, SOLVE_THREADS, smem, c->stream>>>((const __half *)c->dg_pool, c->dg_scale, c->dg_perm, c->m,
                                                                c->cells, x, z);
     c->launched();
@@ -719,6 +788,13 @@ template <typename TF> void ilu2_apply(dgh_ctx *c, const double *x, double *z) {
     c->launched(launches);
 }
 
+// The DG cell blocks' block-Jacobi solve z = M^{-1} x with grid shape `shape` (solve_grid).
+void dg_block_solve(dgh_ctx *c, int shape, const double *x, double *z) {
+    const size_t stride = (size_t)c->m * c->m;
+    if (c->half16()) launch_solve_half(c, x, z, shape);
+    else if (c->mixed()) launch_solve<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z, shape);
+    else launch_solve<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z, shape);
+}
 void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     Timed tm(c, DGH_TIMER_PRECOND);
     if (c->d1()) {
@@ -759,10 +835,7 @@ void precond_apply(dgh_ctx *c, int op, const double *x, double *z) {
     }
     if (op == DGH_OP_DG) {
         need(c->dg_factored, "Refresh the block-Jacobi preconditioner before applying it");
-        const size_t stride = (size_t)c->m * c->m;
-        if (c->half16()) launch_solve_half(c, x, z);
-        else if (c->mixed()) launch_solve<float>(c, (const float *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
-        else launch_solve<double>(c, (const double *)c->dg_pool, c->dg_perm, stride, c->m, c->cells, x, z);
+        dg_block_solve(c, std::max(0, c->solve_shape), x, z);
     } else {
         need(c->face_factored, "Refresh the block-Jacobi preconditioner before applying it");
         const size_t stride = (size_t)c->fw * c->fw;
@@ -1026,7 +1099,9 @@ __global__ void k_gmres_setup(GmresDev *d, double rhs_norm, double tol, int limi
     d->count = 0;
 }
 
+bool lockstep_gmres(dgh_ctx *c, const double *rhs, double *x, int limit, double tol, int &iters, double &rel);
 void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
+    if (op == DGH_OP_DG && c->ls && lockstep_gmres(c, rhs, x, limit, tol, iters, rel)) return;
     GmresCall g;
     g.op = op;
     g.n = op == DGH_OP_HDG ? c->NT : c->N;
@@ -1092,6 +1167,299 @@ void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double t
         if (iters >= limit) fail(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
     }
     copy_out();
+}
+
+// ---- lockstep batch of DG GMRES solves ----------------------------------------------------------
+// The block solves z = M^{-1} src of every gated member, one launch per factor layout.
+void ls_solve_all(dgh_lockstep *L, int src, int dst, int j, int gate) {
+    for (const auto &r : L->layouts) {
+        if (r.key == 0)
+            k_ls_solve<double, false><<<r.blocks, SOLVE_THREADS, r.smem, L->stream>>>(L->table, r.first, r.count, src, dst,
+                                                                                     j, gate);
+        else if (r.key == 1)
+            k_ls_solve<float, false><<<r.blocks, SOLVE_THREADS, r.smem, L->stream>>>(L->table, r.first, r.count, src, dst,
+                                                                                    j, gate);
+        else if (r.key == 2)
+            k_ls_solve<float, true><<<r.blocks, SOLVE_THREADS, r.smem, L->stream>>>(L->table, r.first, r.count, src, dst,
+                                                                                   j, gate);
+        else
+            k_ls_solve_half<<<r.blocks, SOLVE_THREADS, r.smem, L->stream>>>(L->table, r.first, r.count, src, dst, j, gate);
+        L->launched();
+    }
+}
+// dst = J src for every gated member: the face traces of src, then J·v, one pair of launches per degree.
+void ls_jv_all(dgh_lockstep *L, int src, int dst, int gate) {
+    for (const auto &r : L->degrees) {
+        DGH_DISPATCH_N(r.key, {
+            k_ls_face_trace<N><<<r.blocks, Team<N>::THREADS, 0, L->stream>>>(L->table, r.first, r.count, src, gate);
+            k_ls_dg_apply<N><<<r.blocks, Team<N>::THREADS, 0, L->stream>>>(L->table, r.first, r.count, src, dst, gate);
+        });
+        L->launched(2);
+    }
+}
+// The three segments of a lockstep restart cycle (gmres()'s start, Arnoldi step j, finish) on
+// stream `st`; each returns the launches it issued.
+int ls_seg_start(dgh_lockstep *L, cudaStream_t st) {
+    const int cnt = (int)L->members.size();
+    k_ls_wnorm2<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt);
+    k_ls_reduce<<<cnt, KR_THREADS, 0, st>>>(L->table, cnt, 1, 2, 0);
+    k_ls_scale_div<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, LS_R, LS_VJ, 0, 0);
+    k_ls_gmres_init<<<cnt, 32, 0, st>>>(L->table);
+    L->launched(4);
+    return 4;
+}
+int ls_seg_step(dgh_lockstep *L, cudaStream_t st, int j) {
+    const int cnt = (int)L->members.size();
+    const int64_t before = L->launches;
+    cudaStream_t keep = L->stream;
+    L->stream = st;
+    ls_solve_all(L, LS_VJ, LS_Z, j, 1);
+    ls_jv_all(L, LS_Z, LS_W, 1);
+    L->stream = keep;
+    const int K = j + 1;
+#define C_(NV) k_ls_mdot<NV><<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, K)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    k_ls_reduce<<<cnt * K, KR_THREADS, 0, st>>>(L->table, cnt, K, 0, 1);
+#define C_(NV) k_ls_maxpy<NV, 0><<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, K)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    k_ls_reduce<<<cnt * K, KR_THREADS, 0, st>>>(L->table, cnt, K, 1, 1);
+#define C_(NV) k_ls_maxpy<NV, 1><<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, K)
+    DGH_DISPATCH_K(K, C_);
+#undef C_
+    k_ls_reduce<<<cnt, KR_THREADS, 0, st>>>(L->table, cnt, 1, 2, 1);
+    k_ls_scale_div<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, LS_W, LS_VJ1, j, 1);
+    k_ls_gmres_update<<<cnt, 32, 0, st>>>(L->table, j);
+    L->launched(8);
+    return (int)(L->launches - before);
+}
+int ls_seg_finish(dgh_lockstep *L, cudaStream_t st) {
+    const int cnt = (int)L->members.size();
+    const int64_t before = L->launches;
+    cudaStream_t keep = L->stream;
+    L->stream = st;
+    k_ls_gmres_backsolve<<<cnt, 32, 0, st>>>(L->table);
+    k_ls_lincomb<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt);
+    L->launched(2);
+    ls_solve_all(L, LS_W, LS_Z, 0, 0);
+    k_ls_axpby<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, 1., LS_X, 1., LS_Z, LS_X);
+    L->launched();
+    ls_jv_all(L, LS_X, LS_W, 0);
+    k_ls_axpby<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt, 1., LS_RHS, -1., LS_W, LS_R);
+    k_ls_wnorm2<<<L->red_total, KR_THREADS, 0, st>>>(L->table, cnt);
+    k_ls_reduce<<<cnt, KR_THREADS, 0, st>>>(L->table, cnt, 1, 3, 0);
+    k_ls_tails<<<(cnt + 127) / 128, 128, 0, st>>>(L->table, cnt, L->tails);
+    L->launched(4);
+    L->stream = keep;
+    return (int)(L->launches - before);
+}
+// Captures one lockstep restart cycle as a CUDA graph: the start segment, one IF node per
+// Arnoldi step whose handle the preceding k_ls_cont_cond sets (any member continues), the finish
+// segment; the step bodies are captured on the auxiliary stream (as build_cycle_graph does for
+// one context).
+void ls_build_graph(dgh_lockstep *L) {
+    const int cnt = (int)L->members.size();
+    if (!L->aux) ck(cudaStreamCreateWithFlags(&L->aux, cudaStreamNonBlocking), "cudaStreamCreate");
+    const int64_t launches0 = L->launches;
+    cudaGraph_t cap = nullptr;
+    ck(cudaGraphCreate(&cap, 0), "cudaGraphCreate");
+    std::vector<cudaGraphConditionalHandle> h(L->restart);
+    for (auto &hj : h)
+        ck(cudaGraphConditionalHandleCreate(&hj, cap, 0, cudaGraphCondAssignDefault), "cudaGraphConditionalHandleCreate");
+    ck(cudaStreamBeginCaptureToGraph(L->stream, cap, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+       "cudaStreamBeginCaptureToGraph");
+    int fixed = ls_seg_start(L, L->stream), per_step = 0;
+    k_ls_cont_cond<<<1, 1024, 0, L->stream>>>(L->table, cnt, h[0]);
+    L->launched();
+    ++fixed;
+    cudaStreamCaptureStatus stc;
+    for (int j = 0; j < L->restart; ++j) {
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        ck(cudaStreamGetCaptureInfo(L->stream, &stc, nullptr, nullptr, &deps, &nd), "cudaStreamGetCaptureInfo");
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h[j];
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        ck(cudaGraphAddNode(&node, cap, deps, nd, &cp), "cudaGraphAddNode");
+        ck(cudaStreamUpdateCaptureDependencies(L->stream, &node, 1, cudaStreamSetCaptureDependencies),
+           "cudaStreamUpdateCaptureDependencies");
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ck(cudaStreamBeginCaptureToGraph(L->aux, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+           "cudaStreamBeginCaptureToGraph");
+        per_step = ls_seg_step(L, L->aux, j);
+        if (j + 1 < L->restart) {
+            k_ls_cont_cond<<<1, 1024, 0, L->aux>>>(L->table, cnt, h[j + 1]);
+            L->launched();
+            ++per_step;
+        }
+        ck(cudaStreamEndCapture(L->aux, &body), "cudaStreamEndCapture (body)");
+    }
+    fixed += ls_seg_finish(L, L->stream);
+    ck(cudaStreamEndCapture(L->stream, &cap), "cudaStreamEndCapture");
+    ck(cudaGraphInstantiate(&L->cycle, cap, 0), "cudaGraphInstantiate");
+    ck(cudaGraphDestroy(cap), "cudaGraphDestroy");
+    L->launches = launches0;  // counted when replayed
+    L->graph_fixed = fixed;
+    L->graph_step = per_step;
+}
+// One session's lockstep solve: gmres() of every live member, restart cycle by restart cycle
+// and Arnoldi step by Arnoldi step, each phase one launch over the members.  Stepped, the host
+// reads one continue flag per member after each step; replayed (when every member replays its
+// own cycles as graphs), each cycle is one graph launch whose steps are conditional on any
+// member continuing.  After each cycle the host reads one tail record per member and applies
+// gmres()'s stopping and failure rules per member.
+void ls_run(dgh_lockstep *L) {
+    const int cnt = (int)L->members.size();
+    cudaStream_t gs = L->stream;
+    bool any = false, graph = true;
+    for (int i = 0; i < cnt; ++i) {
+        auto &sl = L->slots[i];
+        const bool live = sl.arrived && !sl.trivial && sl.code == DGH_OK;
+        L->host[i].live = live ? 1 : 0;
+        L->host[i].inv_step = L->members[i]->inv_step;
+        if (live) ck(cudaStreamWaitEvent(gs, sl.ready, 0), "cudaStreamWaitEvent");
+        any = any || live;
+        graph = graph && L->members[i]->use_graph;
+    }
+    if (!any) return;
+    ++L->sessions;
+    if (graph && !L->cycle) ls_build_graph(L);
+    const size_t tb = sizeof(LsMember) * (size_t)cnt;
+    for (;;) {
+        ck(cudaMemcpyAsync(L->table, L->host, tb, cudaMemcpyHostToDevice, gs), "copy member table");
+        ++L->cycles;
+        if (graph) {
+            ck(cudaGraphLaunch(L->cycle, gs), "cudaGraphLaunch");
+        } else {
+            ls_seg_start(L, gs);
+            for (int j = 0; j < L->restart; ++j) {
+                k_ls_cont<<<(cnt + 127) / 128, 128, 0, gs>>>(L->table, cnt, L->flags);
+                L->launched();
+                ck(cudaMemcpyAsync(L->flags_host, L->flags, sizeof(int) * cnt, cudaMemcpyDeviceToHost, gs), "copy flags");
+                ck(cudaStreamSynchronize(gs), "cudaStreamSynchronize");
+                bool cont = false;
+                for (int i = 0; i < cnt; ++i) cont = cont || L->flags_host[i];
+                if (!cont) break;
+                ++L->steps;
+                ls_seg_step(L, gs, j);
+            }
+            ls_seg_finish(L, gs);
+        }
+        ck(cudaMemcpyAsync(L->tails_host, L->tails, sizeof(LsTail) * cnt, cudaMemcpyDeviceToHost, gs), "copy tails");
+        ck(cudaStreamSynchronize(gs), "cudaStreamSynchronize");
+        if (graph) {  // the replayed steps: as many as the longest member's basis this cycle
+            int taken = 0;
+            for (int i = 0; i < cnt; ++i)
+                if (L->host[i].live) taken = std::max(taken, L->tails_host[i].count);
+            L->steps += taken;
+            L->launches += L->graph_fixed + (int64_t)taken * L->graph_step;
+        }
+        bool more = false;
+        for (int i = 0; i < cnt; ++i) {
+            if (!L->host[i].live) continue;
+            auto &sl = L->slots[i];
+            const LsTail &t = L->tails_host[i];
+            sl.iters = t.iters;
+            bool done = false;
+            auto failed = [&](int code, const char *msg) {
+                sl.code = code;
+                sl.msg = msg;
+                done = true;
+            };
+            if (t.status) failed(DGH_ERR_BREAKDOWN, "GMRES Arnoldi breakdown");
+            else if (t.count == 0) {
+                if (t.beta <= sl.tol * sl.rhs_norm) {
+                    sl.rel = t.beta / sl.rhs_norm;
+                    done = true;
+                } else failed(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+            } else {
+                sl.rel = std::sqrt(std::max(0.0, t.rnorm2)) / sl.rhs_norm;
+                if (!std::isfinite(sl.rel)) failed(DGH_ERR_NONFINITE, "Nonfinite GMRES residual");
+                else if (sl.rel <= sl.tol) done = true;
+                else if (sl.iters >= sl.limit) failed(DGH_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+            }
+            if (done) L->host[i].live = 0;
+            more = more || !done;
+        }
+        if (!more) break;
+    }
+}
+// Ends a session: the last arrival (or withdrawal) runs the lockstep solve, then wakes the others.
+void ls_complete(dgh_lockstep *L) {
+    try {
+        ls_run(L);
+    } catch (const Failure &e) {
+        for (auto &sl : L->slots)
+            if (sl.arrived && sl.code == DGH_OK) {
+                sl.code = e.code;
+                sl.msg = e.message;
+            }
+    } catch (const std::exception &e) {
+        for (auto &sl : L->slots)
+            if (sl.arrived && sl.code == DGH_OK) {
+                sl.code = DGH_ERR_CUDA;
+                sl.msg = e.what();
+            }
+    }
+    cudaEventRecord(L->finished, L->stream);
+    std::lock_guard<std::mutex> lk(L->mu);
+    L->open = false;
+    ++L->generation;
+    L->cv.notify_all();
+}
+void ls_arrive(dgh_lockstep *L, int idx) {
+    std::unique_lock<std::mutex> lk(L->mu);
+    const uint64_t gen = L->generation;
+    L->slots[idx].arrived = true;
+    ++L->arrived;
+    if (L->arrived + L->withdrawn == L->expected) {
+        lk.unlock();
+        ls_complete(L);
+        return;
+    }
+    L->cv.wait(lk, [&] { return L->generation != gen; });
+}
+// gmres() of op DG for a member of an open session: the solve's own copies and |rhs| on the
+// member's stream, then the rendezvous; false when the context has no open session to join.
+bool lockstep_gmres(dgh_ctx *c, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
+    dgh_lockstep *L = c->ls;
+    {
+        std::lock_guard<std::mutex> lk(L->mu);
+        if (!L->open) return false;
+        const auto &sl = L->slots[c->ls_index];
+        if (sl.arrived || sl.withdrawn) return false;  // one solve per member and session
+    }
+    auto &sl = L->slots[c->ls_index];
+    const long long n = c->N;
+    double *r = c->gres[DGH_OP_DG];
+    ck(cudaMemcpyAsync(c->g_rhs, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    ck(cudaMemsetAsync(c->g_x, 0, n * sizeof(double), c->stream), "memset");
+    ck(cudaMemcpyAsync(r, c->g_rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(c->g_rhs, c->inv_mass, false, n)));
+    sl.tol = tol;
+    sl.limit = limit;
+    sl.rhs_norm = rhs_norm;
+    sl.trivial = rhs_norm == 0;
+    sl.iters = 0;
+    sl.rel = 0;
+    sl.code = DGH_OK;
+    sl.msg.clear();
+    if (!sl.trivial) {
+        k_gmres_setup<<<1, 32, 0, c->stream>>>(c->gdev, rhs_norm, tol, limit, (int)std::min<long long>(n, c->cfg.restart));
+        c->launched();
+    }
+    ck(cudaEventRecord(sl.ready, c->stream), "cudaEventRecord");
+    ls_arrive(L, c->ls_index);
+    if (sl.code != DGH_OK) fail(sl.code, sl.msg);
+    ck(cudaStreamWaitEvent(c->stream, L->finished, 0), "cudaStreamWaitEvent");
+    iters = sl.iters;
+    rel = sl.rel;
+    ck(cudaMemcpyAsync(x, c->g_x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    return true;
 }
 
 void build_rule(dgh_ctx *c) {
@@ -1993,7 +2361,7 @@ int dgh_dg_block(dgh_ctx *c, int row, int col, double *host_block) {
 // ---- factorisation variants and the per-degree autotuner ------------------------------------------
 namespace {
 std::mutex g_tune_mutex;
-std::map<std::tuple<int, int, int>, int> g_tune_cache;  // (kind, n, precision) -> variant
+std::map<std::tuple<int, int, int, int>, int> g_tune_cache;  // (kind, n, precision, cells of kind 3) -> variant
 
 // DG blocks of cells [first, first + count): assembly and LU with the given variant.
 void dg_factor(dgh_ctx *c, int variant, int first, int count) {
@@ -2202,10 +2570,12 @@ template <class F> int tune_pick(dgh_ctx *c, F &&f, double *ms_out) {
     ms_out[1] = best[1];
     return best[1] < best[0] ? 1 : 0;
 }
-// The cached or newly tuned variant of one kind (0 DG blocks, 1 condensation).
+// The cached or newly tuned variant of one kind (0 DG blocks, 1 FP64 condensation, 2 FP32-storage
+// condensation, 3 the DG block solve's grid shape, which also depends on the block count, 4 the
+// fused DG factorisation's CTAs per SM, variant v = v + 1 CTAs).
 template <class F> int tuned_variant(dgh_ctx *c, int kind, F &&time_both, double *ms_out) {
     if (!c->cfg.autotune) return 0;
-    const auto key = std::make_tuple(kind, c->n, c->cfg.precision);
+    const auto key = std::make_tuple(kind, c->n, c->cfg.precision, kind == 3 ? c->cells : 0);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -2296,9 +2666,27 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
                 c->dg_variant = tuned_variant(c, 0, [&](int v) { dg_factor(c, v, 0, sample); }, c->tune_ms);
                 c->check_status();
             }
+            if (c->fused_ctas < 0) {  // the fused path's residency (kind 4): 1 or 2 CTAs per SM
+                const bool fused = c->mixed() && (c->half16() || c->dg_variant == 0) && !c->overint();
+                if (fused) {
+                    const int sample = std::min(c->cells, std::max(c->lu_grid, 1) * 4);
+                    const int v = tuned_variant(c, 4, [&](int k) {
+                        c->fused_ctas = k + 1;
+                        dg_factor(c, c->dg_variant, 0, sample);
+                    }, c->fused_ms);
+                    c->fused_ctas = c->cfg.autotune ? v + 1 : 2;
+                    c->check_status();
+                } else {
+                    c->fused_ctas = 2;
+                }
+            }
             dg_factor(c, c->dg_variant, 0, c->cells);
             c->check_status();
             c->dg_factored = true;
+            if (c->solve_shape < 0) {  // timed on a zero right-hand side (the same loads and flops)
+                ck(cudaMemsetAsync(c->gw, 0, (size_t)c->N * sizeof(double), c->stream), "cudaMemsetAsync");
+                c->solve_shape = tuned_variant(c, 3, [&](int v) { dg_block_solve(c, v, c->gw, c->gz); }, c->solve_ms);
+            }
         } else {
             need(c->face_pool, "context has no HDG operator");
             need(c->condensed, "Condense the HDG operator before refreshing its preconditioner");
@@ -2500,6 +2888,23 @@ int dgh_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, doubl
         if (relative) *relative = rel;
     });
 }
+int dgh_shape_set(dgh_ctx *c, int which, int value) {
+    if (!c) return DGH_ERR_INVALID;
+    if (which == DGH_SHAPE_SOLVE_GRID && (value == 0 || value == 1)) c->solve_shape = value;
+    else if (which == DGH_SHAPE_FUSED_CTAS && (value == 1 || value == 2)) c->fused_ctas = value;
+    else return DGH_ERR_INVALID;
+    return DGH_OK;
+}
+int dgh_autotune_shapes(const dgh_ctx *c, double out[6]) {
+    if (!c || !out) return DGH_ERR_INVALID;
+    out[0] = c->solve_shape;
+    out[1] = c->solve_ms[0];
+    out[2] = c->solve_ms[1];
+    out[3] = c->fused_ctas;
+    out[4] = c->fused_ms[0];
+    out[5] = c->fused_ms[1];
+    return DGH_OK;
+}
 int dgh_autotune_report(const dgh_ctx *c, double out[6]) {
     if (!c || !out) return DGH_ERR_INVALID;
     out[0] = c->dg_variant;
@@ -2671,6 +3076,214 @@ int dgh_block_jacobi_perm(const dgh_block_jacobi *bj, int *host_perm) {
         ck(cudaMemcpy(host_perm, bj->perm, sizeof(int) * (size_t)bj->m * bj->count, cudaMemcpyDeviceToHost),
            "copy perm");
     });
+}
+
+}  // extern "C"
+
+// ---- lockstep batch of DG GMRES solves (no counterpart in the reference) ------------------------
+namespace {
+thread_local std::string g_ls_error;
+void ls_free(dgh_lockstep *L) {
+    if (L->stream) cudaStreamSynchronize(L->stream);
+    for (dgh_ctx *c : L->members) {
+        c->ls = nullptr;
+        c->ls_index = -1;
+    }
+    for (auto &sl : L->slots)
+        if (sl.ready) cudaEventDestroy(sl.ready);
+    if (L->finished) cudaEventDestroy(L->finished);
+    if (L->table) cudaFree(L->table);
+    if (L->flags) cudaFree(L->flags);
+    if (L->tails) cudaFree(L->tails);
+    if (L->host) cudaFreeHost(L->host);
+    if (L->flags_host) cudaFreeHost(L->flags_host);
+    if (L->tails_host) cudaFreeHost(L->tails_host);
+    if (L->cycle) cudaGraphExecDestroy(L->cycle);
+    if (L->aux) cudaStreamDestroy(L->aux);
+    if (L->stream) cudaStreamDestroy(L->stream);
+    delete L;
+}
+}  // namespace
+
+extern "C" {
+
+const char *dgh_lockstep_error(void) { return g_ls_error.c_str(); }
+
+int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) {
+    if (!members || count <= 0 || !out) return DGH_ERR_INVALID;
+    *out = nullptr;
+    auto reject = [&](int i, const char *m) {
+        g_ls_error = "lockstep member " + std::to_string(i) + ": " + m;
+        return DGH_ERR_INVALID;
+    };
+    for (int i = 0; i < count; ++i) {
+        const dgh_ctx *c = members[i];
+        if (!c) return reject(i, "null context");
+        if (c->d1()) return reject(i, "lockstep members are 2D contexts");
+        if (!c->has_dg()) return reject(i, "the context has no DG operator");
+        if (c->overint()) return reject(i, "lockstep members use the collocated volume rule");
+        if (c->ilu()) return reject(i, "lockstep members use block Jacobi");
+        if (c->ls) return reject(i, "the context is already in a lockstep group");
+        for (int k = 0; k < i; ++k)
+            if (members[k] == c) return reject(i, "the context is listed twice");
+        const dgh_ctx *c0 = members[0];
+        if (c->cfg.device != c0->cfg.device) return reject(i, "lockstep members share one device");
+        if (c->cfg.precision != c0->cfg.precision) return reject(i, "lockstep members share one precision");
+        if (std::min<long long>(c->N, c->cfg.restart) != std::min<long long>(c0->N, c0->cfg.restart))
+            return reject(i, "lockstep members share one GMRES restart length");
+    }
+    auto *L = new dgh_lockstep;
+    const int rc = [&]() -> int {
+        try {
+            const dgh_ctx *c0 = members[0];
+            L->device = c0->cfg.device;
+            L->precision = c0->cfg.precision;
+            L->restart = (int)std::min<long long>(c0->N, c0->cfg.restart);
+            ck(cudaSetDevice(L->device), "cudaSetDevice");
+            std::vector<int> order(count);
+            for (int i = 0; i < count; ++i) order[i] = i;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return members[a]->n < members[b]->n; });
+            for (int i : order) L->members.push_back(members[i]);
+            ck(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaEventCreateWithFlags(&L->finished, cudaEventDisableTiming), "cudaEventCreate");
+            L->slots.resize(count);
+            for (auto &sl : L->slots) ck(cudaEventCreateWithFlags(&sl.ready, cudaEventDisableTiming), "cudaEventCreate");
+            ck(cudaMalloc(&L->table, sizeof(LsMember) * count), "cudaMalloc");
+            ck(cudaMalloc(&L->flags, sizeof(int) * count), "cudaMalloc");
+            ck(cudaMalloc(&L->tails, sizeof(LsTail) * count), "cudaMalloc");
+            ck(cudaMallocHost(&L->host, sizeof(LsMember) * count), "cudaMallocHost");
+            ck(cudaMallocHost(&L->flags_host, sizeof(int) * count), "cudaMallocHost");
+            ck(cudaMallocHost(&L->tails_host, sizeof(LsTail) * count), "cudaMallocHost");
+            constexpr int wpc = SOLVE_THREADS / 32;
+            auto layout_of = [&](const dgh_ctx *c) { return c->half16() ? 3 : !c->mixed() ? 0 : c->m < 64 ? 2 : 1; };
+            for (int i = 0; i < count; ++i) {
+                dgh_ctx *c = L->members[i];
+                LsMember &t = L->host[i];
+                std::memset(&t, 0, sizeof(t));
+                t.gdev = c->gdev;
+                t.V = c->V;
+                t.w = c->gw;
+                t.z = c->gz;
+                t.red = c->red;
+                t.partial = c->partial;
+                t.coef = c->gcoef;
+                t.x = c->g_x;
+                t.rhs = c->g_rhs;
+                t.r = c->gres[DGH_OP_DG];
+                t.W = c->inv_mass;
+                t.ld = (size_t)c->vld;
+                t.n = c->N;
+                t.red_blocks = c->red_grid;
+                t.red0 = L->red_total;
+                L->red_total += c->red_grid;
+                t.pool = c->dg_pool;
+                t.scale = c->dg_scale;
+                t.perm = c->dg_perm;
+                t.stride = (size_t)c->m * c->m;
+                t.m = c->m;
+                t.cells = c->cells;
+                t.traces = c->traces2;
+                t.vol = c->vol;
+                t.fcache = c->fcache;
+                t.speeds = c->speeds;
+                t.basis = c->basis_dev;
+                t.g = c->g;
+                t.inv_step = c->inv_step;
+                // ranges: one per degree (J·v) and one per factor layout (block solve)
+                if (L->degrees.empty() || L->degrees.back().key != c->n) {
+                    dgh_lockstep::Range r;
+                    r.first = i;
+                    r.key = c->n;
+                    L->degrees.push_back(r);
+                }
+                auto &dr = L->degrees.back();
+                int cpb = 1;
+                DGH_DISPATCH_N(c->n, { cpb = Team<N>::CPB; });
+                t.team0 = dr.blocks;
+                dr.blocks += c->team_blocks(cpb);
+                ++dr.count;
+                const int key = layout_of(c);
+                if (L->layouts.empty() || L->layouts.back().key != key) {
+                    dgh_lockstep::Range r;
+                    r.first = i;
+                    r.key = key;
+                    L->layouts.push_back(r);
+                }
+                auto &lr = L->layouts.back();
+                t.solve0 = lr.blocks;
+                lr.blocks += (c->cells + wpc - 1) / wpc;
+                ++lr.count;
+                const size_t row = key == 3 ? sizeof(float) * pad8(c->m) : (key == 0 ? sizeof(double) : sizeof(float)) * c->m;
+                lr.smem = std::max(lr.smem, row * wpc);
+            }
+            for (const auto &r : L->layouts)
+                for (const auto &q : L->layouts)
+                    if (&r != &q && r.key == q.key) fail(DGH_ERR_INVALID, "lockstep factor layouts are not contiguous");
+            for (int i = 0; i < count; ++i) {
+                L->members[i]->ls = L;
+                L->members[i]->ls_index = i;
+            }
+            return DGH_OK;
+        } catch (const Failure &e) {
+            g_ls_error = e.message;
+            return e.code;
+        } catch (const std::exception &e) {
+            g_ls_error = e.what();
+            return DGH_ERR_CUDA;
+        }
+    }();
+    if (rc != DGH_OK) {
+        for (dgh_ctx *c : L->members) c->ls = nullptr;
+        L->members.clear();
+        ls_free(L);
+        return rc;
+    }
+    *out = L;
+    return DGH_OK;
+}
+
+int dgh_lockstep_destroy(dgh_lockstep *L) {
+    if (!L) return DGH_ERR_INVALID;
+    ls_free(L);
+    return DGH_OK;
+}
+
+int dgh_lockstep_begin(dgh_lockstep *L, int expected) {
+    if (!L || expected < 0 || expected > (int)L->members.size()) return DGH_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(L->mu);
+    if (L->open) return DGH_ERR_STATE;
+    for (auto &sl : L->slots) {
+        sl.arrived = sl.withdrawn = sl.trivial = false;
+        sl.code = DGH_OK;
+        sl.msg.clear();
+    }
+    L->arrived = L->withdrawn = 0;
+    L->expected = expected;
+    L->open = expected > 0;
+    return DGH_OK;
+}
+
+int dgh_lockstep_leave(dgh_lockstep *L, dgh_ctx *c) {
+    if (!L || !c || c->ls != L) return DGH_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(L->mu);
+    auto &sl = L->slots[c->ls_index];
+    if (!L->open || sl.arrived || sl.withdrawn) return DGH_OK;
+    sl.withdrawn = true;
+    ++L->withdrawn;
+    if (L->arrived + L->withdrawn == L->expected) {
+        lk.unlock();
+        ls_complete(L);
+    }
+    return DGH_OK;
+}
+
+int dgh_lockstep_report(const dgh_lockstep *L, int64_t out[4]) {
+    if (!L || !out) return DGH_ERR_INVALID;
+    out[0] = L->sessions;
+    out[1] = L->cycles;
+    out[2] = L->steps;
+    out[3] = L->launches;
+    return DGH_OK;
 }
 
 }  // extern "C"

@@ -17,13 +17,15 @@ template <int N> struct Team {
 // traces[(cell*4 + side)*N*4 + q*4 + v] = sum_i e_side[i] u[v][face_node(side,q,i)]
 // Optionally checks admissibility (discretization.cpp:211-233): every nodal value finite, and
 // density and pressure above 1e-13 at the nodes and the four face restrictions.
+// (The kernel bodies below take their block index bx explicitly, so the batched kernels of a
+// lockstep batch run the same arithmetic per member.)
 template <int N, bool CHECK>
-__global__ void __launch_bounds__(Team<N>::THREADS)
-k_face_trace(const double *__restrict__ u, double *__restrict__ traces, Basis1D b, Grid g, int *ok) {
+__device__ __forceinline__ void face_trace_body(int bx, const double *__restrict__ u, double *__restrict__ traces,
+                                                const Basis1D &b, const Grid &g, int *ok) {
     using T = Team<N>;
     __shared__ double su[T::CPB][NVAR * T::P];
     const int sub = threadIdx.x / T::TPC, lt = threadIdx.x % T::TPC;
-    const int cell = blockIdx.x * T::CPB + sub;
+    const int cell = bx * T::CPB + sub;
     const bool active = cell < g.cells;
     const double *uc = u + (size_t)cell * NVAR * T::P;
     if (active)
@@ -46,7 +48,7 @@ k_face_trace(const double *__restrict__ u, double *__restrict__ traces, Basis1D 
         for (int v = 0; v < NVAR; ++v) {
             double acc = 0;
 #pragma unroll
-            for (int i = 0; i < N; ++i) acc += e[i] * su[sub][v * T::P + face_node(N, side, q, i)];
+            for (int i = 0; i < N; ++i) acc = rfma(e[i], su[sub][v * T::P + face_node(N, side, q, i)], acc);
             s[v] = acc;
             tc[k * NVAR + v] = acc;
         }
@@ -56,6 +58,11 @@ k_face_trace(const double *__restrict__ u, double *__restrict__ traces, Basis1D 
         }
     }
     if (CHECK && !good) atomicExch(ok, 0);
+}
+template <int N, bool CHECK>
+__global__ void __launch_bounds__(Team<N>::THREADS)
+k_face_trace(const double *__restrict__ u, double *__restrict__ traces, Basis1D b, Grid g, int *ok) {
+    face_trace_body<N, CHECK>(blockIdx.x, u, traces, b, g, ok);
 }
 
 // ---- frozen HLL speeds (discretization.cpp:163-177) -----------------------------------------
@@ -229,13 +236,38 @@ __global__ void k_face_cache(const double *__restrict__ traces, const double *__
     c[7] = w * a / (a + bb);
 }
 
+// normal_action (dgh_common.cuh) with every product and sum explicitly rounded, for the J·v
+// body shared by the single-problem and the lockstep kernels (same bits in both).
+__device__ __forceinline__ void normal_action_rn(double gamma, double u, double v, double H, const double d[4], int axis,
+                                                 double out[4]) {
+    const double dr = d[0], dx = d[1], dy = d[2], de = d[3];
+    const double q2 = rfma(u, u, rmul(v, v));
+    double t = rfma(-u, dx, de);
+    t = rfma(-v, dy, t);
+    t = rfma(rmul(.5, q2), dr, t);
+    const double dp = rmul(rsub(gamma, 1.), t);
+    const double uv = rmul(u, v);
+    if (axis == 0) {
+        out[0] = dx;
+        out[1] = rfma(rmul(2., u), dx, rfma(-rmul(u, u), dr, dp));
+        out[2] = rfma(u, dy, rfma(v, dx, -rmul(uv, dr)));
+        out[3] = rfma(H, rfma(-u, dr, dx), rmul(u, radd(de, dp)));
+    } else {
+        out[0] = dy;
+        out[1] = rfma(u, dy, rfma(v, dx, -rmul(uv, dr)));
+        out[2] = rfma(rmul(2., v), dy, rfma(-rmul(v, v), dr, dp));
+        out[3] = rfma(H, rfma(-v, dr, dy), rmul(v, radd(de, dp)));
+    }
+}
+
 // ---- matrix-free J·v (volume_jacobian.cpp:59-71 + dg_operator.cpp:10-21) ---------------------
 // Needs the face traces of the direction d (k_face_trace on d).
 template <int N>
-__global__ void __launch_bounds__(Team<N>::THREADS, 65536 / (Team<N>::THREADS * 72))
-k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const double *__restrict__ vol,
-           const double *__restrict__ fcache, const double *__restrict__ speeds, double *__restrict__ out,
-           const Basis1D *__restrict__ bp, Grid g, double inv_step, int volterm = 1) {
+__device__ __forceinline__ void dg_apply_body(int bx, const double *__restrict__ d, const double *__restrict__ dtr,
+                                              const double *__restrict__ vol, const double *__restrict__ fcache,
+                                              const double *__restrict__ speeds, double *__restrict__ out,
+                                              const Basis1D *__restrict__ bp, const Grid &g, double inv_step,
+                                              int volterm) {
     // the basis tables are indexed per thread: read them through L1 from a device copy rather
     // than from the kernel's parameter bank, where lane-varying indices serialise
     const Basis1D &b = *bp;
@@ -243,7 +275,7 @@ k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const d
     __shared__ double fx[T::CPB][NVAR * T::P], fy[T::CPB][NVAR * T::P];
     __shared__ double ff[T::CPB][NFACES * N * NVAR];
     const int sub = threadIdx.x / T::TPC, lt = threadIdx.x % T::TPC;
-    const int cell = blockIdx.x * T::CPB + sub;
+    const int cell = bx * T::CPB + sub;
     const bool active = cell < g.cells;
     const size_t base = (size_t)cell * NVAR * T::P;
     double dd[4] = {0, 0, 0, 0};
@@ -252,8 +284,8 @@ k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const d
         for (int v = 0; v < NVAR; ++v) dd[v] = d[base + v * T::P + lt];
         const double *c = vol + ((size_t)cell * T::P + lt) * 3;
         double a[4], e[4];
-        normal_action(g.gamma, c[0], c[1], c[2], dd, 0, a);
-        normal_action(g.gamma, c[0], c[1], c[2], dd, 1, e);
+        normal_action_rn(g.gamma, c[0], c[1], c[2], dd, 0, a);
+        normal_action_rn(g.gamma, c[0], c[1], c[2], dd, 1, e);
 #pragma unroll
         for (int v = 0; v < NVAR; ++v) {
             fx[sub][v * T::P + lt] = a[v];
@@ -274,34 +306,43 @@ k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const d
             }
             const double *c = fcache + ((size_t)face * N + q) * 8;
             double al[4], ar[4];
-            normal_action(g.gamma, c[0], c[1], c[2], L, axis, al);
-            normal_action(g.gamma, c[3], c[4], c[5], R, axis, ar);
+            normal_action_rn(g.gamma, c[0], c[1], c[2], L, axis, al);
+            normal_action_rn(g.gamma, c[3], c[4], c[5], R, axis, ar);
             const double sa = speeds[2 * (face * N + q)], sb = speeds[2 * (face * N + q) + 1];
-            const double pen = face_weight(g, b, face, q) * sa * sb / (sa + sb);
+            const double pen = rmul(rmul(face_weight(g, b, face, q), sa), sb) / radd(sa, sb);
             const double sign = side % 2 ? 1. : -1.;
 #pragma unroll
             for (int v = 0; v < NVAR; ++v)
-                ff[sub][k * NVAR + v] = sign * (c[6] * al[v] + c[7] * ar[v] + pen * (L[v] - R[v]));
+                ff[sub][k * NVAR + v] = rmul(sign, rfma(c[6], al[v], rfma(c[7], ar[v], rmul(pen, rsub(L[v], R[v])))));
         }
     __syncthreads();
     if (!active || lt >= T::P) return;
     const int ix = lt % N, iy = lt / N;
-    const double mass = .25 * g.hx * g.hy * b.w[ix] * b.w[iy];
-    const double sx = .5 * g.hy, sy = .5 * g.hx;
+    const double mass = rmul(rmul(rmul(rmul(.25, g.hx), g.hy), b.w[ix]), b.w[iy]);
+    const double sxw = rmul(rmul(.5, g.hy), b.w[iy]), syw = rmul(rmul(.5, g.hx), b.w[ix]);
 #pragma unroll
     for (int v = 0; v < NVAR; ++v) {
         double wx = 0, wy = 0;
 #pragma unroll
         for (int q = 0; q < N; ++q) {
-            wx += b.dw[q * N + ix] * fx[sub][v * T::P + q + N * iy];
-            wy += fy[sub][v * T::P + ix + N * q] * b.dw[q * N + iy];
+            wx = rfma(b.dw[q * N + ix], fx[sub][v * T::P + q + N * iy], wx);
+            wy = rfma(fy[sub][v * T::P + ix + N * q], b.dw[q * N + iy], wy);
         }
-        double val = mass * dd[v] * inv_step;
-        if (N > 1 && volterm) val -= sx * b.w[iy] * wx + sy * b.w[ix] * wy;
-        val += b.eL[ix] * ff[sub][(0 * N + iy) * NVAR + v] + b.eR[ix] * ff[sub][(1 * N + iy) * NVAR + v] +
-               b.eL[iy] * ff[sub][(2 * N + ix) * NVAR + v] + b.eR[iy] * ff[sub][(3 * N + ix) * NVAR + v];
-        out[base + v * T::P + lt] = val;
+        double val = rmul(rmul(mass, dd[v]), inv_step);
+        if (N > 1 && volterm) val = rsub(val, rfma(sxw, wx, rmul(syw, wy)));
+        const double lift = rfma(b.eL[ix], ff[sub][(0 * N + iy) * NVAR + v],
+                                 rfma(b.eR[ix], ff[sub][(1 * N + iy) * NVAR + v],
+                                      rfma(b.eL[iy], ff[sub][(2 * N + ix) * NVAR + v],
+                                           rmul(b.eR[iy], ff[sub][(3 * N + ix) * NVAR + v]))));
+        out[base + v * T::P + lt] = radd(val, lift);
     }
+}
+template <int N>
+__global__ void __launch_bounds__(Team<N>::THREADS, 65536 / (Team<N>::THREADS * 72))
+k_dg_apply(const double *__restrict__ d, const double *__restrict__ dtr, const double *__restrict__ vol,
+           const double *__restrict__ fcache, const double *__restrict__ speeds, double *__restrict__ out,
+           const Basis1D *__restrict__ bp, Grid g, double inv_step, int volterm = 1) {
+    dg_apply_body<N>(blockIdx.x, d, dtr, vol, fcache, speeds, out, bp, g, inv_step, volterm);
 }
 
 // ---- adjoint J^T w (the transpose of k_dg_apply, same frozen speeds and caches) -------------

@@ -617,10 +617,12 @@ k_inv_apply(const float *__restrict__ inv, int m, int count, const double *__res
 // FP32 form for narrow blocks (the HDG face blocks, m = 4n), whose time is mostly triangles.
 constexpr int SOLVE_THREADS = 256;
 template <typename T, bool DIAG> constexpr int solve_min_blocks() { return sizeof(T) == 4 && !DIAG ? 5 : 4; }
+// The body takes its block index bx and block count G explicitly (the batched solve of a
+// lockstep batch runs it over each member's blocks).
 template <typename T, bool DIAG>
-__global__ void __launch_bounds__(SOLVE_THREADS, (solve_min_blocks<T, DIAG>()))
-k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stride, int m, int count,
-           const double *__restrict__ rhs, double *__restrict__ z) {
+__device__ __forceinline__ void lu_solve_body(int bx, int G, const T *__restrict__ pool, const int *__restrict__ perm,
+                                              size_t stride, int m, int count, const double *__restrict__ rhs,
+                                              double *__restrict__ z) {
     using SV = SlabVec<T>;
     using V = typename SV::V;
     constexpr int W = SV::W, ND = 32 / W;
@@ -629,9 +631,9 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
     T *y = reinterpret_cast<T *>(smraw) + (size_t)wib * m;
     // m * sizeof(T) is a multiple of 16 (m = 4n^2 or 4n), so every warp's y is 16-byte aligned
     const V *yv = reinterpret_cast<const V *>(y);
-    const int warps = gridDim.x * (SOLVE_THREADS / 32);
+    const int warps = G * (SOLVE_THREADS / 32);
     const int slabs = (m + 31) / 32;
-    for (int blk = blockIdx.x * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
+    for (int blk = bx * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
         const T *A = pool + (size_t)blk * stride;
         const int *pm = perm + (size_t)blk * m;
         const double *b = rhs + (size_t)blk * m;
@@ -716,6 +718,12 @@ k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stri
         __syncwarp();
     }
 }
+template <typename T, bool DIAG>
+__global__ void __launch_bounds__(SOLVE_THREADS, (solve_min_blocks<T, DIAG>()))
+k_lu_solve(const T *__restrict__ pool, const int *__restrict__ perm, size_t stride, int m, int count,
+           const double *__restrict__ rhs, double *__restrict__ z) {
+    lu_solve_body<T, DIAG>(blockIdx.x, gridDim.x, pool, perm, stride, m, count, rhs, z);
+}
 
 // ---- 16-bit factor storage (the DG cell blocks, DGH_PRECISION_MIXED16) -------------------------
 // FP16 slabs with 8 columns per 16-byte group and rows padded to mp = m rounded up to 8 (zeros
@@ -757,14 +765,15 @@ __global__ void k_pack_half(const double *__restrict__ src, int m, int count, __
 // z = A^{-1} b per block from the FP16 slabs: k_lu_solve's structure (one warp per block, lane
 // i owns row 32 s + i, four 16-byte loads in flight, shuffled diagonal triangles) with FP32
 // arithmetic; the backward sweep multiplies each row's right-hand side by its row scale.
-__global__ void __launch_bounds__(SOLVE_THREADS, 5)
-k_lu_solve_half(const __half *__restrict__ pool, const float *__restrict__ row_scale, const int *__restrict__ perm,
-                int m, int count, const double *__restrict__ rhs, double *__restrict__ z) {
+__device__ __forceinline__ void lu_solve_half_body(int bx, int G, const __half *__restrict__ pool,
+                                                   const float *__restrict__ row_scale, const int *__restrict__ perm,
+                                                   int m, int count, const double *__restrict__ rhs,
+                                                   double *__restrict__ z) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int mp = pad8(m), lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     float *y = reinterpret_cast<float *>(smraw) + (size_t)wib * mp;
     const float4 *yv = reinterpret_cast<const float4 *>(y);
-    const int warps = gridDim.x * (SOLVE_THREADS / 32);
+    const int warps = G * (SOLVE_THREADS / 32);
     const int slabs = (m + 31) / 32;
     auto dot8 = [&](const uint4 &a, int g) {
         const __half2 *h = reinterpret_cast<const __half2 *>(&a);
@@ -774,7 +783,7 @@ k_lu_solve_half(const __half *__restrict__ pool, const float *__restrict__ row_s
         return (f0.x * y0.x + f0.y * y0.y) + (f1.x * y0.z + f1.y * y0.w) + (f2.x * y1.x + f2.y * y1.y) +
                (f3.x * y1.z + f3.y * y1.w);
     };
-    for (int blk = blockIdx.x * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
+    for (int blk = bx * (SOLVE_THREADS / 32) + wib; blk < count; blk += warps) {
         const __half *A = pool + (size_t)blk * m * mp;
         const int *pm = perm + (size_t)blk * m;
         const float *rs = row_scale + (size_t)blk * m;
@@ -843,6 +852,11 @@ k_lu_solve_half(const __half *__restrict__ pool, const float *__restrict__ row_s
         for (int i = lane; i < m; i += 32) z[(size_t)blk * m + i] = (double)y[i];
         __syncwarp();
     }
+}
+__global__ void __launch_bounds__(SOLVE_THREADS, 5)
+k_lu_solve_half(const __half *__restrict__ pool, const float *__restrict__ row_scale, const int *__restrict__ perm,
+                int m, int count, const double *__restrict__ rhs, double *__restrict__ z) {
+    lu_solve_half_body(blockIdx.x, gridDim.x, pool, row_scale, perm, m, count, rhs, z);
 }
 
 // Transposed block solve z = A^{-T} b with the same slab-layout factors (A = P^T L U, so

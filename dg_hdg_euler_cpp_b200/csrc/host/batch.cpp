@@ -33,6 +33,16 @@ struct dgh_batch {
     int pending = 0;
     bool quit = false;
     std::function<int(int)> job;
+    // lockstep groups of the DG members' GMRES solves (dgh_batch_lockstep): one per class of
+    // members that can share one (2D, collocated rule, block Jacobi, same precision and restart)
+    std::vector<dgh_lockstep *> groups;
+    std::vector<int> group_size, group_of;  // members per group; each member's group or -1
+    void drop_groups() {
+        for (auto *g : groups) dgh_lockstep_destroy(g);
+        groups.clear();
+        group_size.clear();
+        group_of.assign(count, -1);
+    }
 
     void worker(int i) {
         cudaSetDevice(cfg[i].device);
@@ -69,6 +79,7 @@ struct dgh_batch {
         return DGH_OK;
     }
     void release() {
+        drop_groups();
         {
             std::lock_guard<std::mutex> lk(mu);
             quit = true;
@@ -100,6 +111,7 @@ int dgh_batch_create(const dgh_config *members, int count, dgh_batch **out) {
     b->count = count;
     b->cfg.assign(members, members + count);
     b->status.assign(count, DGH_OK);
+    b->group_of.assign(count, -1);
     b->errors.assign(count, std::string());
     for (int i = 0; i < count; ++i)
         if (b->cfg[i].method != DGH_METHOD_DG && b->cfg[i].method != DGH_METHOD_HDG) {
@@ -186,12 +198,68 @@ int dgh_batch_stage_begin(dgh_batch *b, const double *const *host_states, double
     return rc;
 }
 
+int dgh_batch_lockstep(dgh_batch *b, int on) {
+    if (!b) return DGH_ERR_INVALID;
+    b->drop_groups();
+    if (!on) return DGH_OK;
+    // classes of DG members that can share a group; the others keep solving independently
+    std::vector<std::vector<int>> classes;
+    std::vector<const dgh_config *> key;
+    for (int i = 0; i < b->count; ++i) {
+        const dgh_config &c = b->cfg[i];
+        const bool collocated = c.quadrature == 0 || c.quadrature <= c.degree + 1;
+        if (c.method != DGH_METHOD_DG || c.dim == 1 || !collocated || c.preconditioner != 0) continue;
+        int cls = -1;
+        for (int q = 0; q < (int)key.size(); ++q)
+            if (key[q]->precision == c.precision && key[q]->restart == c.restart && key[q]->device == c.device) cls = q;
+        if (cls < 0) {
+            cls = (int)key.size();
+            key.push_back(&c);
+            classes.emplace_back();
+        }
+        classes[cls].push_back(i);
+    }
+    for (const auto &members : classes) {
+        std::vector<dgh_ctx *> ctxs;
+        for (int i : members) ctxs.push_back(b->ctx[i]);
+        dgh_lockstep *g = nullptr;
+        const int rc = dgh_lockstep_create(ctxs.data(), (int)ctxs.size(), &g);
+        if (rc != DGH_OK) {
+            g_batch_create_error = dgh_lockstep_error();
+            b->drop_groups();
+            return rc;
+        }
+        for (int i : members) b->group_of[i] = (int)b->groups.size();
+        b->groups.push_back(g);
+        b->group_size.push_back((int)members.size());
+    }
+    return DGH_OK;
+}
+
+int dgh_batch_lockstep_report(const dgh_batch *b, int64_t out[4]) {
+    if (!b || !out) return DGH_ERR_INVALID;
+    for (int i = 0; i < 4; ++i) out[i] = 0;
+    for (auto *g : b->groups) {
+        int64_t r[4];
+        const int rc = dgh_lockstep_report(g, r);
+        if (rc != DGH_OK) return rc;
+        for (int i = 0; i < 4; ++i) out[i] += r[i];
+    }
+    return DGH_OK;
+}
+
 int dgh_batch_newton_update(dgh_batch *b, dgh_update_stats *stats, int *status) {
     if (!b) return DGH_ERR_INVALID;
+    for (size_t g = 0; g < b->groups.size(); ++g) {
+        const int r = dgh_lockstep_begin(b->groups[g], b->group_size[g]);
+        if (r != DGH_OK) return r;
+    }
     const int rc = b->run([&](int i) {
         dgh_update_stats s{};
         const int r = dgh_newton_update(b->it[i], &s);
         if (r != DGH_OK) b->errors[i] = dgh_integrator_error(b->it[i]);
+        // a DG member whose update ended before its GMRES solve leaves the lockstep session
+        if (b->group_of[i] >= 0) dgh_lockstep_leave(b->groups[b->group_of[i]], b->ctx[i]);
         if (stats) stats[i] = s;
         return r;
     });

@@ -242,11 +242,24 @@ class Solver:
         return out
 
     def autotune_report(self) -> dict:
-        """Factorisation variants in use and the last tuning times (dgh_autotune_report)."""
+        """Factorisation variants and the DG block-solve grid shape in use, with the last tuning times
+        (dgh_autotune_report, dgh_autotune_shapes)."""
         out = (ctypes.c_double * 6)()
         self._rc(self.lib.dgh_autotune_report(self.h, out))
+        shape = (ctypes.c_double * 6)()
+        self._rc(self.lib.dgh_autotune_shapes(self.h, shape))
         return {"dg_variant": int(out[0]), "hdg_variant": int(out[1]),
-                "tune_ms": {"dg": [out[2], out[3]], "hdg": [out[4], out[5]]}}
+                "tune_ms": {"dg": [out[2], out[3]], "hdg": [out[4], out[5]]},
+                "solve_shape": int(shape[0]), "solve_ms": [shape[1], shape[2]],
+                "fused_ctas": int(shape[3]), "fused_ms": [shape[4], shape[5]]}
+
+    def solve_shape(self, shape: int):
+        """Grid shape of the DG block-Jacobi solves, 0 or 1 (dgh_shape_set)."""
+        self._rc(self.lib.dgh_shape_set(self.h, 0, int(shape)))
+
+    def fused_ctas(self, ctas: int):
+        """CTAs per SM of the fused reduced-precision DG factorisation, 1 or 2 (dgh_shape_set)."""
+        self._rc(self.lib.dgh_shape_set(self.h, 1, int(ctas)))
 
     # ---- GMRES
     def gmres_graph(self, on: bool = True):
@@ -409,6 +422,21 @@ class Batch:
             rc = self.lib.dgh_gmres_graph_enable(self.member_ctx(i), 1 if on else 0)
             if rc != 0:
                 raise DGHError(rc, self.lib.dgh_last_error(self.member_ctx(i)).decode())
+
+    def lockstep(self, on: bool = True):
+        """Run the 2D DG members' GMRES solves in lockstep, each Arnoldi phase one launch over all
+        members of a group (dgh_batch_lockstep)."""
+        rc = self.lib.dgh_batch_lockstep(self.h, 1 if on else 0)
+        if rc != 0:
+            raise DGHError(rc, self.lib.dgh_batch_error(None, 0).decode())
+
+    def lockstep_report(self) -> dict:
+        """Sessions, restart cycles, Arnoldi steps and kernel launches of the lockstep groups."""
+        out = (ctypes.c_int64 * 4)()
+        rc = self.lib.dgh_batch_lockstep_report(self.h, out)
+        if rc != 0:
+            raise DGHError(rc, "dgh_batch_lockstep_report")
+        return {"sessions": out[0], "cycles": out[1], "steps": out[2], "launches": out[3]}
 
     def _check(self, rc, status):
         if rc != 0:

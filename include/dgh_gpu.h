@@ -78,8 +78,9 @@ typedef struct dgh_config {
     int device;       /* CUDA device ordinal                                               */
     int dim;          /* 2 (dg_hdg_2d, the default) or 1 (dg_hdg_1d)                       */
     int autotune;     /* 2D: time the factorisation variants on the first refresh (per degree) */
-    int preconditioner; /* 0 block Jacobi; 1 block ILU(0), natural ordering (1D only,        */
-                        /* common/src/linalg/block_ilu.cpp:15-84)                            */
+    int preconditioner; /* 0 block Jacobi; 1 block ILU(0), natural ordering                   */
+                        /* (common/src/linalg/block_ilu.cpp:15-84): 1D, and 2D for method DG  */
+                        /* (level-scheduled sweeps; not for the adjoint operator)             */
     int condense32;     /* 2D HDG: 1 = FP32 condensation (see dgh_hdg_retarget); 0 = FP64     */
     int forcing;        /* linear solve stop: 0 = the reference's relative ltol; 1 = also stop */
                         /* at an absolute floor: min(allowance / 2, ntol max(1, r0) sqrt(lx ly) / 10) */
@@ -209,6 +210,20 @@ int dgh_gmres(dgh_ctx *ctx, int op, const double *rhs, double *x, int limit, dou
  * context has not factored yet; out[2..5] = the last tuning times in ms (DG 0, DG 1, HDG 0,
  * HDG 1; 0 where not timed). */
 int dgh_autotune_report(const dgh_ctx *ctx, double out[6]);
+/* Launch shapes inside a variant, tuned per degree with autotune set (no counterpart in the
+ * reference).  DGH_SHAPE_SOLVE_GRID: the grid of the 2D DG block-Jacobi solves, 0 = every
+ * resident CTA slot, 1 = the fewest CTAs with the same number of rounds of blocks per warp (equal
+ * shares); timed at the first DG refresh on the context's own factors, cached per (degree,
+ * precision, cell count); default 0.  DGH_SHAPE_FUSED_CTAS: CTAs per SM of the fused reduced-
+ * precision DG factorisation, 1 (each CTA's FP64 slot fits L2) or 2 (twice the warps); timed at
+ * the first DG refresh on a sample of the cells, cached per (degree, precision); default 2.
+ * dgh_shape_set fixes a shape instead; every shape computes the same bits.
+ * dgh_autotune_shapes: out[0] = the solve grid shape in use (-1 before the first DG refresh),
+ * out[1..2] its tuning times (ms) for shapes 0 and 1; out[3] = the fused CTAs per SM in use
+ * (-1 before), out[4..5] its tuning times for 1 and 2 (0 where not timed). */
+enum { DGH_SHAPE_SOLVE_GRID = 0, DGH_SHAPE_FUSED_CTAS = 1 };
+int dgh_autotune_shapes(const dgh_ctx *ctx, double out[6]);
+int dgh_shape_set(dgh_ctx *ctx, int which, int value);
 /* Replay each GMRES restart cycle as one CUDA graph (its Arnoldi steps are conditional nodes
  * that stop at the reference's inner-loop break, gmres.cpp:65-67) instead of launching it step
  * by step with a host read of the continue flag after every step.  Both ways run the same
@@ -293,6 +308,38 @@ int dgh_batch_stage_begin(dgh_batch *batch, const double *const *host_states, do
 int dgh_batch_newton_update(dgh_batch *batch, dgh_update_stats *stats, int *status);
 /* Member i's current Newton state, copied to the host (size dgh_sizes()[0] of its context). */
 int dgh_batch_download(dgh_batch *batch, int member, double *host_state);
+/* on = 1: from the next dgh_batch_newton_update on, the 2D DG members' GMRES solves run in
+ * lockstep (dgh_lockstep groups, below: one per class of members sharing precision, restart
+ * length and device, on the collocated rule with block Jacobi): every phase of an Arnoldi step is
+ * one kernel launch over all members of a group; each member's rows stay bitwise those of its
+ * own run.  Other members (HDG, 1D, over-integrated, ILU) keep solving independently.  on = 0
+ * returns to independent solves. */
+int dgh_batch_lockstep(dgh_batch *batch, int on);
+/* The sum of the batch's lockstep groups' dgh_lockstep_report (zeros without any). */
+int dgh_batch_lockstep_report(const dgh_batch *batch, int64_t out[4]);
+
+/* ---- Lockstep group of DG GMRES solves (no counterpart in the reference) ------------------------
+ * The restart cycles of the DG GMRES solves of several 2D contexts — any degree and mesh size —
+ * advanced together: per Arnoldi step one launch of each phase over all members (the block
+ * solve once per factor layout present, J*v once per degree present, the CGS2 sweeps,
+ * reductions and Givens updates once), each member on its own buffers with its own block
+ * partition, so every member's result is bitwise its dgh_gmres result.  Members share device,
+ * precision and restart length, use the collocated rule and block Jacobi, and belong to one
+ * group at a time; destroy the group before its member contexts.
+ * A session: dgh_lockstep_begin(group, expected) opens it for `expected` members; each of them
+ * then either calls dgh_gmres(ctx, DGH_OP_DG, ...) (directly or through its integrator) — the
+ * call waits until all expected members have arrived, and the last one to arrive issues the
+ * lockstep solve on the group's stream — or calls dgh_lockstep_leave(group, ctx) to drop out
+ * (a member whose update failed before its solve).  The members' calls come from different host
+ * threads (one per member); contexts outside an open session solve independently.
+ * dgh_lockstep_report: sessions, restart cycles, Arnoldi steps and kernel launches so far. */
+typedef struct dgh_lockstep dgh_lockstep;
+int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out);
+int dgh_lockstep_destroy(dgh_lockstep *group);
+const char *dgh_lockstep_error(void);
+int dgh_lockstep_begin(dgh_lockstep *group, int expected);
+int dgh_lockstep_leave(dgh_lockstep *group, dgh_ctx *member);
+int dgh_lockstep_report(const dgh_lockstep *group, int64_t out[4]);
 
 /* ---- Discrete adjoint of the DG time integration (no counterpart in the reference) -------------
  * Objective J = sum over nodes of M rho^2 at the end of `steps` fixed steps (dt = cfl / rate of
