@@ -476,9 +476,9 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
     {32,64,96,128}, DG or HDG, amplitude-scaled initial states, BE CFL 5, GMRES(30), mixed
     precision): `updates` Newton updates of every member run one member at a time, then all
     members together through dgh_batch (independent solves, each member on its own stream), then
-    through dgh_batch with the DG members' GMRES solves in lockstep (every Arnoldi phase one
-    launch over them); member-updates per second for each and whether every member's rows agree
-    bitwise with its one-at-a-time run."""
+    through dgh_batch with the members' GMRES solves in lockstep (DG and HDG members in a group
+    each, every Arnoldi phase one launch over a group); member-updates per second for each and
+    whether every member's rows agree bitwise with its one-at-a-time run."""
     from dg_hdg_euler_cpp_b200.solver import Batch, batch_member, perturb
 
     draws = [batch_member(s) for s in range(members)]
@@ -538,12 +538,12 @@ def uneven_batch(torch, local: int, members: int = 16, updates: int = 3, graph: 
             "lockstep": {"seconds": lock_s, "member_updates_per_s": work / lock_s,
                          "speedup_vs_one_at_a_time": seq_s / lock_s,
                          "bitwise_equal_rows": same_as_single(lock_rows),
-                         "dg_members": sum(1 for c in cfgs if c["method"] == "dg"),
+                         "groups": "the DG members in one lockstep group, the HDG members in another",
                          "group": lock_report,
-                         "note": "DG members' GMRES cycles in lockstep, " +
+                         "note": "GMRES cycles in lockstep, " +
                                  ("each restart cycle one CUDA graph launch whose Arnoldi steps run while any member "
                                   "continues" if graph else "stepped: the host reads one continue flag per member per "
-                                  "Arnoldi step") + "; HDG members solve independently"}}
+                                  "Arnoldi step")}}
 
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}

@@ -145,6 +145,7 @@ SIGNATURES = {
     "dgh_batch_lockstep": (ctypes.c_int, [_VP, ctypes.c_int]),
     "dgh_batch_lockstep_report": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "dgh_lockstep_create": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.POINTER(_VP)]),
+    "dgh_lockstep_create_op": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "dgh_lockstep_destroy": (ctypes.c_int, [_VP]),
     "dgh_lockstep_error": (ctypes.c_char_p, []),
     "dgh_lockstep_begin": (ctypes.c_int, [_VP, ctypes.c_int]),

@@ -289,7 +289,7 @@ struct dgh_ctx {
 // brings one DG GMRES solve.  The member that completes the count issues the whole lockstep
 // solve on the group's stream; the others wait, then continue on their own streams.
 struct dgh_lockstep {
-    int device = 0, restart = 0, precision = 0;
+    int device = 0, restart = 0, precision = 0, op = DGH_OP_DG;
     cudaStream_t stream = nullptr;
     cudaEvent_t finished = nullptr;
     std::vector<dgh_ctx *> members;
@@ -297,8 +297,11 @@ struct dgh_lockstep {
         int first = 0, count = 0, key = 0, blocks = 0;
         size_t smem = 0;
     };
-    std::vector<Range> degrees;  // J·v launches: key = n (nodes per direction)
-    std::vector<Range> layouts;  // block solves: key 0 FP64, 1 FP32, 2 FP32 narrow (m < 64), 3 FP16
+    std::vector<Range> degrees;  // operator launches (J·v or Schur apply): key = n (nodes per direction)
+    // block-Jacobi launches: key 0 FP64 LU, 1 FP32 LU, 2 FP32 LU narrow (m < 64), 3 FP16 LU,
+    // 4 FP32 inverses (HDG face blocks); for HDG groups re-planned every session
+    std::vector<Range> layouts;
+    std::vector<int> layout_keys;  // the keys the captured cycle graph was built with
     int red_total = 0;
     LsMember *table = nullptr, *host = nullptr;  // device table and its pinned host image
     int *flags = nullptr, *flags_host = nullptr;
@@ -1099,9 +1102,9 @@ __global__ void k_gmres_setup(GmresDev *d, double rhs_norm, double tol, int limi
     d->count = 0;
 }
 
-bool lockstep_gmres(dgh_ctx *c, const double *rhs, double *x, int limit, double tol, int &iters, double &rel);
+bool lockstep_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel);
 void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
-    if (op == DGH_OP_DG && c->ls && lockstep_gmres(c, rhs, x, limit, tol, iters, rel)) return;
+    if (c->ls && lockstep_gmres(c, op, rhs, x, limit, tol, iters, rel)) return;
     GmresCall g;
     g.op = op;
     g.n = op == DGH_OP_HDG ? c->NT : c->N;
@@ -1182,20 +1185,60 @@ void ls_solve_all(dgh_lockstep *L, int src, int dst, int j, int gate) {
         else if (r.key == 2)
             k_ls_solve<float, true><<<r.blocks, SOLVE_THREADS, r.smem, L->stream>>>(L->table, r.first, r.count, src, dst,
                                                                                    j, gate);
-        else
+        else if (r.key == 3)
             k_ls_solve_half<<<r.blocks, SOLVE_THREADS, r.smem, L->stream>>>(L->table, r.first, r.count, src, dst, j, gate);
+        else
+            k_ls_inv_apply<<<r.blocks, INV_APPLY_THREADS, 0, L->stream>>>(L->table, r.first, r.count, src, dst, j, gate);
         L->launched();
     }
 }
-// dst = J src for every gated member: the face traces of src, then J·v, one pair of launches per degree.
+// dst = A src for every gated member, per degree: the face traces of src and J·v (DG, two
+// launches), or the condensed Schur apply (HDG, one launch, a CTA per face).
 void ls_jv_all(dgh_lockstep *L, int src, int dst, int gate) {
     for (const auto &r : L->degrees) {
+        if (L->op == DGH_OP_HDG) {
+            DGH_DISPATCH_N(r.key, {
+                k_ls_hdg_apply<N><<<r.blocks, 256, 0, L->stream>>>(L->table, r.first, r.count, src, dst, gate);
+            });
+            L->launched();
+            continue;
+        }
         DGH_DISPATCH_N(r.key, {
             k_ls_face_trace<N><<<r.blocks, Team<N>::THREADS, 0, L->stream>>>(L->table, r.first, r.count, src, gate);
             k_ls_dg_apply<N><<<r.blocks, Team<N>::THREADS, 0, L->stream>>>(L->table, r.first, r.count, src, dst, gate);
         });
         L->launched(2);
     }
+}
+// The HDG members' face-block Jacobi launches from their current state (FP32 inverses or LU
+// factors, chosen at each refresh): consecutive members with the same form share a launch.
+void ls_plan_face_precond(dgh_lockstep *L) {
+    constexpr int wpc = SOLVE_THREADS / 32;
+    L->layouts.clear();
+    std::vector<int> keys;
+    for (int i = 0; i < (int)L->members.size(); ++i) {
+        const dgh_ctx *c = L->members[i];
+        const int key = c->face_inverse ? 4 : c->mixed() ? 2 : 0;
+        keys.push_back(key);
+        if (L->layouts.empty() || L->layouts.back().key != key) {
+            dgh_lockstep::Range r;
+            r.first = i;
+            r.key = key;
+            L->layouts.push_back(r);
+        }
+        auto &lr = L->layouts.back();
+        L->host[i].solve0 = lr.blocks;
+        L->host[i].pool = c->face_pool;
+        L->host[i].perm = c->face_perm;
+        lr.blocks += (c->faces + wpc - 1) / wpc;
+        ++lr.count;
+        if (key != 4) lr.smem = std::max(lr.smem, (key == 0 ? sizeof(double) : sizeof(float)) * (size_t)c->fw * wpc);
+    }
+    if (keys != L->layout_keys && L->cycle) {  // a different launch plan: capture the cycle again
+        ck(cudaGraphExecDestroy(L->cycle), "cudaGraphExecDestroy");
+        L->cycle = nullptr;
+    }
+    L->layout_keys = keys;
 }
 // The three segments of a lockstep restart cycle (gmres()'s start, Arnoldi step j, finish) on
 // stream `st`; each returns the launches it issued.
@@ -1327,6 +1370,7 @@ void ls_run(dgh_lockstep *L) {
     }
     if (!any) return;
     ++L->sessions;
+    if (L->op == DGH_OP_HDG) ls_plan_face_precond(L);
     if (graph && !L->cycle) ls_build_graph(L);
     const size_t tb = sizeof(LsMember) * (size_t)cnt;
     for (;;) {
@@ -1425,8 +1469,9 @@ void ls_arrive(dgh_lockstep *L, int idx) {
 }
 // gmres() of op DG for a member of an open session: the solve's own copies and |rhs| on the
 // member's stream, then the rendezvous; false when the context has no open session to join.
-bool lockstep_gmres(dgh_ctx *c, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
+bool lockstep_gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double tol, int &iters, double &rel) {
     dgh_lockstep *L = c->ls;
+    if (op != L->op) return false;
     {
         std::lock_guard<std::mutex> lk(L->mu);
         if (!L->open) return false;
@@ -1434,12 +1479,13 @@ bool lockstep_gmres(dgh_ctx *c, const double *rhs, double *x, int limit, double 
         if (sl.arrived || sl.withdrawn) return false;  // one solve per member and session
     }
     auto &sl = L->slots[c->ls_index];
-    const long long n = c->N;
-    double *r = c->gres[DGH_OP_DG];
+    const long long n = op == DGH_OP_HDG ? c->NT : c->N;
+    double *r = c->gres[op];
     ck(cudaMemcpyAsync(c->g_rhs, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
     ck(cudaMemsetAsync(c->g_x, 0, n * sizeof(double), c->stream), "memset");
     ck(cudaMemcpyAsync(r, c->g_rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
-    const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(c->g_rhs, c->inv_mass, false, n)));
+    const double *W = op == DGH_OP_HDG ? c->inv_trace_mass : c->inv_mass;
+    const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(c->g_rhs, W, false, n)));
     sl.tol = tol;
     sl.limit = limit;
     sl.rhs_norm = rhs_norm;
@@ -3110,7 +3156,12 @@ extern "C" {
 const char *dgh_lockstep_error(void) { return g_ls_error.c_str(); }
 
 int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) {
-    if (!members || count <= 0 || !out) return DGH_ERR_INVALID;
+    return dgh_lockstep_create_op(members, count, DGH_OP_DG, out);
+}
+
+int dgh_lockstep_create_op(dgh_ctx *const *members, int count, int op, dgh_lockstep **out) {
+    if (!members || count <= 0 || !out || (op != DGH_OP_DG && op != DGH_OP_HDG)) return DGH_ERR_INVALID;
+    const bool hdg = op == DGH_OP_HDG;
     *out = nullptr;
     auto reject = [&](int i, const char *m) {
         g_ls_error = "lockstep member " + std::to_string(i) + ": " + m;
@@ -3120,7 +3171,8 @@ int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) 
         const dgh_ctx *c = members[i];
         if (!c) return reject(i, "null context");
         if (c->d1()) return reject(i, "lockstep members are 2D contexts");
-        if (!c->has_dg()) return reject(i, "the context has no DG operator");
+        if (!hdg && !c->has_dg()) return reject(i, "the context has no DG operator");
+        if (hdg && !c->has_hdg()) return reject(i, "the context has no HDG operator");
         if (c->overint()) return reject(i, "lockstep members use the collocated volume rule");
         if (c->ilu()) return reject(i, "lockstep members use block Jacobi");
         if (c->ls) return reject(i, "the context is already in a lockstep group");
@@ -3129,7 +3181,8 @@ int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) 
         const dgh_ctx *c0 = members[0];
         if (c->cfg.device != c0->cfg.device) return reject(i, "lockstep members share one device");
         if (c->cfg.precision != c0->cfg.precision) return reject(i, "lockstep members share one precision");
-        if (std::min<long long>(c->N, c->cfg.restart) != std::min<long long>(c0->N, c0->cfg.restart))
+        const long long n = hdg ? c->NT : c->N, n0 = hdg ? c0->NT : c0->N;
+        if (std::min<long long>(n, c->cfg.restart) != std::min<long long>(n0, c0->cfg.restart))
             return reject(i, "lockstep members share one GMRES restart length");
     }
     auto *L = new dgh_lockstep;
@@ -3138,7 +3191,8 @@ int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) 
             const dgh_ctx *c0 = members[0];
             L->device = c0->cfg.device;
             L->precision = c0->cfg.precision;
-            L->restart = (int)std::min<long long>(c0->N, c0->cfg.restart);
+            L->op = op;
+            L->restart = (int)std::min<long long>(hdg ? c0->NT : c0->N, c0->cfg.restart);
             ck(cudaSetDevice(L->device), "cudaSetDevice");
             std::vector<int> order(count);
             for (int i = 0; i < count; ++i) order[i] = i;
@@ -3169,10 +3223,10 @@ int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) 
                 t.coef = c->gcoef;
                 t.x = c->g_x;
                 t.rhs = c->g_rhs;
-                t.r = c->gres[DGH_OP_DG];
-                t.W = c->inv_mass;
+                t.r = c->gres[op];
+                t.W = hdg ? c->inv_trace_mass : c->inv_mass;
                 t.ld = (size_t)c->vld;
-                t.n = c->N;
+                t.n = hdg ? c->NT : c->N;
                 t.red_blocks = c->red_grid;
                 t.red0 = L->red_total;
                 L->red_total += c->red_grid;
@@ -3197,11 +3251,20 @@ int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out) 
                     L->degrees.push_back(r);
                 }
                 auto &dr = L->degrees.back();
+                t.team0 = dr.blocks;
+                ++dr.count;
+                if (hdg) {  // the Schur apply: a CTA per face; the face preconditioner is planned per session
+                    dr.blocks += c->faces;
+                    t.S = c->c32() ? (const void *)c->S32 : (const void *)c->S;
+                    t.c32 = c->c32() ? 1 : 0;
+                    t.stride = (size_t)c->fw * c->fw;
+                    t.m = c->fw;
+                    t.cells = c->faces;
+                    continue;
+                }
                 int cpb = 1;
                 DGH_DISPATCH_N(c->n, { cpb = Team<N>::CPB; });
-                t.team0 = dr.blocks;
                 dr.blocks += c->team_blocks(cpb);
-                ++dr.count;
                 const int key = layout_of(c);
                 if (L->layouts.empty() || L->layouts.back().key != key) {
                     dgh_lockstep::Range r;

@@ -182,14 +182,15 @@ __device__ __forceinline__ double widen_scaled(float f) {
     const unsigned b = __float_as_uint(f);
     return __hiloint2double((int)(((b & 0x7fffffffu) >> 3) | (b & 0x80000000u)), (int)(b << 29));
 }
+// (The Schur-apply bodies take their face explicitly, so the batched kernels of a lockstep
+// batch run the same arithmetic per member; every rounding is explicit: fma() and rfma.)
 template <int N>
-__global__ void __launch_bounds__(256)
-k_hdg_apply32(const float *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
-              double *__restrict__ out, Basis1D b, Grid g) {
+__device__ __forceinline__ void hdg_apply32_body(int face, const float *__restrict__ S, const double *__restrict__ speeds,
+                                                 const double *__restrict__ lam, double *__restrict__ out,
+                                                 const Basis1D &b, const Grid &g) {
     constexpr int FW = NVAR * N, T = NFACES * FW, T4 = T / 4, PASSES = (T4 + 31) / 32;
     constexpr double kScale = 0x1p896;  // undoes the 2^-896 of widen_scaled
     __shared__ __align__(16) double loc[2][T];
-    const int face = blockIdx.x;
     const int axis = face >= g.cells, first = face - axis * g.cells, next = neighbor(g, first, 2 * axis + 1);
     for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
         const int which = k / T, s = (k % T) / FW, j = k % FW;
@@ -224,17 +225,22 @@ k_hdg_apply32(const float *__restrict__ S, const double *__restrict__ speeds, co
         if (lane == 0) {
             const int q = row % N;
             const double d = -face_weight(g, b, face, q) * (speeds[2 * (face * N + q)] + speeds[2 * (face * N + q) + 1]);
-            out[(size_t)face * FW + row] = d * lam[(size_t)face * FW + row] + acc;
+            out[(size_t)face * FW + row] = rfma(d, lam[(size_t)face * FW + row], acc);
         }
     }
 }
 template <int N>
 __global__ void __launch_bounds__(256)
-k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
-            double *__restrict__ out, Basis1D b, Grid g) {
+k_hdg_apply32(const float *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
+              double *__restrict__ out, Basis1D b, Grid g) {
+    hdg_apply32_body<N>(blockIdx.x, S, speeds, lam, out, b, g);
+}
+template <int N>
+__device__ __forceinline__ void hdg_apply_body(int face, const double *__restrict__ S, const double *__restrict__ speeds,
+                                               const double *__restrict__ lam, double *__restrict__ out,
+                                               const Basis1D &b, const Grid &g) {
     constexpr int FW = NVAR * N, T = NFACES * FW, T2 = T / 2, PASSES = (T2 + 31) / 32;
     __shared__ __align__(16) double loc[2][T];
-    const int face = blockIdx.x;
     const int axis = face >= g.cells, first = face - axis * g.cells, next = neighbor(g, first, 2 * axis + 1);
     for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
         const int which = k / T, s = (k % T) / FW, j = k % FW;
@@ -254,7 +260,7 @@ k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, con
             const int j = lane + 32 * t;
             if (j < T2) {
                 const double2 a = s1[j], b = s2[j], x = l0[j], y = l1[j];
-                acc += a.x * x.x + a.y * x.y + b.x * y.x + b.y * y.y;
+                acc = radd(acc, rfma(a.x, x.x, rfma(a.y, x.y, rfma(b.x, y.x, rmul(b.y, y.y)))));
             }
         }
 #pragma unroll
@@ -262,9 +268,15 @@ k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, con
         if (lane == 0) {
             const int q = row % N;
             const double d = -face_weight(g, b, face, q) * (speeds[2 * (face * N + q)] + speeds[2 * (face * N + q) + 1]);
-            out[(size_t)face * FW + row] = d * lam[(size_t)face * FW + row] + acc;
+            out[(size_t)face * FW + row] = rfma(d, lam[(size_t)face * FW + row], acc);
         }
     }
+}
+template <int N>
+__global__ void __launch_bounds__(256)
+k_hdg_apply(const double *__restrict__ S, const double *__restrict__ speeds, const double *__restrict__ lam,
+            double *__restrict__ out, Basis1D b, Grid g) {
+    hdg_apply_body<N>(blockIdx.x, S, speeds, lam, out, b, g);
 }
 
 // du = -X l_local - y per cell (hybrid.cpp:97-105).

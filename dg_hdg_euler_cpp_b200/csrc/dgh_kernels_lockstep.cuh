@@ -7,13 +7,17 @@
 // numbers are bitwise those of its single-problem solve (gmres.cpp:17-86, same kernels).
 #pragma once
 #include "dgh_kernels_dg.cuh"
+#include "dgh_kernels_hdg.cuh"
 #include "dgh_kernels_krylov.cuh"
 #include "dgh_kernels_lu.cuh"
 
 namespace dgh {
 
-// One member: its context's GMRES state and vectors, its block-Jacobi factors, its J·v caches
-// and the first CTA of each batched launch it takes part in.
+// One member: its context's GMRES state and vectors, its block-Jacobi factors, its operator's
+// data and the first CTA of each batched launch it takes part in.  A DG member (operator J)
+// carries its cell-block factors and J·v caches; an HDG member (the condensed Schur operator)
+// carries its face-block factors or FP32 inverses in the same fields (m = fw, cells = faces)
+// and its Schur blocks S (FP64, or FP32 with c32).
 struct LsMember {
     GmresDev *gdev;
     double *V, *w, *z, *red, *partial, *coef, *x, *rhs, *r;
@@ -35,7 +39,10 @@ struct LsMember {
     const Basis1D *basis;
     Grid g;
     double inv_step;
-    int team0;  // first CTA in the batched J·v of its degree
+    int team0;  // first CTA in the batched operator launch of its degree (J·v: cell teams; Schur: faces)
+    // condensed Schur operator (HDG members)
+    const void *S;
+    int c32;
 };
 
 // vector selectors of the batched kernels
@@ -173,6 +180,28 @@ k_ls_solve_half(const LsMember *t, int first, int count, int src, int dst, int j
     const int blocks = (i + 1 < first + count ? t[i + 1].solve0 : gridDim.x) - a.solve0;
     lu_solve_half_body(blockIdx.x - a.solve0, blocks, (const __half *)a.pool, a.scale, a.perm, a.m, a.cells,
                        ls_vec(a, src, j), ls_vec(a, dst, j));
+}
+
+// ---- face-block Jacobi of HDG members from FP32 inverses (k_inv_apply's body) ----------------
+__global__ void __launch_bounds__(INV_APPLY_THREADS)
+k_ls_inv_apply(const LsMember *t, int first, int count, int src, int dst, int j, int gate) {
+    const int i = ls_find(t, first, count, blockIdx.x, LS_SOLVE);
+    const LsMember &a = t[i];
+    if (!ls_on(a, gate)) return;
+    const int blocks = (i + 1 < first + count ? t[i + 1].solve0 : gridDim.x) - a.solve0;
+    inv_apply_body(blockIdx.x - a.solve0, blocks, (const float *)a.pool, a.m, a.cells, ls_vec(a, src, j),
+                   ls_vec(a, dst, j));
+}
+
+// ---- condensed Schur apply of HDG members [first, first + count), all of degree N - 1 ----------
+template <int N>
+__global__ void __launch_bounds__(256) k_ls_hdg_apply(const LsMember *t, int first, int count, int src, int dst,
+                                                      int gate) {
+    const LsMember &a = t[ls_find(t, first, count, blockIdx.x, LS_TEAM)];
+    if (!ls_on(a, gate)) return;
+    const int face = blockIdx.x - a.team0;
+    if (a.c32) hdg_apply32_body<N>(face, (const float *)a.S, a.speeds, ls_vec(a, src, 0), ls_vec(a, dst, 0), *a.basis, a.g);
+    else hdg_apply_body<N>(face, (const double *)a.S, a.speeds, ls_vec(a, src, 0), ls_vec(a, dst, 0), *a.basis, a.g);
 }
 
 // ---- J·v of the members [first, first + count), all of degree N - 1 --------------------------

@@ -572,11 +572,11 @@ k_inv_narrow(const double *__restrict__ pool, int m, int count, float *__restric
 // computes rows r and r + 32 (FP32 accumulation) from 16-byte loads of its row, b broadcast by
 // shuffles.  m is a multiple of 4 (m = 4n).
 constexpr int INV_APPLY_THREADS = 256;
-__global__ void __launch_bounds__(INV_APPLY_THREADS)
-k_inv_apply(const float *__restrict__ inv, int m, int count, const double *__restrict__ rhs, double *__restrict__ z) {
+__device__ __forceinline__ void inv_apply_body(int bx, int G, const float *__restrict__ inv, int m, int count,
+                                               const double *__restrict__ rhs, double *__restrict__ z) {
     const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (INV_APPLY_THREADS / 32);
-    for (int blk = blockIdx.x * (INV_APPLY_THREADS / 32) + (threadIdx.x >> 5); blk < count; blk += warps) {
+    const int warps = G * (INV_APPLY_THREADS / 32);
+    for (int blk = bx * (INV_APPLY_THREADS / 32) + (threadIdx.x >> 5); blk < count; blk += warps) {
         const float4 *A4 = reinterpret_cast<const float4 *>(inv + (size_t)blk * m * m);
         const double *b = rhs + (size_t)blk * m;
         const float b0 = lane < m ? (float)b[lane] : 0.f, b1 = lane + 32 < m ? (float)b[lane + 32] : 0.f;
@@ -603,6 +603,10 @@ k_inv_apply(const float *__restrict__ inv, int m, int count, const double *__res
         if (r0) z[(size_t)blk * m + lane] = (double)acc0;
         if (r1) z[(size_t)blk * m + lane + 32] = (double)acc1;
     }
+}
+__global__ void __launch_bounds__(INV_APPLY_THREADS)
+k_inv_apply(const float *__restrict__ inv, int m, int count, const double *__restrict__ rhs, double *__restrict__ z) {
+    inv_apply_body(blockIdx.x, gridDim.x, inv, m, count, rhs, z);
 }
 
 // Block solve z = A^{-1} b with the factors of k_lu (block_jacobi.hpp:24-39): permute, unit

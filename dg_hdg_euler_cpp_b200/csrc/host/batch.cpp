@@ -33,8 +33,8 @@ struct dgh_batch {
     int pending = 0;
     bool quit = false;
     std::function<int(int)> job;
-    // lockstep groups of the DG members' GMRES solves (dgh_batch_lockstep): one per class of
-    // members that can share one (2D, collocated rule, block Jacobi, same precision and restart)
+    // lockstep groups of the members' GMRES solves (dgh_batch_lockstep): one per class of members
+    // that can share one (2D, collocated rule, block Jacobi, same method, precision and restart)
     std::vector<dgh_lockstep *> groups;
     std::vector<int> group_size, group_of;  // members per group; each member's group or -1
     void drop_groups() {
@@ -202,16 +202,18 @@ int dgh_batch_lockstep(dgh_batch *b, int on) {
     if (!b) return DGH_ERR_INVALID;
     b->drop_groups();
     if (!on) return DGH_OK;
-    // classes of DG members that can share a group; the others keep solving independently
+    // classes of members that can share a group; the others keep solving independently
     std::vector<std::vector<int>> classes;
     std::vector<const dgh_config *> key;
     for (int i = 0; i < b->count; ++i) {
         const dgh_config &c = b->cfg[i];
         const bool collocated = c.quadrature == 0 || c.quadrature <= c.degree + 1;
-        if (c.method != DGH_METHOD_DG || c.dim == 1 || !collocated || c.preconditioner != 0) continue;
+        if (c.method == DGH_METHOD_BOTH || c.dim == 1 || !collocated || c.preconditioner != 0) continue;
         int cls = -1;
         for (int q = 0; q < (int)key.size(); ++q)
-            if (key[q]->precision == c.precision && key[q]->restart == c.restart && key[q]->device == c.device) cls = q;
+            if (key[q]->method == c.method && key[q]->precision == c.precision && key[q]->restart == c.restart &&
+                key[q]->device == c.device)
+                cls = q;
         if (cls < 0) {
             cls = (int)key.size();
             key.push_back(&c);
@@ -223,7 +225,8 @@ int dgh_batch_lockstep(dgh_batch *b, int on) {
         std::vector<dgh_ctx *> ctxs;
         for (int i : members) ctxs.push_back(b->ctx[i]);
         dgh_lockstep *g = nullptr;
-        const int rc = dgh_lockstep_create(ctxs.data(), (int)ctxs.size(), &g);
+        const int op = b->cfg[members[0]].method == DGH_METHOD_HDG ? DGH_OP_HDG : DGH_OP_DG;
+        const int rc = dgh_lockstep_create_op(ctxs.data(), (int)ctxs.size(), op, &g);
         if (rc != DGH_OK) {
             g_batch_create_error = dgh_lockstep_error();
             b->drop_groups();

@@ -308,11 +308,11 @@ int dgh_batch_stage_begin(dgh_batch *batch, const double *const *host_states, do
 int dgh_batch_newton_update(dgh_batch *batch, dgh_update_stats *stats, int *status);
 /* Member i's current Newton state, copied to the host (size dgh_sizes()[0] of its context). */
 int dgh_batch_download(dgh_batch *batch, int member, double *host_state);
-/* on = 1: from the next dgh_batch_newton_update on, the 2D DG members' GMRES solves run in
- * lockstep (dgh_lockstep groups, below: one per class of members sharing precision, restart
+/* on = 1: from the next dgh_batch_newton_update on, the 2D members' GMRES solves run in lockstep
+ * (dgh_lockstep groups, below: one per class of members sharing method, precision, restart
  * length and device, on the collocated rule with block Jacobi): every phase of an Arnoldi step is
  * one kernel launch over all members of a group; each member's rows stay bitwise those of its
- * own run.  Other members (HDG, 1D, over-integrated, ILU) keep solving independently.  on = 0
+ * own run.  Other members (1D, over-integrated, ILU) keep solving independently.  on = 0
  * returns to independent solves. */
 int dgh_batch_lockstep(dgh_batch *batch, int on);
 /* The sum of the batch's lockstep groups' dgh_lockstep_report (zeros without any). */
@@ -335,6 +335,12 @@ int dgh_batch_lockstep_report(const dgh_batch *batch, int64_t out[4]);
  * dgh_lockstep_report: sessions, restart cycles, Arnoldi steps and kernel launches so far. */
 typedef struct dgh_lockstep dgh_lockstep;
 int dgh_lockstep_create(dgh_ctx *const *members, int count, dgh_lockstep **out);
+/* The same for the solves of operator op: DGH_OP_DG (as above) or DGH_OP_HDG (the condensed
+ * Schur solves of 2D contexts with the HDG operator: the Schur apply once per degree, the face
+ * preconditioner once per form present, FP32 inverses or LU factors).  An HDG member's first
+ * Schur solve of an update joins the session; further solves of the same update (the reference's
+ * tolerance retries, FP32-condensation refinement passes) run on their own. */
+int dgh_lockstep_create_op(dgh_ctx *const *members, int count, int op, dgh_lockstep **out);
 int dgh_lockstep_destroy(dgh_lockstep *group);
 const char *dgh_lockstep_error(void);
 int dgh_lockstep_begin(dgh_lockstep *group, int expected);

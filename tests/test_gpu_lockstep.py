@@ -1,9 +1,10 @@
-"""Lockstep batch of DG GMRES solves (dgh_batch_lockstep, dgh_lockstep_*): the restart cycles of
+"""Lockstep batch of GMRES solves (dgh_batch_lockstep, dgh_lockstep_*): the restart cycles of
 members of different degree and mesh size advanced together, every Arnoldi phase one kernel
-launch over all of them.  Each member runs its single-problem kernel bodies on its own buffers
-with its own block partitions, so its update rows and states equal its single run bitwise; HDG,
-1D and other members outside a lockstep class keep solving independently; a member whose solve
-fails reports its own error while the others complete."""
+launch over all of them — DG members (block solve + J·v) and HDG members (face preconditioner +
+Schur apply) in groups of their own.  Each member runs its single-problem kernel bodies on its
+own buffers with its own block partitions, so its update rows and states equal its single run
+bitwise; 1D and other members outside a lockstep class keep solving independently; a member
+whose solve fails reports its own error while the others complete."""
 import ctypes
 
 import numpy as np
@@ -87,9 +88,23 @@ def test_lockstep_members_equal_single_runs_bitwise(precision, graph):
     assert_equal_to_single_runs(members, u0, dts, rows, finals, updates)
 
 
+@pytest.mark.parametrize("precision,condense32,graph", [("mixed", 0, False), ("fp64", 0, False), ("mixed", 1, False),
+                                                       ("mixed", 0, True)])
+def test_lockstep_hdg_members_equal_single_runs_bitwise(precision, condense32, graph):
+    """Six HDG members of degrees 1-8 in lockstep (FP32 face inverses, or FP64 face LU factors;
+    with the FP32 condensation the FP32 Schur blocks and, after the first lockstep solve, the
+    refinement passes' solves on their own), three Newton updates."""
+    members = [dict(COMMON, method="hdg", precision=precision, condense32=condense32, **m) for m in DG_MEMBERS[:6]]
+    updates = 3
+    u0, dts, rows, finals, report = run_batch(members, AMPLITUDES[:6], updates, graph=graph)
+    assert report["sessions"] == updates and report["steps"] > 0
+    assert_equal_to_single_runs(members, u0, dts, rows, finals, updates)
+
+
 def test_lockstep_leaves_other_members_independent():
-    """DG members in two lockstep classes (two precisions) beside HDG, 1D and over-integrated DG
-    members, which keep solving on their own; everything equals the single runs bitwise."""
+    """DG members in two lockstep classes (two precisions) and an HDG member in a third, beside 1D
+    and over-integrated DG members, which keep solving on their own; everything equals the single
+    runs bitwise."""
     members = [dict(COMMON, method="dg", precision="mixed", **DG_MEMBERS[0]),
                dict(COMMON, method="hdg", precision="mixed", nx=6, ny=5, k=3),
                dict(COMMON, method="dg", precision="fp64", **DG_MEMBERS[2]),
@@ -99,7 +114,7 @@ def test_lockstep_leaves_other_members_independent():
                dict(COMMON, method="dg", precision="fp64", **DG_MEMBERS[3])]
     amplitudes = [0.1, 0.2, 0.05, 0.15, 0.1, 0.0, 0.12]
     u0, dts, rows, finals, report = run_batch(members, amplitudes, 2)
-    assert report["sessions"] == 2 * 2  # two groups (mixed, fp64), two updates
+    assert report["sessions"] == 3 * 2  # three groups (DG mixed, DG fp64, HDG mixed), two updates
     assert_equal_to_single_runs(members, u0, dts, rows, finals, 2)
 
 
