@@ -1,7 +1,8 @@
-// Lockstep batch of DG GMRES solves (no counterpart in the reference): the restart cycles of
-// many independent DG Newton systems — of any degree and mesh size — advanced together, each
-// phase of an Arnoldi step one kernel launch over all members (the J·v launches once per degree
-// present, the block solve once per factor layout present).  A launch's CTAs are split into
+// Lockstep batch of GMRES solves (no counterpart in the reference): the restart cycles of many
+// independent DG Newton systems, or of many condensed HDG Schur systems, of any degree and mesh
+// size, advanced together, each phase of an Arnoldi step one kernel launch over all members
+// (the operator once per degree present, the block-Jacobi preconditioner once per factor
+// layout present).  A launch's CTAs are split into
 // per-member ranges; each CTA finds its member in the table and runs the single-problem kernel
 // body on that member's own buffers with that member's own block partition, so every member's
 // numbers are bitwise those of its single-problem solve (gmres.cpp:17-86, same kernels).
