@@ -153,6 +153,17 @@ SIGNATURES = {
     "dgh_lockstep_report": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "dgh_residual_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             _VP, _VP, _VP, _VP, _VP, ctypes.c_char_p, ctypes.c_int]),
+    "dgh_slab_rows": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _I]),
+    "dgh_comm_local_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
+    "dgh_comm_nccl_unique_id": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ubyte)]),
+    "dgh_comm_nccl_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(_VP)]),
+    "dgh_comm_info": (ctypes.c_int, [_VP, _I]),
+    "dgh_comm_fail": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    "dgh_comm_destroy": (ctypes.c_int, [_VP]),
+    "dgh_comm_error": (ctypes.c_char_p, []),
+    "dgh_ctx_create_slab": (ctypes.c_int, [ctypes.POINTER(dgh_config), _VP, ctypes.POINTER(_VP)]),
+    "dgh_slab_info": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
 }
 
 _lib = None

@@ -51,6 +51,7 @@ struct Grid {
     int nx, ny, cells;
     double hx, hy;
     double gamma;
+    int row0;  // global row of local row 0 (a slab of a decomposed mesh; 0 for the whole mesh)
 };
 
 __host__ __device__ inline int neighbor(const Grid &g, int cell, int side) {

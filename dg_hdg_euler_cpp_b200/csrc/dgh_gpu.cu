@@ -4,6 +4,7 @@
 // share the GMRES, the Arnoldi kernels, the vector helpers and the host integrator, and differ
 // in their discretisation kernels (dgh_kernels_dg/hdg.cuh versus dgh_kernels_1d.cuh).
 #include "dgh_gpu.h"
+#include "host/slab.hpp"
 #include "dgh_kernels_1d.cuh"
 #include "dgh_kernels_ilu1d.cuh"
 #include "dgh_kernels_ilu2d.cuh"
@@ -191,6 +192,25 @@ struct dgh_ctx {
     // lockstep batch this context's DG GMRES solves join while a session is open (-1: none)
     dgh_lockstep *ls = nullptr;
     int ls_index = -1;
+    // slab of a decomposed mesh (dgh_ctx_create_slab): global rows [row0, row0 + rows) of ny,
+    // held as local rows 1..rows between ghost rows 0 and rows+1 that the halo exchange fills;
+    // row_len doubles per cell row of a volume vector; buf: device scratch of host collectives
+    struct Slab {
+        dgh_comm *comm = nullptr;
+        int row0 = 0, rows = 0, ny = 0;
+        long long row_len = 0;
+        double *buf = nullptr;
+    } slab;
+    bool slabbed() const { return slab.comm != nullptr; }
+    // a host value reduced over the slab ranks (op 0 sum, 1 maximum); the value itself otherwise
+    void slab_reduce(double *v, int count, int op) {
+        if (!slabbed()) return;
+        ck(cudaMemcpyAsync(slab.buf, v, count * sizeof(double), cudaMemcpyHostToDevice, stream), "copy");
+        slab.comm->allreduce(slab.buf, count, op, stream);
+        ck(cudaMemcpyAsync(pinned + 8, slab.buf, count * sizeof(double), cudaMemcpyDeviceToHost, stream), "copy");
+        sync();
+        std::memcpy(v, pinned + 8, count * sizeof(double));
+    }
     // one captured restart cycle per operator (conditional Arnoldi steps), rebuilt when the
     // captured stage scalar (1/tau, a kernel argument of J*v) changes
     struct CycleGraph {
@@ -256,9 +276,15 @@ struct dgh_ctx {
     int team_blocks(int cpb) const { return (cells + cpb - 1) / cpb; }
     // Deterministic weighted reduction helpers (return host values).
     double reduce_scalar(const double *x, const double *W, bool divide, long long n_) {
+        if (slabbed() && n_ == N) {  // the interior rows, summed over the ranks
+            x += slab.row_len;
+            W += slab.row_len;
+            n_ = (long long)slab.rows * slab.row_len;
+        }
         k_wnorm2<<<red_grid, KR_THREADS, 0, stream>>>(x, W, divide ? 1 : 0, n_, partial);
         k_reduce<<<1, KR_THREADS, 0, stream>>>(partial, red_grid, red);
         launched(2);
+        if (slabbed()) slab.comm->allreduce(red, 1, 0, stream);
         ck(cudaMemcpyAsync(pinned, red, sizeof(double), cudaMemcpyDeviceToHost, stream), "copy");
         sync();
         return pinned[0];
@@ -268,6 +294,12 @@ struct dgh_ctx {
         ck(cudaMemcpyAsync(pinned, status, sizeof(int), cudaMemcpyDeviceToHost, stream), "copy status");
         sync();
         std::memcpy(&s, pinned, sizeof(int));
+        if (slabbed()) {  // every rank raises the union of the ranks' status bits
+            double bits[8];
+            for (int i = 0; i < 8; ++i) bits[i] = (s >> i) & 1;
+            slab_reduce(bits, 8, 1);
+            for (int i = 0; i < 8; ++i) s |= bits[i] > 0 ? 1 << i : 0;
+        }
         if (s) {
             ck(cudaMemsetAsync(status, 0, sizeof(int), stream), "memset");
             (void)mask_clear;
@@ -332,18 +364,28 @@ struct dgh_lockstep {
 };
 
 namespace {
+// A slab context whose call fails on its own (a CUDA or communication error, which its peers
+// cannot have seen) fails its communicator, so that the peer ranks leave their next collective
+// with DGH_ERR_COMM instead of waiting for it.  Failures decided from reduced values (norms,
+// status bits, GMRES counts) happen on every rank alike and leave the group usable.
 template <class F> int guard(dgh_ctx *ctx, F &&f) {
     if (!ctx) return DGH_ERR_INVALID;
+    int code = DGH_OK;
     try {
         f();
         return DGH_OK;
     } catch (const Failure &e) {
         ctx->err = e.message;
-        return e.code;
+        code = e.code;
+    } catch (const dgh_comm_failure &e) {
+        ctx->err = e.what();
+        code = DGH_ERR_COMM;
     } catch (const std::exception &e) {
         ctx->err = e.what();
-        return DGH_ERR_CUDA;
+        code = DGH_ERR_CUDA;
     }
+    if (ctx->slabbed() && (code == DGH_ERR_CUDA || code == DGH_ERR_COMM)) ctx->slab.comm->fail(ctx->err);
+    return code;
 }
 void need(bool c, const char *m) {
     if (!c) fail(DGH_ERR_INVALID, m);
@@ -405,6 +447,29 @@ void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
         }
     });
     c->launched();
+}
+
+// Slab contexts: the ghost rows of a volume vector filled from the neighbouring slabs (before a
+// kernel reads neighbour cells), or cleared (outputs whose ghost rows hold no equation).  The
+// library owns the ghost rows of the vectors passed to it, const or not.
+void slab_halo(dgh_ctx *c, const double *v) {
+    if (!c->slabbed()) return;
+    c->slab.comm->halo(const_cast<double *>(v), c->slab.row_len, c->slab.rows, c->stream);
+}
+void slab_zero_ghosts(dgh_ctx *c, double *v) {
+    if (!c->slabbed()) return;
+    const size_t bytes = (size_t)c->slab.row_len * sizeof(double);
+    ck(cudaMemsetAsync(v, 0, bytes, c->stream), "memset");
+    ck(cudaMemsetAsync(v + (size_t)(c->slab.rows + 1) * c->slab.row_len, 0, bytes, c->stream), "memset");
+}
+// Device values summed over the slab ranks in place (the Arnoldi coefficients and norms).
+void slab_sum(dgh_ctx *c, double *dev, int count) {
+    if (c->slabbed()) c->slab.comm->allreduce(dev, count, 0, c->stream);
+}
+// The interior cells of a slab (all cells otherwise): [first, first + count).
+void interior_cells(const dgh_ctx *c, int &first, int &count) {
+    first = c->slabbed() ? c->g.nx : 0;
+    count = c->slabbed() ? c->g.nx * c->slab.rows : c->cells;
 }
 
 // The dynamic shared-memory cap of a kernel is process-wide state that every context shares (and
@@ -863,6 +928,7 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
         c->launched();
         return;
     }
+    slab_halo(c, v);
     launch_trace(c, v, c->traces2, false);
     DGH_DISPATCH_N(c->n, {
         using T = Team<N>;
@@ -875,9 +941,11 @@ void dg_apply(dgh_ctx *c, const double *v, double *out) {
         }
     });
     c->launched();
+    slab_zero_ghosts(c, out);
 }
 void dg_apply_t(dgh_ctx *c, const double *w, double *out) {
     need(!c->d1(), "The adjoint J^T w is built for the 2D operator only");
+    need(!c->slabbed(), "J^T w is not built for slab contexts");
     need(c->linearised, "Refresh the volume Jacobian before applying it");
     launch_trace(c, w, c->traces2, false);
     DGH_DISPATCH_N(c->n, {
@@ -953,6 +1021,7 @@ void mdot(dgh_ctx *c, const double *V, size_t ld, int K, const double *x, const 
 #undef C_
     k_reduce<<<K, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, out);
     c->launched(2);
+    slab_sum(c, out, K);
 }
 void maxpy_dot(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, double *x, const double *W, long long n,
                double *out) {
@@ -961,6 +1030,7 @@ void maxpy_dot(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, d
 #undef C_
     k_reduce<<<K, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, out);
     c->launched(2);
+    slab_sum(c, out, K);
 }
 void maxpy_norm(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, double *x, const double *W, long long n,
                 double *out) {
@@ -969,6 +1039,7 @@ void maxpy_norm(dgh_ctx *c, const double *V, size_t ld, int K, const double *h, 
 #undef C_
     k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, out);
     c->launched(2);
+    slab_sum(c, out, 1);
 }
 void lincomb(dgh_ctx *c, const double *V, size_t ld, int K, const double *coef, double *out, long long n) {
 #define C_(NV) lincomb_t<NV>(c, V, ld, K, coef, out, n)
@@ -997,6 +1068,7 @@ struct GmresCall {
 int gmres_start(dgh_ctx *c, const GmresCall &g, cudaGraphConditionalHandle h, int use_h) {
     k_wnorm2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(g.r, g.W, 0, g.n, c->partial);
     k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, c->red + 2 * KR_MAXK);
+    slab_sum(c, c->red + 2 * KR_MAXK, 1);
     k_scale_div<<<c->red_grid, KR_THREADS, 0, c->stream>>>(g.r, c->red + 2 * KR_MAXK, 1, c->V, g.n);
     k_gmres_init<<<1, 32, 0, c->stream>>>(c->gdev, c->red + 2 * KR_MAXK, h, use_h);
     c->launched(4);
@@ -1033,6 +1105,7 @@ int gmres_finish(dgh_ctx *c, const GmresCall &g) {
     k_wnorm2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(g.r, g.W, 0, g.n, c->partial);
     k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, &c->gdev->rnorm2);
     c->launched(2);
+    slab_sum(c, &c->gdev->rnorm2, 1);
     return (int)(c->launches - before);
 }
 // Captures one restart cycle of operator op: the start and finish segments on the context's
@@ -1112,7 +1185,9 @@ void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double t
     g.restart = (int)std::min<long long>(g.n, c->cfg.restart);
     g.r = c->gres[op];
     const long long n = g.n;
+    need(!c->slabbed() || op == DGH_OP_DG, "Slab contexts solve the DG operator only");
     ck(cudaMemcpyAsync(c->g_rhs, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+    slab_zero_ghosts(c, c->g_rhs);  // the Krylov vectors of a slab keep zero ghost rows
     ck(cudaMemsetAsync(c->g_x, 0, n * sizeof(double), c->stream), "memset");
     ck(cudaMemcpyAsync(g.r, c->g_rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
     const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(c->g_rhs, g.W, false, n)));
@@ -1742,7 +1817,57 @@ void dgh_config_default(dgh_config *c) {
 
 static thread_local std::string g_create_error;
 
-int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
+}  // extern "C"
+
+namespace {
+// The mesh rows of a slab context (dgh_ctx_create_slab), and of every other context none.
+struct SlabInit {
+    dgh_comm *comm = nullptr;
+    int row0 = 0, rows = 0, ny = 0;
+};
+int create_ctx(const dgh_config *cfg, const SlabInit *slab, dgh_ctx **out);
+}  // namespace
+
+extern "C" {
+int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) { return create_ctx(cfg, nullptr, out); }
+
+int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out) {
+    if (!cfg || !out) return DGH_ERR_INVALID;
+    *out = nullptr;
+    const char *why = nullptr;
+    if (!comm) why = "null communicator";
+    else if (cfg->dim != 2 || cfg->method != DGH_METHOD_DG) why = "Slab decomposition is built for the 2D DG method";
+    else if (cfg->quadrature != 0 && cfg->quadrature != cfg->degree + 1)
+        why = "Slab decomposition is built for the collocated volume rule";
+    else if (cfg->preconditioner != 0) why = "Slab decomposition is built for the block-Jacobi preconditioner";
+    else if (cfg->ny < 3 || comm->size > cfg->ny) why = "Slab decomposition needs at least one mesh row per rank";
+    if (why) {
+        g_create_error = why;
+        return DGH_ERR_INVALID;
+    }
+    SlabInit si;
+    si.comm = comm;
+    si.ny = cfg->ny;
+    dgh_slab::rows_of(cfg->ny, comm->size, comm->rank, si.row0, si.rows);
+    dgh_config local = *cfg;
+    local.ny = si.rows + 2;  // the slab's rows between its two ghost rows
+    return create_ctx(&local, &si, out);
+}
+
+int dgh_slab_info(const dgh_ctx *c, int64_t out[6]) {
+    if (!c || !out || !c->slabbed()) return DGH_ERR_INVALID;
+    out[0] = c->slab.row0;
+    out[1] = c->slab.rows;
+    out[2] = c->slab.comm->rank;
+    out[3] = c->slab.comm->size;
+    out[4] = c->slab.row_len;
+    out[5] = (int64_t)c->slab.rows * c->slab.row_len;
+    return DGH_OK;
+}
+}  // extern "C"
+
+namespace {
+int create_ctx(const dgh_config *cfg, const SlabInit *slab, dgh_ctx **out) {
     if (!cfg || !out) return DGH_ERR_INVALID;
     *out = nullptr;
     dgh_ctx *c = new dgh_ctx;
@@ -1814,8 +1939,15 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
         c->g.ny = k.ny;
         c->g.cells = c->cells;
         c->g.hx = c->cs.lx / k.nx;
-        c->g.hy = c->cs.ly / k.ny;
+        c->g.hy = c->cs.ly / (slab ? slab->ny : k.ny);
         c->g.gamma = 3.;
+        if (slab) {
+            c->slab.comm = slab->comm;
+            c->slab.row0 = slab->row0;
+            c->slab.rows = slab->rows;
+            c->slab.ny = slab->ny;
+            c->slab.row_len = (long long)k.nx * NVAR * c->n * c->n;
+        }
         // nodal_basis.hpp:34-65
         std::vector<double> x, w;
         gauss_rule(c->n, x, w);
@@ -1972,6 +2104,7 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
             c->lu_tri = c->alloc<double>((size_t)c->lu_grid * P * LL_TRI);
         }
         if (c->has_dg() && c->ilu2d()) ilu2_build(c);
+        if (c->slabbed()) c->slab.buf = c->alloc<double>(16);
         c->sync();
     });
     if (rc != DGH_OK) {
@@ -1982,6 +2115,9 @@ int dgh_ctx_create(const dgh_config *cfg, dgh_ctx **out) {
     *out = c;
     return DGH_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int dgh_ctx_destroy(dgh_ctx *c) {
     if (!c) return DGH_OK;
@@ -2086,10 +2222,17 @@ int dgh_initial(dgh_ctx *c, double *u) {
                 k1_initial<N><<<grid1(c->cells, 64), 64, 0, c->stream>>>(u, c->rule, c->b1, c->g1, c->cs, c->status);
             });
         } else {
-            DGH_DISPATCH_N(c->n, { k_initial<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, c->status); });
+            // a slab projects its interior cells, at their global rows, then fills its ghost rows
+            int first = 0, count = 0;
+            interior_cells(c, first, count);
+            Grid gi = c->g;
+            gi.row0 = c->slabbed() ? c->slab.row0 : 0;
+            double *ui = u + (size_t)first * c->m;
+            DGH_DISPATCH_N(c->n, { k_initial<N><<<count, 256, 0, c->stream>>>(ui, c->rule, c->basis, gi, c->cs, c->status); });
         }
         c->launched();
         c->check_status();
+        slab_halo(c, u);
         // initial_and_error.cpp:53 — the projected state must be admissible
         const int one = 1;
         std::memcpy(c->pinned, &one, sizeof(int));
@@ -2099,6 +2242,11 @@ int dgh_initial(dgh_ctx *c, double *u) {
         c->sync();
         int ok = 0;
         std::memcpy(&ok, c->pinned, sizeof(int));
+        if (c->slabbed()) {
+            double bad = ok ? 0. : 1.;
+            c->slab_reduce(&bad, 1, 1);
+            ok = bad > 0 ? 0 : 1;
+        }
         if (!ok) fail(DGH_ERR_STATE, "Invalid projected initial state");
     });
 }
@@ -2106,6 +2254,7 @@ int dgh_initial(dgh_ctx *c, double *u) {
 int dgh_freeze(dgh_ctx *c, const double *u, double *rate) {
     return guard(c, [&] {
         need(u && rate, "null argument");
+        slab_halo(c, u);
         ck(cudaMemcpyAsync(c->old, u, c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
         launch_trace(c, u, c->traces, false);
         if (c->d1()) {
@@ -2127,6 +2276,8 @@ int dgh_freeze(dgh_ctx *c, const double *u, double *rate) {
             c->linearised = c->dg_factored = c->condensed = c->face_factored = false;
             return;
         }
+        int first = 0, count = 0;  // the rate of a slab is the maximum over its interior cells
+        interior_cells(c, first, count);
         DGH_DISPATCH_N(c->n, {
             const int tot = 2 * c->cells * N;
             k_speeds<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, c->g, c->cfg.safety, c->status);
@@ -2134,17 +2285,19 @@ int dgh_freeze(dgh_ctx *c, const double *u, double *rate) {
             if (c->overint())
                 k_rate_q<N><<<std::min(c->cells, c->sms * 4), Q_THREADS, 0, c->stream>>>(u, c->speeds, c->bq, c->g, c->partial, c->status);
             else
-                k_rate<N><<<c->team_blocks(T::CPB), T::THREADS, 0, c->stream>>>(u, c->speeds, c->g, c->partial, c->status);
+                k_rate<N><<<(count + T::CPB - 1) / T::CPB, T::THREADS, 0, c->stream>>>(u, c->speeds, c->g, c->partial,
+                                                                                     c->status, first, first + count);
         });
         c->launched(2);
         c->check_status();
         DGH_DISPATCH_N(c->n, {
-            const int nb = c->overint() ? std::min(c->cells, c->sms * 4) : c->team_blocks(Team<N>::CPB);
+            const int nb = c->overint() ? std::min(c->cells, c->sms * 4) : (count + Team<N>::CPB - 1) / Team<N>::CPB;
             std::vector<double> part(nb);
             ck(cudaMemcpyAsync(part.data(), c->partial, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
             c->sync();
             double r = 0;
             for (double p : part) r = std::max(r, p);
+            c->slab_reduce(&r, 1, 1);
             *rate = r;
         });
         c->frozen = true;
@@ -2168,6 +2321,7 @@ int dgh_residual(dgh_ctx *c, const double *u, double *r) {
         need(u && r, "null argument");
         need(c->frozen, "Freeze the wave speeds before evaluating the residual");
         Timed tm(c, DGH_TIMER_RESIDUAL);
+        slab_halo(c, u);
         launch_trace(c, u, c->traces, false);
         if (c->d1()) {
             DGH_DISPATCH_N(c->n, {
@@ -2188,12 +2342,14 @@ int dgh_residual(dgh_ctx *c, const double *u, double *r) {
             }
         });
         c->launched();
+        slab_zero_ghosts(c, r);
     });
 }
 
 int dgh_admissible(dgh_ctx *c, const double *u, int *okp) {
     return guard(c, [&] {
         need(u && okp, "null argument");
+        slab_halo(c, u);  // ghost cells are the neighbours' cells: checking them changes nothing
         const int one = 1;
         std::memcpy(c->pinned, &one, sizeof(int));
         ck(cudaMemcpyAsync(c->ok, c->pinned, sizeof(int), cudaMemcpyHostToDevice, c->stream), "copy");
@@ -2201,6 +2357,11 @@ int dgh_admissible(dgh_ctx *c, const double *u, int *okp) {
         ck(cudaMemcpyAsync(c->pinned, c->ok, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "copy");
         c->sync();
         std::memcpy(okp, c->pinned, sizeof(int));
+        if (c->slabbed()) {  // admissible on every slab
+            double bad = *okp ? 0. : 1.;
+            c->slab_reduce(&bad, 1, 1);
+            *okp = bad > 0 ? 0 : 1;
+        }
     });
 }
 
@@ -2242,9 +2403,12 @@ int dgh_integral(dgh_ctx *c, const double *u, double out[4]) {
         std::vector<double> part((size_t)c->cells * 4);
         ck(cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
         c->sync();
+        int first = 0, count = 0;
+        interior_cells(c, first, count);
         for (int v = 0; v < 4; ++v) out[v] = 0;
-        for (int cell = 0; cell < c->cells; ++cell)
+        for (int cell = first; cell < first + count; ++cell)
             for (int v = 0; v < 4; ++v) out[v] += part[(size_t)cell * 4 + v];
+        c->slab_reduce(out, 4, 0);
     });
 }
 
@@ -2256,18 +2420,25 @@ int dgh_l2_error(dgh_ctx *c, const double *u, double time, double out[4]) {
                                                                               c->status);
             });
         } else {
+            int first = 0, count = 0;  // a slab: its interior cells at their global rows
+            interior_cells(c, first, count);
+            Grid gi = c->g;
+            gi.row0 = c->slabbed() ? c->slab.row0 : 0;
             DGH_DISPATCH_N(c->n, {
-                k_l2_error<N><<<c->cells, 256, 0, c->stream>>>(u, c->rule, c->basis, c->g, c->cs, time, c->partial, c->status);
+                k_l2_error<N><<<count, 256, 0, c->stream>>>(u + (size_t)first * c->m, c->rule, c->basis, gi, c->cs, time,
+                                                            c->partial, c->status);
             });
         }
         c->launched();
         c->check_status();
-        std::vector<double> part((size_t)c->cells * 4);
+        const int cells = c->slabbed() ? c->g.nx * c->slab.rows : c->cells;
+        std::vector<double> part((size_t)cells * 4);
         ck(cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
         c->sync();
         for (int v = 0; v < 4; ++v) out[v] = 0;
-        for (int cell = 0; cell < c->cells; ++cell)
+        for (int cell = 0; cell < cells; ++cell)
             for (int v = 0; v < 4; ++v) out[v] += part[(size_t)cell * 4 + v];
+        c->slab_reduce(out, 4, 0);
         for (int v = 0; v < 4; ++v) out[v] = std::sqrt(out[v]);
     });
 }
@@ -2296,6 +2467,7 @@ int dgh_mass_axpby(dgh_ctx *c, double a, const double *x, double b, const double
 int dgh_rho2(dgh_ctx *c, const double *u, double *value, double *grad) {
     return guard(c, [&] {
         need(!c->d1(), "The adjoint objective is built for the 2D problem only");
+        need(!c->slabbed(), "The adjoint objective is not built for slab contexts");
         k_rho2<<<c->red_grid, KR_THREADS, 0, c->stream>>>(u, c->mass, c->P, c->N, grad, c->partial);
         k_reduce<<<1, KR_THREADS, 0, c->stream>>>(c->partial, c->red_grid, c->red);
         c->launched(2);
@@ -2317,6 +2489,7 @@ namespace {
 void linearise(dgh_ctx *c, const double *u) {
     need(c->frozen, "Freeze the wave speeds before refreshing the Jacobian");
     need(c->step_size > 0, "Set the time step before refreshing the Jacobian");
+    slab_halo(c, u);
     launch_trace(c, u, c->traces, false);
     if (c->d1()) {
         DGH_DISPATCH_N(c->n, {
@@ -2627,9 +2800,22 @@ template <class F> int tuned_variant(dgh_ctx *c, int kind, F &&time_both, double
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) return it->second;
     }
-    const int v = tune_pick(c, time_both, ms_out);
-    std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tune_cache[key] = v;
+    int v = tune_pick(c, time_both, ms_out);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[key] = v;
+    }
+    return v;
+}
+// The same, agreed over the ranks of a slab context (the larger variant wins), so that every
+// rank factors alike and takes the same collective steps afterwards.
+template <class F> int tuned_variant_all(dgh_ctx *c, int kind, F &&time_both, double *ms_out) {
+    int v = tuned_variant(c, kind, time_both, ms_out);
+    if (c->slabbed() && c->cfg.autotune) {
+        double d = v;
+        c->slab_reduce(&d, 1, 1);
+        v = (int)d;
+    }
     return v;
 }
 }  // namespace
@@ -2709,14 +2895,14 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             if (c->dg_variant < 0 && c->half16()) c->dg_variant = 0;  // one factorisation form
             if (c->dg_variant < 0) {
                 const int sample = std::min(c->cells, std::max(c->lu_grid, 1) * 4);
-                c->dg_variant = tuned_variant(c, 0, [&](int v) { dg_factor(c, v, 0, sample); }, c->tune_ms);
+                c->dg_variant = tuned_variant_all(c, 0, [&](int v) { dg_factor(c, v, 0, sample); }, c->tune_ms);
                 c->check_status();
             }
             if (c->fused_ctas < 0) {  // the fused path's residency (kind 4): 1 or 2 CTAs per SM
                 const bool fused = c->mixed() && (c->half16() || c->dg_variant == 0) && !c->overint();
                 if (fused) {
                     const int sample = std::min(c->cells, std::max(c->lu_grid, 1) * 4);
-                    const int v = tuned_variant(c, 4, [&](int k) {
+                    const int v = tuned_variant_all(c, 4, [&](int k) {
                         c->fused_ctas = k + 1;
                         dg_factor(c, c->dg_variant, 0, sample);
                     }, c->fused_ms);
@@ -2731,7 +2917,7 @@ int dgh_block_jacobi_refresh(dgh_ctx *c, int op) {
             c->dg_factored = true;
             if (c->solve_shape < 0) {  // timed on a zero right-hand side (the same loads and flops)
                 ck(cudaMemsetAsync(c->gw, 0, (size_t)c->N * sizeof(double), c->stream), "cudaMemsetAsync");
-                c->solve_shape = tuned_variant(c, 3, [&](int v) { dg_block_solve(c, v, c->gw, c->gz); }, c->solve_ms);
+                c->solve_shape = tuned_variant_all(c, 3, [&](int v) { dg_block_solve(c, v, c->gw, c->gz); }, c->solve_ms);
             }
         } else {
             need(c->face_pool, "context has no HDG operator");
@@ -2959,7 +3145,10 @@ int dgh_autotune_report(const dgh_ctx *c, double out[6]) {
     return DGH_OK;
 }
 int dgh_gmres_graph_enable(dgh_ctx *c, int on) {
-    return guard(c, [&] { c->use_graph = on != 0; });
+    return guard(c, [&] {
+        need(!on || !c->slabbed(), "Slab contexts launch their GMRES cycles step by step");
+        c->use_graph = on != 0;
+    });
 }
 const double *dgh_gmres_residual(dgh_ctx *c, int op) {
     if (!c || op < 0 || op > 2) return nullptr;
@@ -3175,6 +3364,7 @@ int dgh_lockstep_create_op(dgh_ctx *const *members, int count, int op, dgh_locks
         if (hdg && !c->has_hdg()) return reject(i, "the context has no HDG operator");
         if (c->overint()) return reject(i, "lockstep members use the collocated volume rule");
         if (c->ilu()) return reject(i, "lockstep members use block Jacobi");
+        if (c->slabbed()) return reject(i, "slab contexts solve on their own");
         if (c->ls) return reject(i, "the context is already in a lockstep group");
         for (int k = 0; k < i; ++k)
             if (members[k] == c) return reject(i, "the context is listed twice");

@@ -88,13 +88,13 @@ __global__ void k_speeds(const double *__restrict__ traces, double *__restrict__
 template <int N>
 __global__ void __launch_bounds__(Team<N>::THREADS)
 k_rate(const double *__restrict__ u, const double *__restrict__ speeds, Grid g, double *__restrict__ partial,
-       int *status) {
+       int *status, int first, int last) {
     using T = Team<N>;
     __shared__ double sa[T::THREADS], sb[T::THREADS];
     const int sub = threadIdx.x / T::TPC, lt = threadIdx.x % T::TPC;
-    const int cell = blockIdx.x * T::CPB + sub;
+    const int cell = first + blockIdx.x * T::CPB + sub;  // cells [first, last)
     double ax = 0, ay = 0;
-    if (cell < g.cells) {
+    if (cell < last) {
         for (int k = lt; k < NFACES * N; k += T::TPC) {
             const int side = k / N, q = k % N;
             const int face = face_of(g, cell, side);
@@ -117,7 +117,7 @@ k_rate(const double *__restrict__ u, const double *__restrict__ speeds, Grid g, 
     if (threadIdx.x == 0) {
         double best = 0;
         for (int c = 0; c < T::CPB; ++c) {
-            if (blockIdx.x * T::CPB + c >= g.cells) break;
+            if (first + blockIdx.x * T::CPB + c >= last) break;
             double mx = 0, my = 0;
             for (int t = 0; t < T::TPC; ++t) {
                 mx = fmax(mx, sa[c * T::TPC + t]);

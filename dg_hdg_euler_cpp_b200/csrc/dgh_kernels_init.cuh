@@ -58,7 +58,7 @@ k_initial(double *__restrict__ u, const ErrorRule *__restrict__ er, Basis1D b, G
     __shared__ double U[NVAR * P];
     __shared__ double chk[(2 * P + MAXQ * MAXQ + NFACES * N) * NVAR];
     __shared__ double mean[NVAR];
-    const int cell = blockIdx.x, cx = cell % g.nx, cy = cell / g.nx;
+    const int cell = blockIdx.x, cx = cell % g.nx, cy = cell / g.nx + g.row0;
     for (int k = threadIdx.x; k < Q * Q; k += blockDim.x) {
         const int i = k % Q, j = k / Q;
         double s[4];
@@ -154,7 +154,7 @@ k_l2_error(const double *__restrict__ u, const ErrorRule *__restrict__ er, Basis
     const int Q = er->Q;
     __shared__ double U[NVAR * P];
     __shared__ double red[4][256];
-    const int cell = blockIdx.x, cx = cell % g.nx, cy = cell / g.nx;
+    const int cell = blockIdx.x, cx = cell % g.nx, cy = cell / g.nx + g.row0;
     for (int k = threadIdx.x; k < NVAR * P; k += blockDim.x) U[k] = u[(size_t)cell * NVAR * P + k];
     __syncthreads();
     double acc[4] = {0, 0, 0, 0};

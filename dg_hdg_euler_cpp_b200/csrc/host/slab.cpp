@@ -1,0 +1,334 @@
+// Slab communicators (slab.hpp): the in-process group of ranks and the NCCL communicator, and
+// their C ABI (dgh_comm_*, dgh_slab_rows in dgh_gpu.h).
+#include "slab.hpp"
+
+#include "dgh_gpu.h"
+
+#include <dlfcn.h>
+#include <nccl.h>
+
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace {
+thread_local std::string g_comm_error;
+
+void cuda_ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw dgh_comm_failure(std::string(what) + ": " + cudaGetErrorString(e));
+}
+double larger(double a, double b) { return (b > a || std::isnan(b)) ? b : a; }
+
+// Copies one row between slab vectors that may live on different devices.
+void copy_row(double *dst, int dst_dev, const double *src, int src_dev, size_t bytes, cudaStream_t st) {
+    if (dst_dev == src_dev) cuda_ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st), "halo copy");
+    else cuda_ck(cudaMemcpyPeerAsync(dst, dst_dev, src, src_dev, bytes, st), "halo peer copy");
+}
+
+// ---- in-process group ------------------------------------------------------------------------
+// The ranks of one group share this state.  A collective is two host barriers: every rank
+// publishes its operand (values read back to the host, or a device pointer after synchronising
+// its stream), waits for all, computes or copies its result, and waits again before the slots
+// may be reused.  Reductions run on the host in rank order, so every rank gets the same bits.
+struct LocalGroup {
+    int size = 1;
+    std::chrono::milliseconds timeout{60000};
+    std::mutex mu;
+    std::condition_variable cv;
+    int arrived = 0;
+    unsigned long long generation = 0;
+    bool failed = false;
+    std::string why;
+    std::vector<std::vector<double>> vals;
+    std::vector<double *> vec;
+    std::vector<int> rows, device;
+    std::vector<long long> row_len;
+
+    void barrier(int rank) {
+        std::unique_lock<std::mutex> lk(mu);
+        if (failed) throw dgh_comm_failure("slab group failed: " + why);
+        const unsigned long long gen = generation;
+        if (++arrived == size) {
+            arrived = 0;
+            ++generation;
+            cv.notify_all();
+            return;
+        }
+        if (!cv.wait_for(lk, timeout, [&] { return generation != gen || failed; })) {
+            failed = true;
+            why = "rank " + std::to_string(rank) + " waited " + std::to_string(timeout.count()) +
+                  " ms in a collective that a peer did not enter";
+            cv.notify_all();
+        }
+        if (generation == gen) throw dgh_comm_failure("slab group failed: " + why);
+    }
+    void fail(const std::string &w) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!failed) {
+            failed = true;
+            why = w;
+        }
+        cv.notify_all();
+    }
+};
+
+struct LocalComm final : dgh_comm {
+    std::shared_ptr<LocalGroup> g;
+    LocalComm(std::shared_ptr<LocalGroup> group, int r) : g(std::move(group)) {
+        rank = r;
+        size = g->size;
+    }
+    const char *kind() const override { return "local"; }
+    void allreduce(double *dev, int count, int op, cudaStream_t st) override {
+        if (size == 1) return;
+        auto &mine = g->vals[rank];
+        mine.assign(count, 0.);
+        cuda_ck(cudaMemcpyAsync(mine.data(), dev, count * sizeof(double), cudaMemcpyDeviceToHost, st), "collective read");
+        cuda_ck(cudaStreamSynchronize(st), "collective read");
+        g->barrier(rank);
+        std::vector<double> res(g->vals[0]);
+        bool same = true;
+        for (int r = 0; r < size; ++r) same = same && (int)g->vals[r].size() == count;
+        if (same)
+            for (int r = 1; r < size; ++r)
+                for (int i = 0; i < count; ++i) res[i] = op == 0 ? res[i] + g->vals[r][i] : larger(res[i], g->vals[r][i]);
+        g->barrier(rank);
+        if (!same) {
+            fail("ranks entered a collective with different counts");
+            throw dgh_comm_failure("slab ranks entered a collective with different counts");
+        }
+        cuda_ck(cudaMemcpyAsync(dev, res.data(), count * sizeof(double), cudaMemcpyHostToDevice, st), "collective write");
+        cuda_ck(cudaStreamSynchronize(st), "collective write");
+    }
+    void halo(double *v, long long row_len, int rows, cudaStream_t st) override {
+        const size_t bytes = (size_t)row_len * sizeof(double);
+        int dev = 0;
+        cuda_ck(cudaGetDevice(&dev), "cudaGetDevice");
+        if (size == 1) {  // the periodic wrap inside one slab
+            copy_row(v, dev, v + (size_t)rows * row_len, dev, bytes, st);
+            copy_row(v + (size_t)(rows + 1) * row_len, dev, v + row_len, dev, bytes, st);
+            return;
+        }
+        cuda_ck(cudaStreamSynchronize(st), "halo");
+        g->vec[rank] = v;
+        g->rows[rank] = rows;
+        g->device[rank] = dev;
+        g->row_len[rank] = row_len;
+        g->barrier(rank);
+        const int below = (rank + size - 1) % size, above = (rank + 1) % size;
+        bool same = g->row_len[below] == row_len && g->row_len[above] == row_len;
+        if (same) {
+            copy_row(v, dev, g->vec[below] + (size_t)g->rows[below] * row_len, g->device[below], bytes, st);
+            copy_row(v + (size_t)(rows + 1) * row_len, dev, g->vec[above] + row_len, g->device[above], bytes, st);
+            cuda_ck(cudaStreamSynchronize(st), "halo");
+        }
+        g->barrier(rank);
+        if (!same) {
+            fail("neighbouring slabs have different row lengths");
+            throw dgh_comm_failure("neighbouring slabs have different row lengths");
+        }
+    }
+    void fail(const std::string &why) noexcept override {
+        try {
+            g->fail("rank " + std::to_string(rank) + ": " + why);
+        } catch (...) {
+        }
+    }
+};
+
+// ---- NCCL --------------------------------------------------------------------------------------
+// libnccl is resolved when the first NCCL communicator is made: the copy already loaded into the
+// process (by torch, for instance) if there is one, else DGH_NCCL_LIBRARY, else libnccl.so.2.
+struct NcclApi {
+    std::string why;
+    ncclResult_t (*get_unique_id)(ncclUniqueId *) = nullptr;
+    ncclResult_t (*init_rank)(ncclComm_t *, int, ncclUniqueId, int) = nullptr;
+    ncclResult_t (*destroy)(ncclComm_t) = nullptr;
+    ncclResult_t (*abort)(ncclComm_t) = nullptr;
+    ncclResult_t (*allreduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t) = nullptr;
+    ncclResult_t (*send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+    ncclResult_t (*recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+    ncclResult_t (*group_start)() = nullptr;
+    ncclResult_t (*group_end)() = nullptr;
+    const char *(*error_string)(ncclResult_t) = nullptr;
+    bool ok() const { return why.empty(); }
+};
+template <class F> void resolve(void *h, const char *name, F &f, std::string &why) {
+    f = reinterpret_cast<F>(dlsym(h, name));
+    if (!f && why.empty()) why = std::string("libnccl lacks ") + name;
+}
+NcclApi load_nccl() {
+    NcclApi a;
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (!h) {
+        if (const char *path = std::getenv("DGH_NCCL_LIBRARY")) h = dlopen(path, RTLD_NOW | RTLD_GLOBAL);
+    }
+    if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) {
+        const char *e = dlerror();
+        a.why = std::string("cannot load libnccl: ") + (e ? e : "not found");
+        return a;
+    }
+    resolve(h, "ncclGetUniqueId", a.get_unique_id, a.why);
+    resolve(h, "ncclCommInitRank", a.init_rank, a.why);
+    resolve(h, "ncclCommDestroy", a.destroy, a.why);
+    resolve(h, "ncclCommAbort", a.abort, a.why);
+    resolve(h, "ncclAllReduce", a.allreduce, a.why);
+    resolve(h, "ncclSend", a.send, a.why);
+    resolve(h, "ncclRecv", a.recv, a.why);
+    resolve(h, "ncclGroupStart", a.group_start, a.why);
+    resolve(h, "ncclGroupEnd", a.group_end, a.why);
+    resolve(h, "ncclGetErrorString", a.error_string, a.why);
+    return a;
+}
+NcclApi &nccl() {
+    static NcclApi api = load_nccl();
+    return api;
+}
+void nccl_ck(ncclResult_t r, const char *what) {
+    if (r != ncclSuccess) throw dgh_comm_failure(std::string(what) + ": " + nccl().error_string(r));
+}
+
+struct NcclComm final : dgh_comm {
+    ncclComm_t comm = nullptr;
+    int device = 0;
+    bool failed = false;
+    std::string why;
+    const char *kind() const override { return "nccl"; }
+    void check() const {
+        if (failed) throw dgh_comm_failure("slab communicator failed: " + why);
+    }
+    void allreduce(double *dev, int count, int op, cudaStream_t st) override {
+        check();
+        nccl_ck(nccl().allreduce(dev, dev, (size_t)count, ncclDouble, op == 0 ? ncclSum : ncclMax, comm, st),
+                "ncclAllReduce");
+    }
+    void halo(double *v, long long row_len, int rows, cudaStream_t st) override {
+        check();
+        const size_t n = (size_t)row_len;
+        double *bottom = v + n, *top = v + (size_t)rows * n;               // interior rows sent
+        double *ghost_below = v, *ghost_above = v + (size_t)(rows + 1) * n;  // ghost rows received
+        if (size == 1) {
+            copy_row(ghost_below, device, top, device, n * sizeof(double), st);
+            copy_row(ghost_above, device, bottom, device, n * sizeof(double), st);
+            return;
+        }
+        // With two ranks both neighbours are the same peer, and NCCL matches that peer's
+        // messages in posting order: each rank sends bottom then top, and receives into the
+        // ghost above (the peer's bottom row) then the ghost below (the peer's top row).
+        const int below = (rank + size - 1) % size, above = (rank + 1) % size;
+        nccl_ck(nccl().group_start(), "ncclGroupStart");
+        nccl_ck(nccl().send(bottom, n, ncclDouble, below, comm, st), "ncclSend");
+        nccl_ck(nccl().send(top, n, ncclDouble, above, comm, st), "ncclSend");
+        nccl_ck(nccl().recv(ghost_above, n, ncclDouble, above, comm, st), "ncclRecv");
+        nccl_ck(nccl().recv(ghost_below, n, ncclDouble, below, comm, st), "ncclRecv");
+        nccl_ck(nccl().group_end(), "ncclGroupEnd");
+    }
+    void fail(const std::string &w) noexcept override {
+        if (failed) return;
+        failed = true;
+        why = w;
+        if (comm) nccl().abort(comm);  // peers blocked on this rank see the communicator go away
+        comm = nullptr;
+    }
+    ~NcclComm() override {
+        if (comm) nccl().destroy(comm);
+    }
+};
+
+template <class F> int comm_guard(F &&f) {
+    g_comm_error.clear();
+    try {
+        f();
+        return DGH_OK;
+    } catch (const dgh_comm_failure &e) {
+        g_comm_error = e.what();
+        return DGH_ERR_COMM;
+    } catch (const std::exception &e) {
+        g_comm_error = e.what();
+        return DGH_ERR_COMM;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char *dgh_comm_error(void) { return g_comm_error.c_str(); }
+
+int dgh_slab_rows(int ny, int size, int rank, int out[4]) {
+    if (!out || size < 1 || rank < 0 || rank >= size || ny < size) return DGH_ERR_INVALID;
+    dgh_slab::rows_of(ny, size, rank, out[0], out[1]);
+    out[2] = (rank + size - 1) % size;
+    out[3] = (rank + 1) % size;
+    return DGH_OK;
+}
+
+int dgh_comm_local_create(int size, int timeout_ms, dgh_comm **ranks) {
+    return comm_guard([&] {
+        if (!ranks || size < 1 || timeout_ms < 1) throw dgh_comm_failure("invalid group size, timeout or output");
+        auto g = std::make_shared<LocalGroup>();
+        g->size = size;
+        g->timeout = std::chrono::milliseconds(timeout_ms);
+        g->vals.resize(size);
+        g->vec.assign(size, nullptr);
+        g->rows.assign(size, 0);
+        g->device.assign(size, 0);
+        g->row_len.assign(size, 0);
+        for (int r = 0; r < size; ++r) ranks[r] = new LocalComm(g, r);
+    });
+}
+
+int dgh_comm_nccl_unique_id(unsigned char id[128]) {
+    return comm_guard([&] {
+        if (!id) throw dgh_comm_failure("null output");
+        if (!nccl().ok()) throw dgh_comm_failure(nccl().why);
+        ncclUniqueId u;
+        nccl_ck(nccl().get_unique_id(&u), "ncclGetUniqueId");
+        static_assert(sizeof(u.internal) == 128, "NCCL unique id size");
+        std::memcpy(id, u.internal, 128);
+    });
+}
+
+int dgh_comm_nccl_create(const unsigned char id[128], int size, int rank, int device, dgh_comm **out) {
+    return comm_guard([&] {
+        if (!id || !out || size < 1 || rank < 0 || rank >= size) throw dgh_comm_failure("invalid rank, size or id");
+        *out = nullptr;
+        if (!nccl().ok()) throw dgh_comm_failure(nccl().why);
+        cuda_ck(cudaSetDevice(device), "cudaSetDevice");
+        ncclUniqueId u;
+        std::memcpy(u.internal, id, 128);
+        auto c = std::make_unique<NcclComm>();
+        c->rank = rank;
+        c->size = size;
+        c->device = device;
+        nccl_ck(nccl().init_rank(&c->comm, size, u, rank), "ncclCommInitRank");
+        *out = c.release();
+    });
+}
+
+int dgh_comm_info(const dgh_comm *comm, int out[3]) {
+    if (!comm || !out) return DGH_ERR_INVALID;
+    out[0] = comm->rank;
+    out[1] = comm->size;
+    out[2] = std::strcmp(comm->kind(), "nccl") == 0 ? 1 : 0;
+    return DGH_OK;
+}
+
+int dgh_comm_fail(dgh_comm *comm, const char *why) {
+    if (!comm) return DGH_ERR_INVALID;
+    comm->fail(why ? why : "failed by its host");
+    return DGH_OK;
+}
+
+int dgh_comm_destroy(dgh_comm *comm) {
+    delete comm;
+    return DGH_OK;
+}
+
+}  // extern "C"

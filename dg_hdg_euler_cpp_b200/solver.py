@@ -60,19 +60,30 @@ def _ptr(t) -> ctypes.c_void_p:
 class Solver:
     """One GPU context: the Problem plus the DG and/or HDG operators of one configuration.
     Solver(dim=1, cells=..., k=...) is the 1D problem of dg_hdg_1d (three variables per node,
-    NVAR values per face trace)."""
+    NVAR values per face trace).  Solver(comm=SlabComm, ...) is one rank's slab of the mesh
+    (dgh_ctx_create_slab): its vectors carry a ghost cell row below and above the slab's rows;
+    `slab` describes the slab and `interior(v)` is the view of a vector without its ghosts."""
 
-    def __init__(self, **kw):
+    def __init__(self, comm: "SlabComm | None" = None, **kw):
         import torch
 
         self.torch = torch
         self.lib = _lib.load()
         self.cfg = make_config(**kw)
         h = ctypes.c_void_p()
-        rc = self.lib.dgh_ctx_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if comm is None:
+            rc = self.lib.dgh_ctx_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        else:
+            rc = self.lib.dgh_ctx_create_slab(ctypes.byref(self.cfg), comm.h, ctypes.byref(h))
         if rc != 0:
             raise DGHError(rc, self.lib.dgh_last_error(None).decode())
         self.h = h
+        self.comm = comm  # the communicator outlives the context
+        self.slab = None
+        if comm is not None:
+            info = (ctypes.c_int64 * 6)()
+            self._rc(self.lib.dgh_slab_info(self.h, info))
+            self.slab = dict(zip(("row0", "rows", "rank", "size", "offset", "length"), (int(x) for x in info)))
         s = (ctypes.c_int64 * 8)()
         self._rc(self.lib.dgh_sizes(self.h, s))
         self.size, self.trace_size, self.block, self.cells, self.faces, self.n, self.local_trace, self.face_width = (
@@ -107,6 +118,12 @@ class Solver:
 
     def vec(self, n=None):
         return self.torch.zeros(self.size if n is None else n, dtype=self.torch.float64, device=self.device)
+
+    def interior(self, v):
+        """The slab's own rows of a volume vector (the whole vector outside a slab)."""
+        if self.slab is None:
+            return v
+        return v[self.slab["offset"]:self.slab["offset"] + self.slab["length"]]
 
     def tensor(self, a):
         return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=self.device)
@@ -502,6 +519,113 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ---- slab domain decomposition ------------------------------------------------------------------
+def slab_rows(ny: int, size: int, rank: int) -> tuple[int, int, int, int]:
+    """(first global row, rows, rank below, rank above) of rank `rank` (dgh_slab_rows)."""
+    lib = _lib.load()
+    out = (ctypes.c_int * 4)()
+    rc = lib.dgh_slab_rows(ny, size, rank, out)
+    if rc != 0:
+        raise DGHError(rc, f"no slab partition of {ny} rows over {size} ranks for rank {rank}")
+    return tuple(int(x) for x in out)
+
+
+class SlabComm:
+    """One rank's communicator of the slab decomposition (dgh_comm_*): NCCL across processes and
+    GPUs, or an in-process group whose ranks are host threads (several slabs on one GPU)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self.lib = _lib.load()
+        self.h = handle
+        info = (ctypes.c_int * 3)()
+        self.lib.dgh_comm_info(self.h, info)
+        self.rank, self.size = int(info[0]), int(info[1])
+        self.kind = "nccl" if info[2] == 1 else "local"
+
+    @staticmethod
+    def _check(rc: int):
+        if rc != 0:
+            raise DGHError(rc, _lib.load().dgh_comm_error().decode())
+
+    @classmethod
+    def local_group(cls, size: int, timeout_ms: int = 60000) -> list["SlabComm"]:
+        lib = _lib.load()
+        hs = (ctypes.c_void_p * size)()
+        cls._check(lib.dgh_comm_local_create(size, timeout_ms, hs))
+        return [cls(ctypes.c_void_p(h)) for h in hs]
+
+    @staticmethod
+    def nccl_unique_id() -> bytes:
+        buf = (ctypes.c_ubyte * 128)()
+        SlabComm._check(_lib.load().dgh_comm_nccl_unique_id(buf))
+        return bytes(buf)
+
+    @classmethod
+    def nccl(cls, unique_id: bytes, size: int, rank: int, device: int) -> "SlabComm":
+        buf = (ctypes.c_ubyte * 128).from_buffer_copy(unique_id)
+        h = ctypes.c_void_p()
+        cls._check(_lib.load().dgh_comm_nccl_create(buf, size, rank, device, ctypes.byref(h)))
+        return cls(h)
+
+    def fail(self, why: str = "failed by its host"):
+        self.lib.dgh_comm_fail(self.h, why.encode())
+
+    def close(self):
+        if self.h:
+            self.lib.dgh_comm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def share_unique_id(make_id=None, group=None) -> bytes:
+    """Rank 0's NCCL id, broadcast to every rank of the initialised torch.distributed group (any
+    backend)."""
+    import torch.distributed as dist
+
+    box = [(make_id or SlabComm.nccl_unique_id)() if dist.get_rank(group) == 0 else None]
+    dist.broadcast_object_list(box, src=0, group=group)
+    return box[0]
+
+
+def nccl_slab_comm(device: int, group=None) -> SlabComm:
+    """This process's NCCL slab communicator over the torch.distributed group (one rank per GPU)."""
+    import torch.distributed as dist
+
+    uid = share_unique_id(group=group)
+    return SlabComm.nccl(uid, dist.get_world_size(group), dist.get_rank(group), device)
+
+
+def run_ranks(comms: list[SlabComm], body) -> list:
+    """Runs body(rank, comm) for every rank of an in-process group, each on its own host thread;
+    returns the results in rank order.  A rank that raises fails the group (its peers then leave
+    their collectives with DGH_ERR_COMM instead of waiting), and the first error is re-raised."""
+    import threading
+
+    results, errors = [None] * len(comms), [None] * len(comms)
+
+    def run(r):
+        try:
+            results[r] = body(r, comms[r])
+        except BaseException as e:  # noqa: BLE001 — reported below, after every rank has ended
+            errors[r] = e
+            comms[r].fail(f"{type(e).__name__}: {e}")
+
+    threads = [threading.Thread(target=run, args=(r,)) for r in range(len(comms))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for e in errors:
+        if e is not None:
+            raise e
+    return results
 
 
 # ---- the uneven-batch workload: 16 members drawn from seeds 0-15 --------------------------------

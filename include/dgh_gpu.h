@@ -43,7 +43,8 @@ typedef enum dgh_status {
     DGH_ERR_GMRES_LIMIT = 5,  /* GMRES iteration limit reached (gmres.cpp:121)             */
     DGH_ERR_BREAKDOWN = 6,    /* GMRES Arnoldi breakdown (gmres.cpp:92)                    */
     DGH_ERR_STATE = 7,        /* invalid physical state (physics.cpp:108, discretization)  */
-    DGH_ERR_SOLVER = 8        /* Newton / line search / HDG acceptance failure             */
+    DGH_ERR_SOLVER = 8,       /* Newton / line search / HDG acceptance failure             */
+    DGH_ERR_COMM = 9          /* slab collective failed: a peer rank failed or timed out   */
 } dgh_status;
 
 enum { DGH_METHOD_DG = 0, DGH_METHOD_HDG = 1, DGH_METHOD_BOTH = 2 };
@@ -346,6 +347,52 @@ const char *dgh_lockstep_error(void);
 int dgh_lockstep_begin(dgh_lockstep *group, int expected);
 int dgh_lockstep_leave(dgh_lockstep *group, dgh_ctx *member);
 int dgh_lockstep_report(const dgh_lockstep *group, int64_t out[4]);
+
+/* ---- Slab domain decomposition (multi-GPU; the reference runs one process on one mesh) ---------
+ * One 2D DG problem split into slabs of whole cell rows, one rank per slab: rank r of `size`
+ * owns global rows [row0, row0 + rows) (dgh_slab_rows: ny = size * base + extra, the first
+ * `extra` ranks take base + 1 rows; out = {row0, rows, rank below, rank above}, periodic).
+ * A slab context (dgh_ctx_create_slab; cfg as for the whole mesh, cfg->ny the global row count)
+ * holds its rows plus one ghost row below and one above: every volume vector of it has
+ * (rows + 2) * nx cells in the usual cell-major layout, local row 0 and row rows+1 being the
+ * ghosts, so dgh_sizes()[0] = (rows + 2) * nx * 4 (k+1)^2 and dgh_slab_info gives the interior
+ * (its first double and its length).  The ghost rows of vectors passed in belong to the library:
+ * dgh_freeze, dgh_residual, dgh_admissible, dgh_dg_refresh, dgh_dg_apply and dgh_initial fill
+ * them from the neighbouring slabs (a halo exchange) before reading neighbours, and the
+ * residual and J*v outputs come back with zero ghost rows.  Norms, integrals, L2 errors,
+ * admissibility, the CFL rate, kernel status bits and the GMRES inner products are reduced over
+ * all ranks, so every rank takes the same decisions (Newton, line search, GMRES restarts) and
+ * receives the same scalars; every rank must make the same calls in the same order, each from
+ * its own host thread or process.  Interior results equal the single-domain ones: residual,
+ * J*v, frozen speeds and the CFL rate bitwise; norms and the Newton update to rounding of the
+ * reduction order.  Covered: method DG, collocated rule, block Jacobi, every precision, BE and
+ * DIRK3 (dgh_integrator_* on a slab context).  Not with slabs: HDG, over-integration, block
+ * ILU(0), J^T / the adjoint, lockstep groups and graph-replayed GMRES cycles (refused).
+ * Communicators (the communicator must outlive its contexts):
+ *  - dgh_comm_nccl_create: one rank per process and GPU over NCCL; rank 0 makes the id with
+ *    dgh_comm_nccl_unique_id and the host shares it (e.g. a torch.distributed broadcast).
+ *    libnccl is resolved at run time (the copy already loaded, else DGH_NCCL_LIBRARY, else
+ *    libnccl.so.2).
+ *  - dgh_comm_local_create: `size` ranks inside one process (ranks[r] for rank r), each driven
+ *    by its own host thread, on any devices (several slabs on one GPU included); collectives
+ *    synchronise the ranks' streams and meet at host barriers, and a rank that waits longer
+ *    than timeout_ms for its peers fails the group (DGH_ERR_COMM on every rank).
+ *  - dgh_comm_fail: marks the group failed (a host that caught an error on one rank releases
+ *    the others; a context failing with DGH_ERR_CUDA or DGH_ERR_COMM does this itself).
+ * dgh_comm_info: {rank, size, kind (0 local, 1 NCCL)}.  dgh_comm_error: the calling thread's
+ * last dgh_comm_* failure. */
+typedef struct dgh_comm dgh_comm;
+int dgh_slab_rows(int ny, int size, int rank, int out[4]);
+int dgh_comm_local_create(int size, int timeout_ms, dgh_comm **ranks);
+int dgh_comm_nccl_unique_id(unsigned char id[128]);
+int dgh_comm_nccl_create(const unsigned char id[128], int size, int rank, int device, dgh_comm **out);
+int dgh_comm_info(const dgh_comm *comm, int out[3]);
+int dgh_comm_fail(dgh_comm *comm, const char *why);
+int dgh_comm_destroy(dgh_comm *comm);
+const char *dgh_comm_error(void);
+int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out);
+/* {global first row, interior rows, rank, size, first interior double, interior doubles} */
+int dgh_slab_info(const dgh_ctx *ctx, int64_t out[6]);
 
 /* ---- Discrete adjoint of the DG time integration (no counterpart in the reference) -------------
  * Objective J = sum over nodes of M rho^2 at the end of `steps` fixed steps (dt = cfl / rate of

@@ -68,3 +68,50 @@ def test_noalloc_rejects_meshes_beyond_its_scratch():
     rc = lib.dgh_residual_noalloc(200, 200, 8, 0, ctypes.c_double(0.01), p, p, p, p, None, errbuf, len(errbuf))
     assert rc == 1
     assert b"too large" in errbuf.value and b"2097152" in errbuf.value
+
+
+def test_noalloc_residual_inside_cuda_graph_capture():
+    """The use the entry point exists for: after one warm call (which looks up the scratch
+    address), one call is captured into a CUDA graph on torch's capture stream; the graph is then
+    replayed on two states copied into the captured input buffer, and each replay must match
+    dgh_residual."""
+    import torch
+
+    from dg_hdg_euler_cpp_b200.solver import TESTCASES, Solver
+
+    nx, ny, k = 10, 8, 5
+    s = Solver(nx=nx, ny=ny, k=k, cfl=1.0, integrator="be", steps=1, method="dg", testcase="diagonal")
+    u0 = s.initial()
+    s.freeze(u0)
+    dt = 0.02
+    s.set_stage(u0, dt)
+    speeds = torch.as_tensor(s.speeds().reshape(-1).copy(), device=s.device)
+    errbuf = ctypes.create_string_buffer(256)
+    u_in = u0.clone()
+    r_out = torch.full_like(u0, float("nan"))
+
+    def call(stream):
+        return s.lib.dgh_residual_noalloc(nx, ny, k, TESTCASES["diagonal"], ctypes.c_double(dt),
+                                          ctypes.c_void_p(u_in.data_ptr()), ctypes.c_void_p(u0.data_ptr()),
+                                          ctypes.c_void_p(speeds.data_ptr()), ctypes.c_void_p(r_out.data_ptr()),
+                                          stream, errbuf, len(errbuf))
+
+    assert call(None) == 0, errbuf.value.decode()  # warm call before the capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.graph(g, stream=side):
+        rc = call(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, errbuf.value.decode()
+    states = [u0 + 1e-3 * s.tensor(direction(s.size)), u0 - 3e-3 * s.tensor(direction(s.size)[::-1].copy())]
+    for u in states:
+        u_in.copy_(u)
+        r_out.fill_(float("nan"))
+        g.replay()
+        torch.cuda.synchronize()
+        got = r_out.cpu().numpy()
+        ref = s.residual(u).cpu().numpy()
+        assert np.all(np.isfinite(got))
+        assert np.max(np.abs(got - ref)) <= RTOL * np.max(np.abs(ref))
+    del g
+    s.close()
