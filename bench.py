@@ -19,6 +19,12 @@ reduced form's speed-up, state error and Krylov change against FP64 at the top l
 repeats the headline forms' timed updates through the C ABI with host buffers
 (dgh_newton_update_host: state H2D, update, state D2H every step).
 
+Multi-GPU: by default N ranks solve N independent replicas ("scaling": "weak", value = N x the
+per-replica rate).  --slabs instead splits ONE mesh into N slabs of cell rows, one per GPU, with
+the ghost-row halo exchange and the reductions over NCCL ("scaling": "strong", DG forms only).
+On one GPU the breakdown's slab_nccl_one_rank entry runs the DG headline form as a one-rank
+NCCL slab against the whole-mesh context (the decomposition's own cost and its state).
+
 cpu_baseline and --impl reference time the reference algorithm's CPU implementation (the oracle
 restatement; the reference itself needs Eigen, which this image lacks) on the host cores:
 single-threaded (the reference is single-threaded by construction) and as P concurrent
@@ -85,6 +91,11 @@ def parse():
     p.add_argument("--stepped", action="store_true",
                    help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
+    p.add_argument("--slabs", action="store_true",
+                   help="strong scaling: the DG forms solve ONE mesh split into N slabs of cell rows (one per GPU, "
+                        "NCCL halo exchange and reductions) instead of N independent replicas")
+    p.add_argument("--no-slab-check", action="store_true",
+                   help="skip the one-rank NCCL slab run of the DG headline form (1 GPU)")
     return p.parse_args()
 
 
@@ -206,17 +217,20 @@ def protocol_units(k: int) -> list[int]:
 
 
 def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: bool, rank: int, local: int,
-               e2e: bool):
+               e2e: bool, comm=None):
+    """One configuration through its protocol units; with `comm` (a slab communicator) this rank
+    solves its slab of the mesh and `final` is the slab's interior."""
     from dg_hdg_euler_cpp_b200 import _lib
     from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
 
     K, W = args.steps, args.warmup
-    s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=4,
+    s = Solver(comm=comm, nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=4,
                method=method, precision=FORMS[precision][0], condense32=FORMS[precision][1],
                forcing=FORMS[precision][2], restart=args.restart,
                max_linear=1500, ntol=args.ltol, ltol=args.ltol,
                safety=1.1, device=local, autotune=1 if args.autotune else 0)
-    s.gmres_graph(not args.stepped)
+    graphs = not args.stepped and comm is None  # slab contexts launch their cycles step by step
+    s.gmres_graph(graphs)
     it = Integrator(s, method)
     lib = s.lib
     stream = torch.cuda.ExternalStream(s.stream(), device=s.device)
@@ -266,11 +280,13 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
     lib.dgh_timing_enable(s.h, 0)
     final = np.empty(s.size)
     lib.dgh_download(s.h, final.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(it.state_ptr()), s.size)
+    if comm is not None:
+        final = final[s.slab["offset"]:s.slab["offset"] + s.slab["length"]]
     # Inside the replayed cycle graphs the per-call timers see no launches: the per-kernel figures
     # (the roofline's average launch time) come from one more update, from the same stage start,
     # with the cycles launched step by step (the same kernels with the same arguments).
     kernel_timers = timers
-    if not args.stepped:
+    if graphs:
         s.gmres_graph(False)
         it.stage_begin(u0)
         lib.dgh_timing_enable(s.h, 1)
@@ -284,7 +300,7 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
         "krylov_update1": [r["krylov_iterations"] for r in firsts],
         "rms": [r["residual_physical_rms"] for r in rows], "damping": [r["damping"] for r in rows],
         "launches": launches, "timers_all_unit_updates": timers, "device_gb": s.device_bytes() / 1e9,
-        "clocks": sampler.summary() if sampler else None, "gmres_cycles": "stepped" if args.stepped else "cuda_graph",
+        "clocks": sampler.summary() if sampler else None, "gmres_cycles": "cuda_graph" if graphs else "stepped",
         "autotune": s.autotune_report(),
     }
     # dominant per-iteration kernel of this configuration
@@ -306,12 +322,14 @@ def run_config(args, method: str, precision: str, torch, pg, peaks, sampler_on: 
         out["roofline"] = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "bytes_per_launch": kb,
                            "avg_launch_ms": avg_ms, "launches": tk["launches"]}
-        if not args.stepped:
+        if graphs:
             out["roofline"]["measured_on"] = "protocol update 1, cycles launched step by step"
     else:
         out["roofline"] = None
-    if not args.stepped:
+    if graphs:
         out["kernel_timers_stepped_update"] = kernel_timers
+    if comm is not None:
+        out["slab"] = dict(s.slab, kind=comm.kind)
     if e2e:
         out["e2e"] = e2e_units(args, s, it, u0, torch, pg)
     it.close()
@@ -347,15 +365,15 @@ def e2e_units(args, s, it, u0, torch, pg) -> dict:
             "d2h_bytes_per_step": s.size * 8}
 
 
-def e2e_config(args, method: str, precision: str, torch, pg, local: int) -> dict:
+def e2e_config(args, method: str, precision: str, torch, pg, local: int, comm=None) -> dict:
     """e2e_units on a fresh context of one configuration (after one untimed protocol unit)."""
     from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
 
-    s = Solver(nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=4,
+    s = Solver(comm=comm, nx=args.nx, ny=args.nx, k=args.k, cfl=5.0, integrator="be", steps=1, newton_steps=4,
                method=method, precision=FORMS[precision][0], condense32=FORMS[precision][1],
                forcing=FORMS[precision][2], restart=args.restart, max_linear=1500, ntol=args.ltol, ltol=args.ltol,
                safety=1.1, device=local, autotune=1 if args.autotune else 0)
-    s.gmres_graph(not args.stepped)
+    s.gmres_graph(not args.stepped and comm is None)
     it = Integrator(s, method)
     u0 = s.initial()
     it.stage_begin(u0)
@@ -365,6 +383,43 @@ def e2e_config(args, method: str, precision: str, torch, pg, local: int) -> dict
     s.close()
     torch.cuda.empty_cache()
     return out
+
+
+def slab_comm(local: int, world: int):
+    """This rank's NCCL slab communicator: over the torch.distributed group, or alone on one GPU."""
+    from dg_hdg_euler_cpp_b200.solver import SlabComm, nccl_slab_comm
+
+    if world > 1:
+        return nccl_slab_comm(local)
+    return SlabComm.nccl(SlabComm.nccl_unique_id(), 1, 0, local)
+
+
+def slab_check(args, torch, peaks, local: int, form: str, whole_ups: float, whole_final) -> dict:
+    """The DG headline form as a one-rank NCCL slab of the full mesh (ghost rows, halo copies,
+    ncclAllReduce reductions, cycles launched step by step) against the whole-mesh context, the
+    latter also with stepped cycles: the decomposition's cost on one GPU, and its state."""
+    import copy
+
+    stepped = copy.copy(args)
+    stepped.stepped = True
+    comm = slab_comm(local, 1)
+    try:
+        out, final = run_config(stepped, "dg", form, torch, None, peaks, False, 0, local, False, comm=comm)
+    finally:
+        comm.close()
+    ref, ref_final = run_config(stepped, "dg", form, torch, None, peaks, False, 0, local, False)
+    return {"form": form, "updates_per_s": out["updates_per_s"], "ms_per_update": out["ms_per_update"],
+            "krylov": out["krylov"], "whole_mesh_stepped_updates_per_s": ref["updates_per_s"],
+            "whole_mesh_graph_updates_per_s": whole_ups,
+            "ratio_vs_whole_mesh_stepped": out["updates_per_s"] / ref["updates_per_s"],
+            "krylov_whole_mesh": ref["krylov"],
+            "rel_state_diff_vs_whole_mesh": float(np.max(np.abs(final - ref_final)) / np.max(np.abs(ref_final))),
+            "rel_state_diff_vs_whole_mesh_graph": (float(np.max(np.abs(final - whole_final)) /
+                                                         np.max(np.abs(whole_final)))
+                                                   if whole_final is not None else None),
+            "slab": out.get("slab"),
+            "note": "one NCCL rank holding all 256 rows between two ghost rows; multi-GPU slabs: bench.py --slabs "
+                    "--gpus N under torchrun"}
 
 
 def graph_comparison(torch, local: int):
@@ -696,10 +751,17 @@ def main():
     for _, form in configs:
         if form not in FORMS:
             raise SystemExit(f"unknown precision form {form}")
+    comm = None
+    if args.slabs:  # one mesh over all ranks: the DG forms only
+        configs = [c for c in configs if c[0] == "dg"]
+        if not configs:
+            raise SystemExit("--slabs decomposes the DG forms only")
+        comm = slab_comm(local, world)
+    copies = 1 if comm is not None else world  # independent problems solved by the job
     results = {}
     finals = {}
     for method, precision in configs:
-        out, final = run_config(args, method, precision, torch, pg, peaks, rank == 0, rank, local, False)
+        out, final = run_config(args, method, precision, torch, pg, peaks, rank == 0, rank, local, False, comm=comm)
         results[f"{method}_{precision}"] = out
         finals[(method, precision)] = final
     # every reduced-precision form against the all-FP64 form: state error after the same
@@ -732,20 +794,23 @@ def main():
     if not args.no_e2e:  # the headline forms end to end through the C ABI with host buffers
         for k in head:
             method, form = k.split("_", 1)
-            results[k]["e2e"] = e2e_config(args, method, form, torch, pg, local)
+            results[k]["e2e"] = e2e_config(args, method, form, torch, pg, local, comm=comm)
     tot_upd = sum(results[k]["updates"] for k in head)
     tot_ms = sum(results[k]["ms"] for k in head)
-    value = world * 1000.0 * tot_upd / tot_ms
+    value = copies * 1000.0 * tot_upd / tot_ms
     dom = results[head[0]]["roofline"]
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": tot_ms / tot_upd, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": tot_ms / tot_upd, "higher_is_better": True,
+        "scaling": "strong" if comm is not None else "weak",
         "vs_baseline": None, "dtype": "f64 (reduced forms: FP32 block-Jacobi factors, FP16 DG factors in mixed16, FP32 "
                  "condensation in mixed32; residuals, J.v, Arnoldi and acceptance in FP64)", "data": "synthetic",
         "config": {"workload": f"{args.nx}x{args.nx} k={args.k} rotated simple wave, BE CFL5, GMRES(20), exact "
                                f"block-Jacobi, ntol=ltol={args.ltol:g}, one Newton update per step, timed updates "
                                f"are protocol updates 2-4 of ceil(K/3) reset-and-warm units; value combines "
-                               f"the {' and '.join(head)} solves", "parallelism": f"replicas x{world}",
+                               f"the {' and '.join(head)} solves",
+                   "parallelism": f"slabs x{world} (one mesh, NCCL halo and reductions)" if comm is not None
+                   else f"replicas x{world}",
                    "l2": "inputs larger than L2 (factor pool 27-55 GB, Schur pool 10.9 GB)",
                    "value_definition": "(K_dg+K_hdg)/(t_dg+t_hdg) over the fastest reduced-precision DG and HDG "
                                        "forms (headline_forms), all at the reference's acceptance tolerance"},
@@ -756,7 +821,7 @@ def main():
             "kernel": dom["kernel"], "peak_source": peak_src,
             "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_launch_ms"]}) if dom else None,
         "gpu_launches": int(sum(results[k]["launches"] for k in head)),
-        "with_forcing_floor": ({"value": world * 1000.0 * sum(results[k]["updates"] for k in head_af) /
+        "with_forcing_floor": ({"value": copies * 1000.0 * sum(results[k]["updates"] for k in head_af) /
                                          sum(results[k]["ms"] for k in head_af),
                                 "forms": head_af} if head_af and head_af != head else None),
         "headline_forms": {k.split("_", 1)[0]: k.split("_", 1)[1] + ": " + FORMS[k.split("_", 1)[1]][3] for k in head},
@@ -773,7 +838,7 @@ def main():
                           "reasons": sorted({r for c in clocks for r in c["reasons"]})}
     if not args.no_e2e and all("e2e" in results[k] for k in head):
         e2e_s = sum(results[k]["e2e"]["seconds"] for k in head)
-        line["e2e"] = {"value": world * tot_upd / e2e_s, "unit": "updates/s",
+        line["e2e"] = {"value": copies * tot_upd / e2e_s, "unit": "updates/s",
                        "h2d_bytes_per_step": results[head[0]]["e2e"]["h2d_bytes_per_step"],
                        "d2h_bytes_per_step": results[head[0]]["e2e"]["d2h_bytes_per_step"]}
     if rank == 0 and world == 1 and args.n512:
@@ -797,10 +862,18 @@ def main():
         line["breakdown"]["uneven_batch_16"] = uneven_batch(torch, local, graph=not args.stepped)
     if rank == 0 and world == 1 and not args.no_graph_check:
         line["breakdown"]["gmres_graph_vs_stepped"] = graph_comparison(torch, local)
+    dg_head = [k for k in head if k.startswith("dg_")]
+    if rank == 0 and world == 1 and comm is None and not args.no_slab_check and dg_head:
+        form = dg_head[0].split("_", 1)[1]
+        line["breakdown"]["slab_nccl_one_rank"] = slab_check(args, torch, peaks, local, form,
+                                                             results[dg_head[0]]["updates_per_s"],
+                                                             finals.get(("dg", form)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if comm is not None:
+        comm.close()
     if pg is not None:
         pg.destroy_process_group()
 
