@@ -193,12 +193,15 @@ struct dgh_ctx {
     dgh_lockstep *ls = nullptr;
     int ls_index = -1;
     // slab of a decomposed mesh (dgh_ctx_create_slab): global rows [row0, row0 + rows) of ny,
-    // held as local rows 1..rows between ghost rows 0 and rows+1 that the halo exchange fills;
-    // row_len doubles per cell row of a volume vector; buf: device scratch of host collectives
+    // held as local rows 1..rows above ghost row 0 and below `above` ghost rows (1 for the DG
+    // operator; 2 for HDG, whose top ghost cells are condensed and need their own upper faces);
+    // row_len doubles per cell row of a volume vector, face_row per face row of a trace vector;
+    // the halo plans of volume and trace vectors; buf: device scratch of host collectives
     struct Slab {
         dgh_comm *comm = nullptr;
-        int row0 = 0, rows = 0, ny = 0;
-        long long row_len = 0;
+        int row0 = 0, rows = 0, ny = 0, above = 1;
+        long long row_len = 0, face_row = 0;
+        dgh_halo_plan vol, trace;
         double *buf = nullptr;
     } slab;
     bool slabbed() const { return slab.comm != nullptr; }
@@ -275,8 +278,10 @@ struct dgh_ctx {
     bool has_hdg() const { return cfg.method == DGH_METHOD_HDG || cfg.method == DGH_METHOD_BOTH; }
     int team_blocks(int cpb) const { return (cells + cpb - 1) / cpb; }
     // Deterministic weighted reduction helpers (return host values).
-    double reduce_scalar(const double *x, const double *W, bool divide, long long n_) {
-        if (slabbed() && n_ == N) {  // the interior rows, summed over the ranks
+    // interior: x is a volume vector whose ghost rows a slab must skip (otherwise its ghost rows
+    // or faces are zero)
+    double reduce_scalar(const double *x, const double *W, bool divide, long long n_, bool interior = false) {
+        if (slabbed() && interior) {  // the interior rows, summed over the ranks
             x += slab.row_len;
             W += slab.row_len;
             n_ = (long long)slab.rows * slab.row_len;
@@ -453,14 +458,29 @@ void launch_trace(dgh_ctx *c, const double *u, double *tr, bool check) {
 // kernel reads neighbour cells), or cleared (outputs whose ghost rows hold no equation).  The
 // library owns the ghost rows of the vectors passed to it, const or not.
 void slab_halo(dgh_ctx *c, const double *v) {
-    if (!c->slabbed()) return;
-    c->slab.comm->halo(const_cast<double *>(v), c->slab.row_len, c->slab.rows, c->stream);
+    if (c->slabbed()) c->slab.comm->exchange(const_cast<double *>(v), c->slab.vol, c->stream);
 }
 void slab_zero_ghosts(dgh_ctx *c, double *v) {
     if (!c->slabbed()) return;
-    const size_t bytes = (size_t)c->slab.row_len * sizeof(double);
-    ck(cudaMemsetAsync(v, 0, bytes, c->stream), "memset");
-    ck(cudaMemsetAsync(v + (size_t)(c->slab.rows + 1) * c->slab.row_len, 0, bytes, c->stream), "memset");
+    const size_t row = (size_t)c->slab.row_len;
+    ck(cudaMemsetAsync(v, 0, row * sizeof(double), c->stream), "memset");
+    ck(cudaMemsetAsync(v + (c->slab.rows + 1) * row, 0, c->slab.above * row * sizeof(double), c->stream), "memset");
+}
+// Trace vectors of a slab (HDG): the owned faces are the x faces and the upper y faces of the
+// slab's own rows.  The halo brings the faces the Schur apply, the recovery and the recovered
+// residual of owned faces and interior cells read: the lower y faces of row 1 (owned by the rank
+// below), and the x and upper y faces of the first ghost row above (owned by the rank above).
+void slab_trace_halo(dgh_ctx *c, const double *v) {
+    if (c->slabbed()) c->slab.comm->exchange(const_cast<double *>(v), c->slab.trace, c->stream);
+}
+void slab_zero_ghost_faces(dgh_ctx *c, double *v) {
+    if (!c->slabbed()) return;
+    const size_t fr = (size_t)c->slab.face_row, y0 = (size_t)c->cells * c->fw;
+    const size_t top = (size_t)(c->slab.rows + 1) * fr, tail = (size_t)c->slab.above * fr;
+    for (size_t base : {(size_t)0, y0}) {
+        ck(cudaMemsetAsync(v + base, 0, fr * sizeof(double), c->stream), "memset");
+        ck(cudaMemsetAsync(v + base + top, 0, tail * sizeof(double), c->stream), "memset");
+    }
 }
 // Device values summed over the slab ranks in place (the Arnoldi coefficients and norms).
 void slab_sum(dgh_ctx *c, double *dev, int count) {
@@ -968,11 +988,13 @@ void hdg_apply(dgh_ctx *c, const double *lam, double *out) {
         c->launched();
         return;
     }
+    slab_trace_halo(c, lam);
     DGH_DISPATCH_N(c->n, {
         if (c->c32()) k_hdg_apply32<N><<<c->faces, 256, 0, c->stream>>>(c->S32, c->speeds, lam, out, c->basis, c->g);
         else k_hdg_apply<N><<<c->faces, 256, 0, c->stream>>>(c->S, c->speeds, lam, out, c->basis, c->g);
     });
     c->launched();
+    slab_zero_ghost_faces(c, out);
 }
 // Face-block Jacobi blocks of the current Schur operator (FP64 or FP32 Schur blocks) into pool.
 template <typename TF> void face_blocks(dgh_ctx *c, TF *pool) {
@@ -1185,9 +1207,10 @@ void gmres(dgh_ctx *c, int op, const double *rhs, double *x, int limit, double t
     g.restart = (int)std::min<long long>(g.n, c->cfg.restart);
     g.r = c->gres[op];
     const long long n = g.n;
-    need(!c->slabbed() || op == DGH_OP_DG, "Slab contexts solve the DG operator only");
+    need(!c->slabbed() || op != DGH_OP_DG_T, "Slab contexts do not solve with J^T");
     ck(cudaMemcpyAsync(c->g_rhs, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
-    slab_zero_ghosts(c, c->g_rhs);  // the Krylov vectors of a slab keep zero ghost rows
+    if (op == DGH_OP_HDG) slab_zero_ghost_faces(c, c->g_rhs);  // a slab's Krylov vectors keep zero ghosts
+    else slab_zero_ghosts(c, c->g_rhs);
     ck(cudaMemsetAsync(c->g_x, 0, n * sizeof(double), c->stream), "memset");
     ck(cudaMemcpyAsync(g.r, c->g_rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
     const double rhs_norm = std::sqrt(std::max(0.0, c->reduce_scalar(c->g_rhs, g.W, false, n)));
@@ -1836,11 +1859,14 @@ int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out) {
     *out = nullptr;
     const char *why = nullptr;
     if (!comm) why = "null communicator";
-    else if (cfg->dim != 2 || cfg->method != DGH_METHOD_DG) why = "Slab decomposition is built for the 2D DG method";
+    else if (cfg->dim != 2 || cfg->method == DGH_METHOD_BOTH)
+        why = "Slab decomposition is built for the 2D DG or HDG method";
     else if (cfg->quadrature != 0 && cfg->quadrature != cfg->degree + 1)
         why = "Slab decomposition is built for the collocated volume rule";
     else if (cfg->preconditioner != 0) why = "Slab decomposition is built for the block-Jacobi preconditioner";
     else if (cfg->ny < 3 || comm->size > cfg->ny) why = "Slab decomposition needs at least one mesh row per rank";
+    else if (cfg->method == DGH_METHOD_HDG && cfg->ny < 2 * comm->size)
+        why = "HDG slabs need at least two mesh rows per rank";
     if (why) {
         g_create_error = why;
         return DGH_ERR_INVALID;
@@ -1850,11 +1876,11 @@ int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out) {
     si.ny = cfg->ny;
     dgh_slab::rows_of(cfg->ny, comm->size, comm->rank, si.row0, si.rows);
     dgh_config local = *cfg;
-    local.ny = si.rows + 2;  // the slab's rows between its two ghost rows
+    local.ny = si.rows + 1 + (cfg->method == DGH_METHOD_HDG ? 2 : 1);  // the slab's rows with its ghost rows
     return create_ctx(&local, &si, out);
 }
 
-int dgh_slab_info(const dgh_ctx *c, int64_t out[6]) {
+int dgh_slab_info(const dgh_ctx *c, int64_t out[8]) {
     if (!c || !out || !c->slabbed()) return DGH_ERR_INVALID;
     out[0] = c->slab.row0;
     out[1] = c->slab.rows;
@@ -1862,6 +1888,8 @@ int dgh_slab_info(const dgh_ctx *c, int64_t out[6]) {
     out[3] = c->slab.comm->size;
     out[4] = c->slab.row_len;
     out[5] = (int64_t)c->slab.rows * c->slab.row_len;
+    out[6] = c->slab.above;
+    out[7] = c->slab.face_row;
     return DGH_OK;
 }
 }  // extern "C"
@@ -1946,7 +1974,23 @@ int create_ctx(const dgh_config *cfg, const SlabInit *slab, dgh_ctx **out) {
             c->slab.row0 = slab->row0;
             c->slab.rows = slab->rows;
             c->slab.ny = slab->ny;
+            c->slab.above = k.ny - 1 - slab->rows;
             c->slab.row_len = (long long)k.nx * NVAR * c->n * c->n;
+            c->slab.face_row = (long long)k.nx * c->fw;
+            // volume vectors: rows 1..above go to the rank below (its upper ghost rows), row
+            // `rows` to the rank above (its ghost row 0)
+            const long long rl = c->slab.row_len, R = slab->rows, A = c->slab.above;
+            c->slab.vol.to_below = {{rl, A * rl}};
+            c->slab.vol.to_above = {{R * rl, rl}};
+            c->slab.vol.from_above = {{(R + 1) * rl, A * rl}};
+            c->slab.vol.from_below = {{0, rl}};
+            // trace vectors (x faces, then y faces): row 1's x and upper y faces to the rank
+            // below, row `rows`' upper y faces to the rank above
+            const long long fr = c->slab.face_row, y0 = (long long)c->cells * c->fw;
+            c->slab.trace.to_below = {{fr, fr}, {y0 + fr, fr}};
+            c->slab.trace.to_above = {{y0 + R * fr, fr}};
+            c->slab.trace.from_above = {{(R + 1) * fr, fr}, {y0 + (R + 1) * fr, fr}};
+            c->slab.trace.from_below = {{y0, fr}};
         }
         // nodal_basis.hpp:34-65
         std::vector<double> x, w;
@@ -2383,10 +2427,10 @@ int dgh_trace(dgh_ctx *c, const double *u, double *lam) {
 }
 
 int dgh_dual_norm(dgh_ctx *c, const double *r, double *out) {
-    return guard(c, [&] { *out = std::sqrt(c->reduce_scalar(r, c->mass, true, c->N)); });
+    return guard(c, [&] { *out = std::sqrt(c->reduce_scalar(r, c->mass, true, c->N, true)); });
 }
 int dgh_state_norm(dgh_ctx *c, const double *u, double *out) {
-    return guard(c, [&] { *out = std::sqrt(c->reduce_scalar(u, c->mass, false, c->N)); });
+    return guard(c, [&] { *out = std::sqrt(c->reduce_scalar(u, c->mass, false, c->N, true)); });
 }
 
 int dgh_integral(dgh_ctx *c, const double *u, double out[4]) {
@@ -2960,6 +3004,7 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
     return guard(c, [&] {
         need(c->has_hdg(), "context has no HDG operator");
         Timed tm(c, DGH_TIMER_CONDENSE);
+        slab_halo(c, r);  // the ghost cells are condensed too, with their own residual rows
         linearise(c, u);
         const int ld = c->m + c->t + 1;
         if (c->d1()) {
@@ -2992,7 +3037,7 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
             };
             if (c->hdg_variant < 0) {
                 const int sample = std::min(aug_chunk<double>(c), std::max(c->lu_grid, 1) * 4);
-                c->hdg_variant = tuned_variant(c, 2, [&](int v) { chunk(v, 0, sample); }, c->tune_ms + 2);
+                c->hdg_variant = tuned_variant_all(c, 2, [&](int v) { chunk(v, 0, sample); }, c->tune_ms + 2);
                 c->check_status();
             }
             const int per = c->hdg_variant == 0 ? aug_chunk<double>(c) : aug_chunk<float>(c);
@@ -3005,7 +3050,7 @@ int dgh_hdg_refresh_projected(dgh_ctx *c, const double *u, const double *r) {
         }
         if (c->hdg_variant < 0) {
             const int sample = std::min(c->aug_cells, std::max(c->lu_grid, 1) * 4);
-            c->hdg_variant = tuned_variant(c, 1, [&](int v) { hdg_condense_chunk(c, v, r, 0, sample); }, c->tune_ms + 2);
+            c->hdg_variant = tuned_variant_all(c, 1, [&](int v) { hdg_condense_chunk(c, v, r, 0, sample); }, c->tune_ms + 2);
             c->check_status();
         }
         for (int first = 0; first < c->cells; first += c->aug_cells)
@@ -3023,6 +3068,7 @@ int dgh_hdg_rhs(dgh_ctx *c, double *rhs) {
     return guard(c, [&] {
         need(c->condensed, "Condense the HDG operator first");
         ck(cudaMemcpyAsync(rhs, c->hrhs, c->NT * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+        slab_zero_ghost_faces(c, rhs);
     });
 }
 int dgh_hdg_apply(dgh_ctx *c, const double *lam, double *out) {
@@ -3051,6 +3097,7 @@ int dgh_hdg_block(dgh_ctx *c, int row, int col, double *host_block) {
 int dgh_hdg_recover(dgh_ctx *c, const double *dl, double *du) {
     return guard(c, [&] {
         need(c->condensed, "Condense the HDG operator first");
+        slab_trace_halo(c, dl);
         if (c->d1()) {
             DGH_DISPATCH_N(c->n, { k1_hdg_recover<N><<<grid1(c->N), K1_THREADS, 0, c->stream>>>(c->X, c->Y, dl, du, c->g1); });
         } else if (c->c32()) {
@@ -3074,6 +3121,7 @@ int dgh_hdg_retarget(dgh_ctx *c, const double *r) {
         need(c->condensed, "Condense the HDG operator first");
         need(c->c32(), "Retargeting needs the kept FP32 cell factors (condense32)");
         Timed tm(c, DGH_TIMER_CONDENSE);
+        slab_halo(c, r);
         // y = A^{-1} r with the kept factors, C y per cell, and the condensed right-hand side
         launch_solve<float>(c, c->lu32, c->lu32_perm, (size_t)c->m * c->m, c->m, c->cells, r, c->Y);
         DGH_DISPATCH_N(c->n, {
@@ -3088,6 +3136,7 @@ int dgh_hdg_retarget(dgh_ctx *c, const double *r) {
 int dgh_hdg_recovered_residual(dgh_ctx *c, const double *e, double *out) {
     return guard(c, [&] {
         need(c->condensed, "Condense the HDG operator first");
+        slab_trace_halo(c, e);
         if (c->d1()) {
             DGH_DISPATCH_N(c->n, {
                 k1_hdg_recovered_residual<N><<<grid1(c->N), K1_THREADS, 0, c->stream>>>(e, c->speeds, out, c->b1, c->g1);

@@ -47,8 +47,8 @@ struct LocalGroup {
     std::string why;
     std::vector<std::vector<double>> vals;
     std::vector<double *> vec;
-    std::vector<int> rows, device;
-    std::vector<long long> row_len;
+    std::vector<const dgh_halo_plan *> plan;
+    std::vector<int> device;
 
     void barrier(int rank) {
         std::unique_lock<std::mutex> lk(mu);
@@ -106,33 +106,43 @@ struct LocalComm final : dgh_comm {
         cuda_ck(cudaMemcpyAsync(dev, res.data(), count * sizeof(double), cudaMemcpyHostToDevice, st), "collective write");
         cuda_ck(cudaStreamSynchronize(st), "collective write");
     }
-    void halo(double *v, long long row_len, int rows, cudaStream_t st) override {
-        const size_t bytes = (size_t)row_len * sizeof(double);
+    void exchange(double *v, const dgh_halo_plan &p, cudaStream_t st) override {
         int dev = 0;
         cuda_ck(cudaGetDevice(&dev), "cudaGetDevice");
-        if (size == 1) {  // the periodic wrap inside one slab
-            copy_row(v, dev, v + (size_t)rows * row_len, dev, bytes, st);
-            copy_row(v + (size_t)(rows + 1) * row_len, dev, v + row_len, dev, bytes, st);
+        if (size == 1) {  // the periodic wrap inside one slab: this rank is its own neighbour
+            copy_regions(v, dev, p.from_below, v, dev, p.to_above, st);
+            copy_regions(v, dev, p.from_above, v, dev, p.to_below, st);
             return;
         }
         cuda_ck(cudaStreamSynchronize(st), "halo");
         g->vec[rank] = v;
-        g->rows[rank] = rows;
+        g->plan[rank] = &p;
         g->device[rank] = dev;
-        g->row_len[rank] = row_len;
         g->barrier(rank);
         const int below = (rank + size - 1) % size, above = (rank + 1) % size;
-        bool same = g->row_len[below] == row_len && g->row_len[above] == row_len;
+        const bool same = matches(p.from_below, g->plan[below]->to_above) && matches(p.from_above, g->plan[above]->to_below);
         if (same) {
-            copy_row(v, dev, g->vec[below] + (size_t)g->rows[below] * row_len, g->device[below], bytes, st);
-            copy_row(v + (size_t)(rows + 1) * row_len, dev, g->vec[above] + row_len, g->device[above], bytes, st);
+            copy_regions(v, dev, p.from_below, g->vec[below], g->device[below], g->plan[below]->to_above, st);
+            copy_regions(v, dev, p.from_above, g->vec[above], g->device[above], g->plan[above]->to_below, st);
             cuda_ck(cudaStreamSynchronize(st), "halo");
         }
         g->barrier(rank);
         if (!same) {
-            fail("neighbouring slabs have different row lengths");
-            throw dgh_comm_failure("neighbouring slabs have different row lengths");
+            fail("neighbouring slabs exchange regions of different sizes");
+            throw dgh_comm_failure("neighbouring slabs exchange regions of different sizes");
         }
+    }
+    static bool matches(const std::vector<dgh_region> &a, const std::vector<dgh_region> &b) {
+        if (a.size() != b.size()) return false;
+        for (size_t i = 0; i < a.size(); ++i)
+            if (a[i].count != b[i].count) return false;
+        return true;
+    }
+    static void copy_regions(double *dst, int dst_dev, const std::vector<dgh_region> &into, const double *src, int src_dev,
+                             const std::vector<dgh_region> &from, cudaStream_t st) {
+        for (size_t i = 0; i < into.size() && i < from.size(); ++i)
+            copy_row(dst + into[i].offset, dst_dev, src + from[i].offset, src_dev,
+                     (size_t)into[i].count * sizeof(double), st);
     }
     void fail(const std::string &why) noexcept override {
         try {
@@ -209,25 +219,27 @@ struct NcclComm final : dgh_comm {
         nccl_ck(nccl().allreduce(dev, dev, (size_t)count, ncclDouble, op == 0 ? ncclSum : ncclMax, comm, st),
                 "ncclAllReduce");
     }
-    void halo(double *v, long long row_len, int rows, cudaStream_t st) override {
+    void exchange(double *v, const dgh_halo_plan &p, cudaStream_t st) override {
         check();
-        const size_t n = (size_t)row_len;
-        double *bottom = v + n, *top = v + (size_t)rows * n;               // interior rows sent
-        double *ghost_below = v, *ghost_above = v + (size_t)(rows + 1) * n;  // ghost rows received
         if (size == 1) {
-            copy_row(ghost_below, device, top, device, n * sizeof(double), st);
-            copy_row(ghost_above, device, bottom, device, n * sizeof(double), st);
+            for (size_t i = 0; i < p.from_below.size(); ++i)
+                copy_row(v + p.from_below[i].offset, device, v + p.to_above[i].offset, device,
+                         (size_t)p.from_below[i].count * sizeof(double), st);
+            for (size_t i = 0; i < p.from_above.size(); ++i)
+                copy_row(v + p.from_above[i].offset, device, v + p.to_below[i].offset, device,
+                         (size_t)p.from_above[i].count * sizeof(double), st);
             return;
         }
         // With two ranks both neighbours are the same peer, and NCCL matches that peer's
-        // messages in posting order: each rank sends bottom then top, and receives into the
-        // ghost above (the peer's bottom row) then the ghost below (the peer's top row).
+        // messages in posting order: every rank sends its to_below regions, then its to_above
+        // regions, and receives its from_above regions (the peer's to_below), then its
+        // from_below regions (the peer's to_above).
         const int below = (rank + size - 1) % size, above = (rank + 1) % size;
         nccl_ck(nccl().group_start(), "ncclGroupStart");
-        nccl_ck(nccl().send(bottom, n, ncclDouble, below, comm, st), "ncclSend");
-        nccl_ck(nccl().send(top, n, ncclDouble, above, comm, st), "ncclSend");
-        nccl_ck(nccl().recv(ghost_above, n, ncclDouble, above, comm, st), "ncclRecv");
-        nccl_ck(nccl().recv(ghost_below, n, ncclDouble, below, comm, st), "ncclRecv");
+        for (const auto &r : p.to_below) nccl_ck(nccl().send(v + r.offset, (size_t)r.count, ncclDouble, below, comm, st), "ncclSend");
+        for (const auto &r : p.to_above) nccl_ck(nccl().send(v + r.offset, (size_t)r.count, ncclDouble, above, comm, st), "ncclSend");
+        for (const auto &r : p.from_above) nccl_ck(nccl().recv(v + r.offset, (size_t)r.count, ncclDouble, above, comm, st), "ncclRecv");
+        for (const auto &r : p.from_below) nccl_ck(nccl().recv(v + r.offset, (size_t)r.count, ncclDouble, below, comm, st), "ncclRecv");
         nccl_ck(nccl().group_end(), "ncclGroupEnd");
     }
     void fail(const std::string &w) noexcept override {
@@ -277,9 +289,8 @@ int dgh_comm_local_create(int size, int timeout_ms, dgh_comm **ranks) {
         g->timeout = std::chrono::milliseconds(timeout_ms);
         g->vals.resize(size);
         g->vec.assign(size, nullptr);
-        g->rows.assign(size, 0);
+        g->plan.assign(size, nullptr);
         g->device.assign(size, 0);
-        g->row_len.assign(size, 0);
         for (int r = 0; r < size; ++r) ranks[r] = new LocalComm(g, r);
     });
 }

@@ -1,11 +1,12 @@
 // Communicators of the slab domain decomposition (dgh_comm_*, dgh_ctx_create_slab).
 //
 // The 2D mesh is split into slabs of whole cell rows, one per rank.  A slab context holds its
-// rows plus one ghost row below and one above (local rows 0 and rows+1); a volume vector of the
-// slab is (rows + 2) * row_len contiguous doubles, row_len = nx * 4 (k+1)^2.  A communicator
-// provides the two exchanges the DG Newton update needs: the sum or maximum of a few doubles
-// over all ranks (norms, Arnoldi coefficients, the CFL rate, status bits) and the halo exchange
-// that fills a vector's ghost rows from the neighbouring slabs.  Two kinds exist:
+// rows plus ghost rows (one below; one above for the DG operator, two for HDG, whose top ghost
+// cells are condensed and need their own upper faces).  A communicator provides the two
+// exchanges a Newton update needs: the sum or maximum of a few doubles over all ranks (norms,
+// Arnoldi coefficients, the CFL rate, status bits) and a halo exchange that copies regions of a
+// vector between neighbouring slabs (ghost cell rows of a volume vector, ghost face rows of a
+// trace vector).  Two kinds exist:
 //  - nccl:  one rank per process and GPU; collectives are NCCL calls on the caller's stream
 //           (ncclAllReduce, grouped ncclSend/ncclRecv), libnccl resolved at run time;
 //  - local: several ranks inside one process (one host thread each, any devices), exchanging
@@ -16,10 +17,21 @@
 
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 // A collective that could not complete: a peer failed, or did not arrive in time.
 struct dgh_comm_failure : std::runtime_error {
     using std::runtime_error::runtime_error;
+};
+
+// A region of a vector: `count` doubles from `offset`.
+struct dgh_region {
+    long long offset = 0, count = 0;
+};
+// Regions sent to the rank below and to the rank above, and regions received from the rank above
+// and from the rank below, each list in order.
+struct dgh_halo_plan {
+    std::vector<dgh_region> to_below, to_above, from_above, from_below;
 };
 
 struct dgh_comm {
@@ -29,9 +41,10 @@ struct dgh_comm {
     // In place over all ranks: op 0 sums, op 1 takes the maximum of count doubles at dev; ordered
     // on stream.  Every rank receives the same bits.
     virtual void allreduce(double *dev, int count, int op, cudaStream_t stream) = 0;
-    // Fills the ghost rows of a slab vector: local row 0 from the top interior row of the rank
-    // below, local row rows+1 from the bottom interior row of the rank above (periodic in rank).
-    virtual void halo(double *vec, long long row_len, int rows, cudaStream_t stream) = 0;
+    // The halo exchange of one vector under `plan`: the i-th region sent to a neighbour lands in
+    // that neighbour's i-th region received from this side (below and above are periodic in rank;
+    // every rank uses a plan of the same shape).
+    virtual void exchange(double *vec, const dgh_halo_plan &plan, cudaStream_t stream) = 0;
     // Marks the group failed so that peers waiting in (or entering) a collective end with an error.
     virtual void fail(const std::string &why) noexcept = 0;
 };

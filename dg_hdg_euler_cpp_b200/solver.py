@@ -81,9 +81,10 @@ class Solver:
         self.comm = comm  # the communicator outlives the context
         self.slab = None
         if comm is not None:
-            info = (ctypes.c_int64 * 6)()
+            info = (ctypes.c_int64 * 8)()
             self._rc(self.lib.dgh_slab_info(self.h, info))
-            self.slab = dict(zip(("row0", "rows", "rank", "size", "offset", "length"), (int(x) for x in info)))
+            self.slab = dict(zip(("row0", "rows", "rank", "size", "offset", "length", "above", "face_row"),
+                                 (int(x) for x in info)))
         s = (ctypes.c_int64 * 8)()
         self._rc(self.lib.dgh_sizes(self.h, s))
         self.size, self.trace_size, self.block, self.cells, self.faces, self.n, self.local_trace, self.face_width = (
@@ -124,6 +125,14 @@ class Solver:
         if self.slab is None:
             return v
         return v[self.slab["offset"]:self.slab["offset"] + self.slab["length"]]
+
+    def owned_faces(self, lam):
+        """The slab's own faces of a trace vector (x faces, then upper y faces, of its rows),
+        concatenated; the whole vector outside a slab."""
+        if self.slab is None:
+            return lam
+        fr, rows, half = self.slab["face_row"], self.slab["rows"], self.trace_size // 2
+        return self.torch.cat([lam[fr:fr * (rows + 1)], lam[half + fr:half + fr * (rows + 1)]])
 
     def tensor(self, a):
         return self.torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=self.device)

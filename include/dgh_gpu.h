@@ -349,25 +349,30 @@ int dgh_lockstep_leave(dgh_lockstep *group, dgh_ctx *member);
 int dgh_lockstep_report(const dgh_lockstep *group, int64_t out[4]);
 
 /* ---- Slab domain decomposition (multi-GPU; the reference runs one process on one mesh) ---------
- * One 2D DG problem split into slabs of whole cell rows, one rank per slab: rank r of `size`
+ * One 2D DG or HDG problem split into slabs of whole cell rows, one rank per slab: rank r of `size`
  * owns global rows [row0, row0 + rows) (dgh_slab_rows: ny = size * base + extra, the first
  * `extra` ranks take base + 1 rows; out = {row0, rows, rank below, rank above}, periodic).
  * A slab context (dgh_ctx_create_slab; cfg as for the whole mesh, cfg->ny the global row count)
- * holds its rows plus one ghost row below and one above: every volume vector of it has
- * (rows + 2) * nx cells in the usual cell-major layout, local row 0 and row rows+1 being the
- * ghosts, so dgh_sizes()[0] = (rows + 2) * nx * 4 (k+1)^2 and dgh_slab_info gives the interior
- * (its first double and its length).  The ghost rows of vectors passed in belong to the library:
- * dgh_freeze, dgh_residual, dgh_admissible, dgh_dg_refresh, dgh_dg_apply and dgh_initial fill
- * them from the neighbouring slabs (a halo exchange) before reading neighbours, and the
- * residual and J*v outputs come back with zero ghost rows.  Norms, integrals, L2 errors,
+ * holds its rows plus ghost rows: one below and A above (A = 1 for the DG method, 2 for HDG,
+ * whose first ghost row above is condensed and needs its own upper faces).  Every volume vector
+ * has (rows + 1 + A) * nx cells in the usual cell-major layout, local row 0 and rows
+ * rows+1..rows+A being the ghosts, and every trace vector the faces of those cells (x faces, then
+ * y faces, each face owned by the cell below or left of it); dgh_slab_info gives where the
+ * interior starts and its length.  The ghost rows and faces of vectors passed in belong to the
+ * library: dgh_freeze, dgh_residual, dgh_admissible, dgh_dg_refresh, dgh_dg_apply, dgh_initial,
+ * dgh_hdg_refresh_projected (state and residual), dgh_hdg_retarget, dgh_hdg_apply,
+ * dgh_hdg_recover and dgh_hdg_recovered_residual fill them from the neighbouring slabs (a halo
+ * exchange of cell rows or face rows) before reading neighbours, and the residual, J*v, Schur
+ * apply and HDG right-hand-side outputs come back with zero ghosts.  Norms, integrals, L2 errors,
  * admissibility, the CFL rate, kernel status bits and the GMRES inner products are reduced over
  * all ranks, so every rank takes the same decisions (Newton, line search, GMRES restarts) and
  * receives the same scalars; every rank must make the same calls in the same order, each from
  * its own host thread or process.  Interior results equal the single-domain ones: residual,
- * J*v, frozen speeds and the CFL rate bitwise; norms and the Newton update to rounding of the
- * reduction order.  Covered: method DG, collocated rule, block Jacobi, every precision, BE and
- * DIRK3 (dgh_integrator_* on a slab context).  Not with slabs: HDG, over-integration, block
- * ILU(0), J^T / the adjoint, lockstep groups and graph-replayed GMRES cycles (refused).
+ * J*v, frozen speeds, the CFL rate, the condensed right-hand side and the Schur apply on owned
+ * faces bitwise; norms and the Newton update to rounding of the reduction order.  Covered: methods DG and HDG (HDG: at least two rows per rank), collocated
+ * rule, block Jacobi, every precision and the FP32 condensation, BE and DIRK3 (dgh_integrator_*
+ * on a slab context).  Not with slabs: method "both", over-integration, block ILU(0), J^T / the
+ * adjoint, lockstep groups and graph-replayed GMRES cycles (refused).
  * Communicators (the communicator must outlive its contexts):
  *  - dgh_comm_nccl_create: one rank per process and GPU over NCCL; rank 0 makes the id with
  *    dgh_comm_nccl_unique_id and the host shares it (e.g. a torch.distributed broadcast).
@@ -391,8 +396,9 @@ int dgh_comm_fail(dgh_comm *comm, const char *why);
 int dgh_comm_destroy(dgh_comm *comm);
 const char *dgh_comm_error(void);
 int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out);
-/* {global first row, interior rows, rank, size, first interior double, interior doubles} */
-int dgh_slab_info(const dgh_ctx *ctx, int64_t out[6]);
+/* {global first row, interior rows, rank, size, first interior double of a volume vector,
+ *  interior doubles, ghost rows above, doubles per face row of a trace vector} */
+int dgh_slab_info(const dgh_ctx *ctx, int64_t out[8]);
 
 /* ---- Discrete adjoint of the DG time integration (no counterpart in the reference) -------------
  * Objective J = sum over nodes of M rho^2 at the end of `steps` fixed steps (dt = cfl / rate of

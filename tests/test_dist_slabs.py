@@ -45,8 +45,9 @@ def test_slab_context_refuses_uncovered_configurations():
 
     lib = _lib.load()
     comms = SlabComm.local_group(2)
-    cases = [(dict(method="hdg"), "2D DG method"), (dict(dim=1, cells=12), "2D DG method"),
-             (dict(quad=6, k=3), "collocated volume rule"), (dict(precond="block-ilu0"), "block-Jacobi")]
+    cases = [(dict(method="both"), "2D DG or HDG method"), (dict(dim=1, cells=12), "2D DG or HDG method"),
+             (dict(quad=6, k=3), "collocated volume rule"), (dict(precond="block-ilu0"), "block-Jacobi"),
+             (dict(method="hdg", ny=3), "two mesh rows per rank")]
     for kw, msg in cases:
         base = dict(nx=8, ny=8, k=3, method="dg")
         base.update(kw)

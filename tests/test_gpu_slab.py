@@ -118,7 +118,7 @@ def newton_rows(kw, u_global, updates, comm=None):
     from dg_hdg_euler_cpp_b200.solver import Integrator, Solver
 
     s = Solver(comm=comm, **kw)
-    it = Integrator(s, "dg")
+    it = Integrator(s, kw["method"])
     u = to_slab(s, u_global) if comm is not None else s.tensor(u_global)
     dt = it.stage_begin(u)
     rows = [it.update() for _ in range(updates)]
@@ -156,6 +156,95 @@ def test_slab_newton_updates_match_whole_mesh(size, precision):
     for a, b in zip(ranks[0][1], ranks[-1][1]):  # every rank reports the same statistics
         assert all(a[key] == b[key] for key in KEYS)
     assert np.max(np.abs(got - state)) <= 1e-10 * scale
+
+
+def owned_of(lam: np.ndarray, nx: int, fw: int, cells: int, row0: int, rows: int) -> np.ndarray:
+    """The faces of global rows [row0, row0 + rows) of a whole-mesh trace vector: x faces, then
+    upper y faces."""
+    fr, half = nx * fw, cells * fw
+    return np.concatenate([lam[row0 * fr:(row0 + rows) * fr], lam[half + row0 * fr:half + (row0 + rows) * fr]])
+
+
+def to_slab_trace(s, lam_global: np.ndarray, cells: int):
+    """The slab's trace vector of a whole-mesh one: its own faces, NaN elsewhere."""
+    fr, rows, row0 = s.slab["face_row"], s.slab["rows"], s.slab["row0"]
+    out = s.vec(s.trace_size)
+    out.fill_(float("nan"))
+    half, ghalf = s.trace_size // 2, cells * s.face_width
+    out[fr:fr * (rows + 1)] = s.tensor(lam_global[row0 * fr:(row0 + rows) * fr])
+    out[half + fr:half + fr * (rows + 1)] = s.tensor(lam_global[ghalf + row0 * fr:ghalf + (row0 + rows) * fr])
+    return out
+
+
+@pytest.mark.parametrize("size", [1, 2, 3])
+@pytest.mark.parametrize("precision,condense32", [("fp64", 0), ("mixed", 0), ("mixed", 1)])
+def test_slab_hdg_operators_equal_whole_mesh(size, precision, condense32):
+    """The condensed right-hand side and the Schur apply on owned faces, the recovery and the
+    recovered residual on interior cells, bitwise; the trace inputs are NaN off the owned faces."""
+    from dg_hdg_euler_cpp_b200.solver import Solver, perturb
+
+    kw = dict(MESH, cfl=5.0, integrator="be", steps=1, method="hdg", precision=precision, condense32=condense32)
+    nx, ny, k = MESH["nx"], MESH["ny"], MESH["k"]
+    ref = whole(**kw)
+    u = perturb(ref.initial().cpu().numpy(), nx, ny, k, 0.1)
+    ut = ref.tensor(u)
+    dt = 5.0 / ref.freeze(ut)
+    ref.set_stage(ut, dt)
+    r = ref.residual(ut)
+    ref.hdg_refresh_projected(ut, r)
+    lam = np.cos(0.29 * np.arange(ref.trace_size)) * 1e-3
+    want = dict(rhs=ref.hdg_rhs().cpu().numpy(), sa=ref.hdg_apply(ref.tensor(lam)).cpu().numpy(),
+                du=ref.hdg_recover(ref.tensor(lam)).cpu().numpy(),
+                rr=ref.hdg_recovered_residual(ref.tensor(lam)).cpu().numpy())
+    cells, fw, m = ref.cells, ref.face_width, ref.block
+    ref.close()
+
+    def body(rank, comm):
+        s = Solver(comm=comm, **kw)
+        got = {"row0": s.slab["row0"], "rows": s.slab["rows"], "above": s.slab["above"]}
+        ul = to_slab(s, u)
+        s.freeze(ul)
+        s.set_stage(ul, dt)
+        rl = s.residual(ul)
+        s.hdg_refresh_projected(ul, rl)
+        got["rhs"] = s.owned_faces(s.hdg_rhs()).cpu().numpy()
+        got["sa"] = s.owned_faces(s.hdg_apply(to_slab_trace(s, lam, cells))).cpu().numpy()
+        got["du"] = s.interior(s.hdg_recover(to_slab_trace(s, lam, cells))).cpu().numpy()
+        got["rr"] = s.interior(s.hdg_recovered_residual(to_slab_trace(s, lam, cells))).cpu().numpy()
+        s.close()
+        return got
+
+    for g in run_slabs(size, body):
+        assert g["above"] == 2
+        for key in ("rhs", "sa"):
+            assert np.array_equal(g[key], owned_of(want[key], nx, fw, cells, g["row0"], g["rows"])), (key, g["row0"])
+        for key in ("du", "rr"):
+            assert np.array_equal(g[key], rows_of(want[key], nx, m, g["row0"], g["rows"])), (key, g["row0"])
+
+
+@pytest.mark.parametrize("size", [2, 3])
+@pytest.mark.parametrize("precision,condense32", [("fp64", 0), ("mixed", 0), ("mixed", 1)])
+def test_slab_hdg_newton_updates_match_whole_mesh(size, precision, condense32):
+    """The condensed HDG Newton update on 2-3 slabs: three updates as in the DG test."""
+    from dg_hdg_euler_cpp_b200.solver import perturb
+
+    kw = dict(nx=12, ny=12, k=3, cfl=5.0, integrator="be", steps=1, method="hdg", precision=precision,
+              condense32=condense32, restart=20)
+    s0 = whole(**kw)
+    u0 = perturb(s0.initial().cpu().numpy(), 12, 12, 3, 0.15)
+    s0.close()
+    dt, rows, state = newton_rows(kw, u0, 3)
+    ranks = run_slabs(size, lambda rank, comm: newton_rows(kw, u0, 3, comm))
+    got = gather([x[2] for x in ranks])
+    for rdt, rrows, _ in ranks:
+        assert rdt == dt
+        for a, b in zip(rrows, rows):
+            assert abs(a["krylov_iterations"] - b["krylov_iterations"]) <= 2, (a, b)
+            assert abs(a["residual_physical_rms"] - b["residual_physical_rms"]) <= 1e-9 * rows[0]["residual_physical_rms"]
+            assert a["damping"] == b["damping"]
+    for a, b in zip(ranks[0][1], ranks[-1][1]):
+        assert all(a[key] == b[key] for key in KEYS)
+    assert np.max(np.abs(got - state)) <= 1e-10 * np.max(np.abs(state))
 
 
 def test_slab_dirk3_advance_matches_whole_mesh():
