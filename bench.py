@@ -21,9 +21,9 @@ repeats the headline forms' timed updates through the C ABI with host buffers
 
 Multi-GPU: by default N ranks solve N independent replicas ("scaling": "weak", value = N x the
 per-replica rate).  --slabs instead splits ONE mesh into N slabs of cell rows, one per GPU, with
-the ghost-row halo exchange and the reductions over NCCL ("scaling": "strong", DG forms only).
-On one GPU the breakdown's slab_nccl_one_rank entry runs the DG headline form as a one-rank
-NCCL slab against the whole-mesh context (the decomposition's own cost and its state).
+the ghost-row (and, for HDG, ghost-face) halo exchange and the reductions over NCCL ("scaling":
+"strong").  On one GPU the breakdown's slab_nccl_one_rank entry runs each headline form as a
+one-rank NCCL slab against the whole-mesh context (the decomposition's own cost and its state).
 
 cpu_baseline and --impl reference time the reference algorithm's CPU implementation (the oracle
 restatement; the reference itself needs Eigen, which this image lacks) on the host cores:
@@ -92,10 +92,10 @@ def parse():
                    help="launch GMRES restart cycles step by step (default: replay each cycle as a CUDA graph)")
     p.add_argument("--autotune", action="store_true", help="time the factorisation variants per degree")
     p.add_argument("--slabs", action="store_true",
-                   help="strong scaling: the DG forms solve ONE mesh split into N slabs of cell rows (one per GPU, "
+                   help="strong scaling: every form solves ONE mesh split into N slabs of cell rows (one per GPU, "
                         "NCCL halo exchange and reductions) instead of N independent replicas")
     p.add_argument("--no-slab-check", action="store_true",
-                   help="skip the one-rank NCCL slab run of the DG headline form (1 GPU)")
+                   help="skip the one-rank NCCL slab runs of the headline forms (1 GPU)")
     return p.parse_args()
 
 
@@ -394,8 +394,8 @@ def slab_comm(local: int, world: int):
     return SlabComm.nccl(SlabComm.nccl_unique_id(), 1, 0, local)
 
 
-def slab_check(args, torch, peaks, local: int, form: str, whole_ups: float, whole_final) -> dict:
-    """The DG headline form as a one-rank NCCL slab of the full mesh (ghost rows, halo copies,
+def slab_check(args, torch, peaks, local: int, method: str, form: str, whole_ups: float, whole_final) -> dict:
+    """A headline form as a one-rank NCCL slab of the full mesh (ghost rows, halo copies,
     ncclAllReduce reductions, cycles launched step by step) against the whole-mesh context, the
     latter also with stepped cycles: the decomposition's cost on one GPU, and its state."""
     import copy
@@ -404,10 +404,10 @@ def slab_check(args, torch, peaks, local: int, form: str, whole_ups: float, whol
     stepped.stepped = True
     comm = slab_comm(local, 1)
     try:
-        out, final = run_config(stepped, "dg", form, torch, None, peaks, False, 0, local, False, comm=comm)
+        out, final = run_config(stepped, method, form, torch, None, peaks, False, 0, local, False, comm=comm)
     finally:
         comm.close()
-    ref, ref_final = run_config(stepped, "dg", form, torch, None, peaks, False, 0, local, False)
+    ref, ref_final = run_config(stepped, method, form, torch, None, peaks, False, 0, local, False)
     return {"form": form, "updates_per_s": out["updates_per_s"], "ms_per_update": out["ms_per_update"],
             "krylov": out["krylov"], "whole_mesh_stepped_updates_per_s": ref["updates_per_s"],
             "whole_mesh_graph_updates_per_s": whole_ups,
@@ -418,8 +418,8 @@ def slab_check(args, torch, peaks, local: int, form: str, whole_ups: float, whol
                                                          np.max(np.abs(whole_final)))
                                                    if whole_final is not None else None),
             "slab": out.get("slab"),
-            "note": "one NCCL rank holding all 256 rows between two ghost rows; multi-GPU slabs: bench.py --slabs "
-                    "--gpus N under torchrun"}
+            "note": "one NCCL rank holding all 256 rows between its ghost rows (DG: 1 below, 1 above; HDG: 1 "
+                    "below, 2 above); multi-GPU slabs: bench.py --slabs --gpus N under torchrun"}
 
 
 def graph_comparison(torch, local: int):
@@ -752,10 +752,7 @@ def main():
         if form not in FORMS:
             raise SystemExit(f"unknown precision form {form}")
     comm = None
-    if args.slabs:  # one mesh over all ranks: the DG forms only
-        configs = [c for c in configs if c[0] == "dg"]
-        if not configs:
-            raise SystemExit("--slabs decomposes the DG forms only")
+    if args.slabs:  # one mesh over all ranks
         comm = slab_comm(local, world)
     copies = 1 if comm is not None else world  # independent problems solved by the job
     results = {}
@@ -862,12 +859,13 @@ def main():
         line["breakdown"]["uneven_batch_16"] = uneven_batch(torch, local, graph=not args.stepped)
     if rank == 0 and world == 1 and not args.no_graph_check:
         line["breakdown"]["gmres_graph_vs_stepped"] = graph_comparison(torch, local)
-    dg_head = [k for k in head if k.startswith("dg_")]
-    if rank == 0 and world == 1 and comm is None and not args.no_slab_check and dg_head:
-        form = dg_head[0].split("_", 1)[1]
-        line["breakdown"]["slab_nccl_one_rank"] = slab_check(args, torch, peaks, local, form,
-                                                             results[dg_head[0]]["updates_per_s"],
-                                                             finals.get(("dg", form)))
+    if rank == 0 and world == 1 and comm is None and not args.no_slab_check:
+        checks = {}
+        for k in head:
+            method, form = k.split("_", 1)
+            checks[k] = slab_check(args, torch, peaks, local, method, form, results[k]["updates_per_s"],
+                                   finals.get((method, form)))
+        line["breakdown"]["slab_nccl_one_rank"] = checks
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
