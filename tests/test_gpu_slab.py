@@ -341,3 +341,87 @@ def test_slab_refuses_graphs_and_lockstep():
     assert "slab contexts" in lib.dgh_lockstep_error().decode()
     s.close()
     comms[0].close()
+
+
+TWO_GPU_WORKER = r"""
+import datetime, json, os, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np
+import torch
+import torch.distributed as dist
+from dg_hdg_euler_cpp_b200.solver import Integrator, Solver, nccl_slab_comm, perturb
+rank = int(os.environ["RANK"])
+torch.cuda.set_device(rank)
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))  # host plumbing: the NCCL id
+comm = nccl_slab_comm(rank)
+method = sys.argv[2]
+kw = dict(nx=12, ny=12, k=3, cfl=5.0, integrator="be", steps=1, method=method, precision="mixed", restart=20,
+          device=rank)
+whole = Solver(**kw)
+u0 = perturb(whole.initial().cpu().numpy(), 12, 12, 3, 0.15)
+whole.close()
+
+
+def run(s, u):
+    it = Integrator(s, method)
+    dt = it.stage_begin(u)
+    rows = [it.update()["krylov_iterations"] for _ in range(2)]
+    out = np.empty(s.size)
+    import ctypes
+    s.lib.dgh_download(s.h, out.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(it.state_ptr()), s.size)
+    it.close()
+    return dt, rows, out
+
+
+s = Solver(comm=comm, **kw)
+m, row0, rows = s.block, s.slab["row0"], s.slab["rows"]
+u = s.vec()
+s.interior(u).copy_(s.tensor(u0.reshape(-1, 12 * m)[row0:row0 + rows].reshape(-1)))
+dt, kry, out = run(s, u)
+mine = out[s.slab["offset"]:s.slab["offset"] + s.slab["length"]]
+s.close()
+parts = [None, None]
+dist.all_gather_object(parts, (dt, kry, mine.tolist()))
+if rank == 0:
+    ref = Solver(**kw)
+    rdt, rkry, rout = run(ref, ref.tensor(u0))
+    ref.close()
+    got = np.concatenate([np.array(p[2]) for p in parts])
+    print(json.dumps({"dt_equal": all(p[0] == rdt for p in parts), "krylov": [p[1] for p in parts],
+                      "krylov_whole": rkry, "rel": float(np.max(np.abs(got - rout)) / np.max(np.abs(rout)))}))
+comm.close()
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("method", ["dg", "hdg"])
+def test_nccl_two_gpus_match_whole_mesh(method):
+    """Two processes on two GPUs, one NCCL slab each (skipped with fewer GPUs): two Newton
+    updates against the whole mesh on rank 0's GPU."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    import torch
+
+    from conftest import ROOT
+    from test_dist_replicas import free_port
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    port = free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, "-c", TWO_GPU_WORKER, str(ROOT), method], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        out, err = p.communicate(timeout=600)
+        assert p.returncode == 0, err[-2000:]
+        outs.append(out)
+    res = json.loads(outs[0].strip().splitlines()[-1])
+    assert res["dt_equal"] and res["krylov"][0] == res["krylov"][1]
+    assert all(abs(a - b) <= 1 for a, b in zip(res["krylov"][0], res["krylov_whole"]))
+    assert res["rel"] <= 1e-10
