@@ -2412,6 +2412,7 @@ int dgh_admissible(dgh_ctx *c, const double *u, int *okp) {
 int dgh_trace(dgh_ctx *c, const double *u, double *lam) {
     return guard(c, [&] {
         need(c->frozen, "Freeze the wave speeds first");
+        slab_halo(c, u);
         launch_trace(c, u, c->traces, false);
         if (c->d1()) {
             k1_trace_lambda<<<grid1(c->cells), K1_THREADS, 0, c->stream>>>(c->traces, c->speeds, lam, c->g1);
@@ -2423,6 +2424,7 @@ int dgh_trace(dgh_ctx *c, const double *u, double *lam) {
             k_trace_lambda<N><<<(tot + 255) / 256, 256, 0, c->stream>>>(c->traces, c->speeds, lam, c->g);
         });
         c->launched();
+        slab_zero_ghost_faces(c, lam);
     });
 }
 

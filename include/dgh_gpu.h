@@ -360,10 +360,10 @@ int dgh_lockstep_report(const dgh_lockstep *group, int64_t out[4]);
  * y faces, each face owned by the cell below or left of it); dgh_slab_info gives where the
  * interior starts and its length.  The ghost rows and faces of vectors passed in belong to the
  * library: dgh_freeze, dgh_residual, dgh_admissible, dgh_dg_refresh, dgh_dg_apply, dgh_initial,
- * dgh_hdg_refresh_projected (state and residual), dgh_hdg_retarget, dgh_hdg_apply,
+ * dgh_trace, dgh_hdg_refresh_projected (state and residual), dgh_hdg_retarget, dgh_hdg_apply,
  * dgh_hdg_recover and dgh_hdg_recovered_residual fill them from the neighbouring slabs (a halo
- * exchange of cell rows or face rows) before reading neighbours, and the residual, J*v, Schur
- * apply and HDG right-hand-side outputs come back with zero ghosts.  Norms, integrals, L2 errors,
+ * exchange of cell rows or face rows) before reading neighbours, and the residual, J*v, trace,
+ * Schur apply and HDG right-hand-side outputs come back with zero ghosts.  Norms, integrals, L2 errors,
  * admissibility, the CFL rate, kernel status bits and the GMRES inner products are reduced over
  * all ranks, so every rank takes the same decisions (Newton, line search, GMRES restarts) and
  * receives the same scalars; every rank must make the same calls in the same order, each from

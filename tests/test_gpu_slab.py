@@ -179,8 +179,9 @@ def to_slab_trace(s, lam_global: np.ndarray, cells: int):
 @pytest.mark.parametrize("size", [1, 2, 3])
 @pytest.mark.parametrize("precision,condense32", [("fp64", 0), ("mixed", 0), ("mixed", 1)])
 def test_slab_hdg_operators_equal_whole_mesh(size, precision, condense32):
-    """The condensed right-hand side and the Schur apply on owned faces, the recovery and the
-    recovered residual on interior cells, bitwise; the trace inputs are NaN off the owned faces."""
+    """The condensed right-hand side, the Schur apply and the face traces of the state on owned
+    faces, the recovery and the recovered residual on interior cells, bitwise; the trace inputs
+    are NaN off the owned faces."""
     from dg_hdg_euler_cpp_b200.solver import Solver, perturb
 
     kw = dict(MESH, cfl=5.0, integrator="be", steps=1, method="hdg", precision=precision, condense32=condense32)
@@ -194,6 +195,7 @@ def test_slab_hdg_operators_equal_whole_mesh(size, precision, condense32):
     ref.hdg_refresh_projected(ut, r)
     lam = np.cos(0.29 * np.arange(ref.trace_size)) * 1e-3
     want = dict(rhs=ref.hdg_rhs().cpu().numpy(), sa=ref.hdg_apply(ref.tensor(lam)).cpu().numpy(),
+                tr=ref.trace(ut).cpu().numpy(),
                 du=ref.hdg_recover(ref.tensor(lam)).cpu().numpy(),
                 rr=ref.hdg_recovered_residual(ref.tensor(lam)).cpu().numpy())
     cells, fw, m = ref.cells, ref.face_width, ref.block
@@ -208,6 +210,7 @@ def test_slab_hdg_operators_equal_whole_mesh(size, precision, condense32):
         rl = s.residual(ul)
         s.hdg_refresh_projected(ul, rl)
         got["rhs"] = s.owned_faces(s.hdg_rhs()).cpu().numpy()
+        got["tr"] = s.owned_faces(s.trace(to_slab(s, u))).cpu().numpy()
         got["sa"] = s.owned_faces(s.hdg_apply(to_slab_trace(s, lam, cells))).cpu().numpy()
         got["du"] = s.interior(s.hdg_recover(to_slab_trace(s, lam, cells))).cpu().numpy()
         got["rr"] = s.interior(s.hdg_recovered_residual(to_slab_trace(s, lam, cells))).cpu().numpy()
@@ -216,7 +219,7 @@ def test_slab_hdg_operators_equal_whole_mesh(size, precision, condense32):
 
     for g in run_slabs(size, body):
         assert g["above"] == 2
-        for key in ("rhs", "sa"):
+        for key in ("rhs", "sa", "tr"):
             assert np.array_equal(g[key], owned_of(want[key], nx, fw, cells, g["row0"], g["rows"])), (key, g["row0"])
         for key in ("du", "rr"):
             assert np.array_equal(g[key], rows_of(want[key], nx, m, g["row0"], g["rows"])), (key, g["row0"])
