@@ -266,7 +266,9 @@ struct dgh_ctx {
         launches += k;
         ck(cudaGetLastError(), "kernel launch");
     }
-    void sync() { ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
+    // A slab context waits through its communicator (an NCCL rank gives up on a peer that never
+    // joins a collective instead of blocking for good).
+    void sync();
     bool mixed() const { return cfg.precision != DGH_PRECISION_FP64; }
     bool half16() const { return cfg.precision == DGH_PRECISION_MIXED16; }
     float *dg_scale = nullptr;  // FP16 DG factors: per-row reciprocal scales of U
@@ -367,6 +369,11 @@ struct dgh_lockstep {
         ck(cudaGetLastError(), "kernel launch");
     }
 };
+
+void dgh_ctx::sync() {
+    if (slab.comm) slab.comm->wait(stream);
+    else ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+}
 
 namespace {
 // A slab context whose call fails on its own (a CUDA or communication error, which its peers

@@ -15,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -150,6 +151,10 @@ struct LocalComm final : dgh_comm {
         } catch (...) {
         }
     }
+    void set_timeout(int timeout_ms) override {
+        std::lock_guard<std::mutex> lk(g->mu);
+        g->timeout = std::chrono::milliseconds(timeout_ms);
+    }
 };
 
 // ---- NCCL --------------------------------------------------------------------------------------
@@ -210,6 +215,7 @@ struct NcclComm final : dgh_comm {
     int device = 0;
     bool failed = false;
     std::string why;
+    std::chrono::milliseconds timeout{300000};
     const char *kind() const override { return "nccl"; }
     void check() const {
         if (failed) throw dgh_comm_failure("slab communicator failed: " + why);
@@ -248,6 +254,26 @@ struct NcclComm final : dgh_comm {
         why = w;
         if (comm) nccl().abort(comm);  // peers blocked on this rank see the communicator go away
         comm = nullptr;
+    }
+    void set_timeout(int timeout_ms) override { timeout = std::chrono::milliseconds(timeout_ms); }
+    // Polls the stream instead of blocking in it, so that a rank whose peer never joins a
+    // collective (the peer failed on its own) gives up after the timeout: it aborts its
+    // communicator, which ends its own waiting NCCL kernels, and reports the failure.
+    void wait(cudaStream_t st) override {
+        const auto start = std::chrono::steady_clock::now();
+        for (;;) {
+            const cudaError_t e = cudaStreamQuery(st);
+            if (e == cudaSuccess) return;
+            if (e != cudaErrorNotReady)
+                throw std::runtime_error(std::string("cudaStreamQuery: ") + cudaGetErrorString(e));
+            if (std::chrono::steady_clock::now() - start > timeout) {
+                const std::string w = "rank " + std::to_string(rank) + " waited " + std::to_string(timeout.count()) +
+                                      " ms for its stream (a collective that a peer did not enter)";
+                fail(w);
+                throw dgh_comm_failure("slab communicator failed: " + w);
+            }
+            std::this_thread::yield();
+        }
     }
     ~NcclComm() override {
         if (comm) nccl().destroy(comm);
@@ -328,6 +354,12 @@ int dgh_comm_info(const dgh_comm *comm, int out[3]) {
     out[0] = comm->rank;
     out[1] = comm->size;
     out[2] = std::strcmp(comm->kind(), "nccl") == 0 ? 1 : 0;
+    return DGH_OK;
+}
+
+int dgh_comm_set_timeout(dgh_comm *comm, int timeout_ms) {
+    if (!comm || timeout_ms < 1) return DGH_ERR_INVALID;
+    comm->set_timeout(timeout_ms);
     return DGH_OK;
 }
 

@@ -47,6 +47,16 @@ struct dgh_comm {
     virtual void exchange(double *vec, const dgh_halo_plan &plan, cudaStream_t stream) = 0;
     // Marks the group failed so that peers waiting in (or entering) a collective end with an error.
     virtual void fail(const std::string &why) noexcept = 0;
+    // How long a rank waits for its peers, in milliseconds (see the kinds' wait rules).
+    virtual void set_timeout(int timeout_ms) = 0;
+    // Waits for the work queued on `stream` (which may include this rank's collectives).  A CUDA
+    // error is thrown as std::runtime_error; the NCCL kind gives up after its timeout (a peer that
+    // never joins a collective), aborts its communicator so that its own NCCL kernels end, and
+    // throws dgh_comm_failure.
+    virtual void wait(cudaStream_t stream) {
+        const cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) throw std::runtime_error(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
+    }
 };
 
 namespace dgh_slab {

@@ -581,6 +581,10 @@ class SlabComm:
     def fail(self, why: str = "failed by its host"):
         self.lib.dgh_comm_fail(self.h, why.encode())
 
+    def set_timeout(self, timeout_ms: int):
+        """How long this rank waits for its peers (dgh_comm_set_timeout)."""
+        self._check(self.lib.dgh_comm_set_timeout(self.h, timeout_ms))
+
     def close(self):
         if self.h:
             self.lib.dgh_comm_destroy(self.h)

@@ -384,6 +384,11 @@ int dgh_lockstep_report(const dgh_lockstep *group, int64_t out[4]);
  *    than timeout_ms for its peers fails the group (DGH_ERR_COMM on every rank).
  *  - dgh_comm_fail: marks the group failed (a host that caught an error on one rank releases
  *    the others; a context failing with DGH_ERR_CUDA or DGH_ERR_COMM does this itself).
+ *  - dgh_comm_set_timeout: how long a rank waits for its peers (local group: at a barrier,
+ *    default the creation's timeout_ms, for the whole group; NCCL: for its stream, default
+ *    300 s, after which the rank aborts its communicator, ending its own waiting NCCL kernels,
+ *    and the call fails with DGH_ERR_COMM).  A rank that fails on its own therefore ends its
+ *    peers' next collective with DGH_ERR_COMM in every kind.
  * dgh_comm_info: {rank, size, kind (0 local, 1 NCCL)}.  dgh_comm_error: the calling thread's
  * last dgh_comm_* failure. */
 typedef struct dgh_comm dgh_comm;
@@ -393,6 +398,7 @@ int dgh_comm_nccl_unique_id(unsigned char id[128]);
 int dgh_comm_nccl_create(const unsigned char id[128], int size, int rank, int device, dgh_comm **out);
 int dgh_comm_info(const dgh_comm *comm, int out[3]);
 int dgh_comm_fail(dgh_comm *comm, const char *why);
+int dgh_comm_set_timeout(dgh_comm *comm, int timeout_ms);
 int dgh_comm_destroy(dgh_comm *comm);
 const char *dgh_comm_error(void);
 int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out);

@@ -71,6 +71,9 @@ def test_local_group_handles():
 
     g = SlabComm.local_group(3, timeout_ms=500)
     assert [(c.rank, c.size, c.kind) for c in g] == [(0, 3, "local"), (1, 3, "local"), (2, 3, "local")]
+    g[0].set_timeout(2000)
+    with pytest.raises(DGHError):
+        g[0].set_timeout(0)
     g[1].fail("host-side failure")  # marks the group failed; needs no device
     for c in g:
         c.close()
