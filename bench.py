@@ -202,10 +202,24 @@ def algorithmic_bytes(kind: str, m: int, cells: int, fw: int, faces: int, t: int
 # capture at 64x64 k = 8 (4,096 blocks: 1.810513 GB read, 0.010409 GB written); the traffic of a
 # launch grows with the block count.
 SOLVE_FP32_TRAFFIC_PER_BLOCK_K8 = (1.810513e9 + 0.010409e9) / 4096
+# DRAM bytes of one k_lu_solve_half launch per block at k = 8: the DRAM throughput times the
+# duration of one launch at 64x64 k = 8 in one ncu capture (5.02 TB/s x 194.7 us over 4,096 blocks).
+SOLVE_HALF_TRAFFIC_PER_BLOCK_K8 = 5.02e12 * 194.7e-6 / 4096
 
 
-def solve_traffic(args):
-    return SOLVE_FP32_TRAFFIC_PER_BLOCK_K8 * args.nx * args.nx if args.k == 8 else None
+def solve_traffic(args, kernel: str):
+    """(DRAM bytes per launch of the dominant solve kernel at the bench's mesh, their source)."""
+    if args.k != 8:
+        return None, None
+    if kernel.startswith("k_lu_solve<float>"):
+        return (SOLVE_FP32_TRAFFIC_PER_BLOCK_K8 * args.nx * args.nx,
+                "ncu dram bytes of one launch at 64x64 k=8 (profiles/k_lu_solve_fp32_64x64_k8.md) times the "
+                "block-count ratio")
+    if kernel.startswith("k_lu_solve_half"):
+        return (SOLVE_HALF_TRAFFIC_PER_BLOCK_K8 * args.nx * args.nx,
+                "ncu DRAM throughput x duration of one launch at 64x64 k=8 "
+                "(profiles/k_lu_solve_half_and_hdg_apply32_64x64_k8.md) times the block-count ratio")
+    return None, None
 
 
 PROTOCOL_TIMED = 3  # updates 2-4 of every protocol unit are timed (speed_test/2d/benchmark.py:26-36)
@@ -812,9 +826,8 @@ def main():
                    "value_definition": "(K_dg+K_hdg)/(t_dg+t_hdg) over the fastest reduced-precision DG and HDG "
                                        "forms (headline_forms), all at the reference's acceptance tolerance"},
         "roofline": ({k: dom[k] for k in ("bound", "achieved", "peak", "unit", "frac")} | {
-            "traffic": solve_traffic(args) if dom["kernel"].startswith("k_lu_solve<float>") else None,
-            "traffic_source": "ncu dram bytes of one launch at 64x64 k=8 "
-            "(profiles/k_lu_solve_fp32_64x64_k8.md) times the block-count ratio",
+            "traffic": solve_traffic(args, dom["kernel"])[0],
+            "traffic_source": solve_traffic(args, dom["kernel"])[1],
             "kernel": dom["kernel"], "peak_source": peak_src,
             "bytes_per_launch": dom["bytes_per_launch"], "avg_launch_ms": dom["avg_launch_ms"]}) if dom else None,
         "gpu_launches": int(sum(results[k]["launches"] for k in head)),
