@@ -105,3 +105,25 @@ def test_roofline_peaks_file(tmp_path):
     for bad in ("{", json.dumps({"bf16_tflops": 1500.0}), json.dumps({"hbm_gbs": None}), json.dumps({"hbm_gbs": 0})):
         f.write_text(bad)
         assert bench.load_peaks(f) == (bench.FALLBACK_PEAKS, "fallback"), bad
+
+
+def test_roofline_bytes_and_traffic_at_the_bench_mesh():
+    """The per-launch algorithmic bytes of the dominant kernels at 256^2 k = 8 (m = 324, fw = 36,
+    t = 144), and the DRAM traffic the line reports, scaled from the 64^2 captures."""
+    import types
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    E, m, fw, t = 256 * 256, 324, 36, 144
+    assert abs(bench.algorithmic_bytes("dg", m, E, fw, 2 * E, t, "mixed16") - 14.439e9) < 0.01e9
+    assert abs(bench.algorithmic_bytes("dg", m, E, fw, 2 * E, t, "mixed") - 27.94e9) < 0.01e9
+    assert abs(bench.algorithmic_bytes("dg", m, E, fw, 2 * E, t, "fp64") - 55.46e9) < 0.01e9
+    assert abs(bench.algorithmic_bytes("hdg_schur", m, E, fw, 2 * E, t, "mixed") - 5.55e9) < 0.01e9
+    args = types.SimpleNamespace(k=8, nx=256)
+    half, src = bench.solve_traffic(args, "k_lu_solve_half (block-Jacobi solve from FP16 slabs)")
+    assert 1.0 < half / bench.algorithmic_bytes("dg", m, E, fw, 2 * E, t, "mixed16") < 1.1 and "profiles/" in src
+    fp32, _ = bench.solve_traffic(args, "k_lu_solve<float> (block-Jacobi solve)")
+    assert 1.0 < fp32 / bench.algorithmic_bytes("dg", m, E, fw, 2 * E, t, "mixed") < 1.05
+    assert bench.solve_traffic(args, "k_hdg_apply32 (Schur apply)") == (None, None)
+    assert bench.solve_traffic(types.SimpleNamespace(k=4, nx=256), "k_lu_solve_half") == (None, None)
