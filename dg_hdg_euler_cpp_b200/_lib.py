@@ -161,6 +161,8 @@ SIGNATURES = {
     "dgh_comm_info": (ctypes.c_int, [_VP, _I]),
     "dgh_comm_fail": (ctypes.c_int, [_VP, ctypes.c_char_p]),
     "dgh_comm_set_timeout": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "dgh_slab_halo_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int64), _I]),
     "dgh_comm_destroy": (ctypes.c_int, [_VP]),
     "dgh_comm_error": (ctypes.c_char_p, []),
     "dgh_ctx_create_slab": (ctypes.c_int, [ctypes.POINTER(dgh_config), _VP, ctypes.POINTER(_VP)]),

@@ -1984,20 +1984,8 @@ int create_ctx(const dgh_config *cfg, const SlabInit *slab, dgh_ctx **out) {
             c->slab.above = k.ny - 1 - slab->rows;
             c->slab.row_len = (long long)k.nx * NVAR * c->n * c->n;
             c->slab.face_row = (long long)k.nx * c->fw;
-            // volume vectors: rows 1..above go to the rank below (its upper ghost rows), row
-            // `rows` to the rank above (its ghost row 0)
-            const long long rl = c->slab.row_len, R = slab->rows, A = c->slab.above;
-            c->slab.vol.to_below = {{rl, A * rl}};
-            c->slab.vol.to_above = {{R * rl, rl}};
-            c->slab.vol.from_above = {{(R + 1) * rl, A * rl}};
-            c->slab.vol.from_below = {{0, rl}};
-            // trace vectors (x faces, then y faces): row 1's x and upper y faces to the rank
-            // below, row `rows`' upper y faces to the rank above
-            const long long fr = c->slab.face_row, y0 = (long long)c->cells * c->fw;
-            c->slab.trace.to_below = {{fr, fr}, {y0 + fr, fr}};
-            c->slab.trace.to_above = {{y0 + R * fr, fr}};
-            c->slab.trace.from_above = {{(R + 1) * fr, fr}, {y0 + (R + 1) * fr, fr}};
-            c->slab.trace.from_below = {{y0, fr}};
+            c->slab.vol = dgh_slab::volume_plan(c->slab.row_len, slab->rows, c->slab.above);
+            c->slab.trace = dgh_slab::trace_plan(c->slab.face_row, (long long)c->cells * c->fw, slab->rows);
         }
         // nodal_basis.hpp:34-65
         std::vector<double> x, w;

@@ -307,6 +307,23 @@ int dgh_slab_rows(int ny, int size, int rank, int out[4]) {
     return DGH_OK;
 }
 
+int dgh_slab_halo_plan(int nx, int degree, int rows, int above, int trace, int64_t regions[16], int counts[4]) {
+    if (!regions || !counts || nx < 1 || degree < 0 || degree > 8 || rows < above || above < 1 || above > 2)
+        return DGH_ERR_INVALID;
+    const long long n = degree + 1, fw = 4 * n, cells = (long long)nx * (rows + 1 + above);
+    const dgh_halo_plan p = trace ? dgh_slab::trace_plan(nx * fw, cells * fw, rows)
+                                  : dgh_slab::volume_plan(nx * 4 * n * n, rows, above);
+    int k = 0, j = 0;
+    for (const auto *list : {&p.to_below, &p.to_above, &p.from_above, &p.from_below}) {
+        counts[j++] = (int)list->size();
+        for (const auto &r : *list) {
+            regions[k++] = r.offset;
+            regions[k++] = r.count;
+        }
+    }
+    return DGH_OK;
+}
+
 int dgh_comm_local_create(int size, int timeout_ms, dgh_comm **ranks) {
     return comm_guard([&] {
         if (!ranks || size < 1 || timeout_ms < 1) throw dgh_comm_failure("invalid group size, timeout or output");

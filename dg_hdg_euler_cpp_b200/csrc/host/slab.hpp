@@ -66,4 +66,28 @@ inline void rows_of(int ny, int size, int rank, int &row0, int &rows) {
     rows = base + (rank < extra ? 1 : 0);
     row0 = rank * base + (rank < extra ? rank : extra);
 }
+// The halo of a volume vector (row_len doubles per cell row; local row 0 the ghost row below,
+// rows 1..rows the slab's, then `above` ghost rows): rows 1..above go to the rank below (its
+// upper ghost rows), row `rows` to the rank above (its ghost row 0).
+inline dgh_halo_plan volume_plan(long long row_len, int rows, int above) {
+    const long long rl = row_len, R = rows, A = above;
+    dgh_halo_plan p;
+    p.to_below = {{rl, A * rl}};
+    p.to_above = {{R * rl, rl}};
+    p.from_above = {{(R + 1) * rl, A * rl}};
+    p.from_below = {{0, rl}};
+    return p;
+}
+// The halo of a trace vector (x faces, then y faces from y0; face_row doubles per face row; a
+// face belongs to the cell left of or below it): row 1's x and upper y faces go to the rank below
+// (its first ghost row above), row `rows`' upper y faces to the rank above (its ghost row 0's).
+inline dgh_halo_plan trace_plan(long long face_row, long long y0, int rows) {
+    const long long fr = face_row, R = rows;
+    dgh_halo_plan p;
+    p.to_below = {{fr, fr}, {y0 + fr, fr}};
+    p.to_above = {{y0 + R * fr, fr}};
+    p.from_above = {{(R + 1) * fr, fr}, {y0 + (R + 1) * fr, fr}};
+    p.from_below = {{y0, fr}};
+    return p;
+}
 }  // namespace dgh_slab

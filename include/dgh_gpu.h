@@ -399,6 +399,12 @@ int dgh_comm_nccl_create(const unsigned char id[128], int size, int rank, int de
 int dgh_comm_info(const dgh_comm *comm, int out[3]);
 int dgh_comm_fail(dgh_comm *comm, const char *why);
 int dgh_comm_set_timeout(dgh_comm *comm, int timeout_ms);
+/* The halo plan a slab context of mesh width nx, degree, `rows` interior rows and `above` ghost
+ * rows above uses for volume vectors (trace = 0) or trace vectors (trace = 1): counts = the
+ * number of regions sent to the rank below, sent to the rank above, received from the rank above
+ * and received from the rank below; regions = their (offset, count) pairs in doubles, in that
+ * order.  Host arithmetic only (no device). */
+int dgh_slab_halo_plan(int nx, int degree, int rows, int above, int trace, int64_t regions[16], int counts[4]);
 int dgh_comm_destroy(dgh_comm *comm);
 const char *dgh_comm_error(void);
 int dgh_ctx_create_slab(const dgh_config *cfg, dgh_comm *comm, dgh_ctx **out);

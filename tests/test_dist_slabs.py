@@ -121,3 +121,116 @@ def test_two_gloo_ranks_share_the_nccl_id_and_partition(ny):
         assert r["len"] == 128 and r["same"]
         parts = r["parts"]
         assert parts[0][0] == 0 and parts[0][0] + parts[0][1] == parts[1][0] and parts[1][0] + parts[1][1] == ny
+
+
+def halo_plan(nx, k, rows, above, trace):
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    regions, counts = (ctypes.c_int64 * 16)(), (ctypes.c_int * 4)()
+    assert _lib.load().dgh_slab_halo_plan(nx, k, rows, above, trace, regions, counts) == 0
+    out, i = [], 0
+    for c in counts:
+        out.append([(regions[i + 2 * j], regions[i + 2 * j + 1]) for j in range(c)])
+        i += 2 * c
+    return dict(zip(("to_below", "to_above", "from_above", "from_below"), out))
+
+
+def unit_rows(regions, unit, half):
+    """(axis, local row) of every row-sized unit the regions cover; axis 0 for x faces or cells,
+    1 for y faces (offsets at or beyond `half`)."""
+    rows = []
+    for off, cnt in regions:
+        assert off % unit == 0 and cnt % unit == 0
+        for u in range(off // unit, (off + cnt) // unit):
+            rows.append((1, u - half // unit) if half and off >= half else (0, u))
+    return rows
+
+
+@pytest.mark.parametrize("ny,size", [(6, 2), (9, 3), (12, 4), (7, 2), (16, 8)])
+@pytest.mark.parametrize("k", [1, 3, 8])
+def test_trace_halo_brings_every_face_the_owned_schur_rows_read(ny, size, k):
+    """The HDG slab layout against the periodic grid: the Schur apply of an owned face reads the
+    faces of the two cells beside it, the recovery of an interior cell its own four faces; each of
+    those is owned or arrives by the trace halo, every region received holds the same global
+    faces the neighbour sends, and every face sent is owned by its sender."""
+    from dg_hdg_euler_cpp_b200.solver import slab_rows
+
+    nx, above, n = 5, 2, k + 1
+    fw = 4 * n
+    fr = nx * fw
+    parts = [slab_rows(ny, size, r) for r in range(size)]
+    plans = [halo_plan(nx, k, p[1], above, 1) for p in parts]
+    for r, (row0, rows, below, above_rank) in enumerate(parts):
+        L = rows + 1 + above
+        cells = nx * L
+        half = cells * fw
+
+        def nb(cell, side):
+            x, y = cell % nx, cell // nx
+            if side < 2:
+                x = (x + (-1 if side == 0 else 1)) % nx
+            else:
+                y = (y + (-1 if side == 2 else 1)) % L
+            return x + nx * y
+
+        def face_of(cell, side):
+            return [nb(cell, 0), cell, cells + nb(cell, 2), cells + cell][side]
+
+        owned = {f for f in range(2 * cells) if 1 <= (f % cells) // nx <= rows}
+        got = set(owned)
+        for off, cnt in plans[r]["from_above"] + plans[r]["from_below"]:
+            got |= set(range(off // fw, (off + cnt) // fw))
+        for f in owned:
+            axis, first = f // cells, f % cells
+            for cell in (first, nb(first, 2 * axis + 1)):
+                for side in range(4):
+                    assert face_of(cell, side) in got, (r, f, cell, side)
+        # the recovery and the recovered residual of an interior cell read its four faces
+        for cell in range(nx, nx * (rows + 1)):
+            assert all(face_of(cell, side) in got for side in range(4)), (r, cell)
+
+        def global_rows(rank, regions, cells_r):
+            row0_r = parts[rank][0]
+            return [(a, (row0_r - 1 + j) % ny) for a, j in unit_rows(regions, fr, cells_r * fw)]
+
+        cells_above = nx * (parts[above_rank][1] + 1 + above)
+        cells_below = nx * (parts[below][1] + 1 + above)
+        assert global_rows(r, plans[r]["from_above"], cells) == global_rows(above_rank, plans[above_rank]["to_below"],
+                                                                            cells_above)
+        assert global_rows(r, plans[r]["from_below"], cells) == global_rows(below, plans[below]["to_above"],
+                                                                            cells_below)
+        for off, cnt in plans[r]["to_below"] + plans[r]["to_above"]:
+            assert set(range(off // fw, (off + cnt) // fw)) <= owned
+
+
+@pytest.mark.parametrize("ny,size,above", [(6, 2, 1), (9, 3, 1), (5, 5, 1), (12, 4, 2), (7, 3, 2)])
+def test_volume_halo_fills_every_ghost_row_with_the_right_global_row(ny, size, above):
+    from dg_hdg_euler_cpp_b200.solver import slab_rows
+
+    nx, k = 4, 2
+    rl = nx * 4 * (k + 1) ** 2
+    parts = [slab_rows(ny, size, r) for r in range(size)]
+    if min(p[1] for p in parts) < above:
+        pytest.skip("fewer rows than ghost rows above")
+    plans = [halo_plan(nx, k, p[1], above, 0) for p in parts]
+    for r, (row0, rows, below, up) in enumerate(parts):
+        filled = {j for off, cnt in plans[r]["from_above"] + plans[r]["from_below"]
+                  for j in range(off // rl, (off + cnt) // rl)}
+        assert filled == {0} | set(range(rows + 1, rows + 1 + above))  # every ghost row, nothing else
+
+        def g(rank, regions):
+            return [(parts[rank][0] - 1 + j) % ny for _, j in unit_rows(regions, rl, 0)]
+
+        assert g(r, plans[r]["from_above"]) == g(up, plans[up]["to_below"])
+        assert g(r, plans[r]["from_below"]) == g(below, plans[below]["to_above"])
+        for off, cnt in plans[r]["to_below"] + plans[r]["to_above"]:
+            assert all(1 <= j <= rows for j in range(off // rl, (off + cnt) // rl))
+
+
+def test_halo_plan_rejects_bad_shapes():
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    regions, counts = (ctypes.c_int64 * 16)(), (ctypes.c_int * 4)()
+    lib = _lib.load()
+    for args in ((4, 2, 1, 2, 1), (4, 9, 3, 1, 0), (0, 2, 3, 1, 0), (4, 2, 3, 3, 1)):
+        assert lib.dgh_slab_halo_plan(*args, regions, counts) == 1
