@@ -33,6 +33,20 @@ def test_library_exports_every_declared_symbol(lib):
     assert not missing, missing
 
 
+def test_library_exports_nothing_undeclared():
+    """Every extern "C" dgh_* symbol the library exports is declared in the header (no hidden
+    entry points)."""
+    import subprocess
+
+    from dg_hdg_euler_cpp_b200 import _lib
+
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {parts[-1] for parts in (line.split() for line in out.splitlines())
+                if len(parts) >= 3 and parts[1] == "T" and parts[-1].startswith("dgh_")}
+    assert exported and exported <= set(declared_functions()), sorted(exported - set(declared_functions()))
+
+
 def test_python_binding_covers_the_header():
     from dg_hdg_euler_cpp_b200 import _lib
 
